@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Benchmark of the Potts primal-dual segmentation solve on B200.
+
+Workload (one "step" = one full solve): the 768 x 768 x 1024 cylindrical core
+(radius 370, 440,434,688 in-mask voxels), K = 3 labels, lambda = 30,
+tau = tau' = 1/sqrt(12), 1000 iterations, FP64 energies every 50 iterations.
+Input: a seeded synthetic phantom (glass matrix, brine/scCO2 spheres of radius
+6-30, Gaussian blur sigma 1, noise 7e-3), generated on the GPU; the state
+(~30 GB) is far larger than L2, so no L2 flush is needed between steps.
+
+Metric: in-mask voxel-iterations per second (Gvox-iter/s), whole job.
+  value  device-resident input, CUDA events around K solves on the solver's stream
+  e2e    the same solves through the host-buffer C-ABI call (pinned u in,
+         ci[argmax] + label bytes out), copies inside the timed region
+Also: the roofline of the dominant kernel (the fused iteration) from the
+solver's own per-iteration device timing, and a CPU baseline (the FP64 oracle
+on this machine's cores, bounded sample).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun each rank solves its own phantom (weak scaling, no data-path
+collective: the ranks' volumes are independent).
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "Potts PD Gvox-iter/s at k=3, %HBM peak; BF16-store vs FP32 at ≤1e-4 label flips"
+UNIT = "Gvox-iter/s"
+K_LABELS = 3
+LAMBDA = 30.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--iters", type=int, default=1000)
+    p.add_argument("--gap-every", type=int, default=50)
+    p.add_argument("--variant", choices=["fused", "plain"], default="fused")
+    p.add_argument("--workload", choices=["config1", "config0"], default="config1")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
+    return p.parse_args()
+
+
+def tau_baseline() -> float:
+    import numpy as np
+
+    return float(np.float32(1.0) / np.sqrt(np.float32(12.0)))
+
+
+# ----------------------------------------------------------------------------- distributed plumbing
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+
+    def init(self, backend="nccl"):
+        import torch
+        import torch.distributed as dist
+
+        if self.world > 1 and not self.pg:
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            kw = {"device_id": torch.device("cuda", self.local)} if backend == "nccl" else {}
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=900), **kw)
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    def reduce(self, x: float, op: str) -> float:
+        if not self.pg:
+            return x
+        import torch
+        import torch.distributed as dist
+
+        t = torch.tensor([x], dtype=torch.float64, device=torch.device("cuda", self.local))
+        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+            self.pg = False
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.dev), "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in Path(self.path).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+# ----------------------------------------------------------------------------- peaks / traffic
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+        except Exception:
+            pass
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profiled_traffic(variant: str) -> dict | None:
+    """DRAM bytes per voxel-iteration of the dominant kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return d.get(variant)
+    except Exception:
+        return None
+
+
+def bytes_per_voxel_iter(variant: str, k: int = K_LABELS) -> int:
+    """Algorithmic DRAM bytes per in-mask voxel and iteration (FP32 state).
+    fused: Xi (3(K-1)) and V (K-1) read and written once, u read once;
+    split: dual launch reads Vbar, Xi and writes Xi; primal launch reads Xi, V, u
+           and writes V, Vbar."""
+    if variant == "fused":
+        return 4 * (8 * (k - 1) + 1)
+    return 4 * (13 * (k - 1) + 1)
+
+
+# ----------------------------------------------------------------------------- CPU baseline (oracle)
+def cpu_sample_phantom():
+    from segmentctscans_b200.phantom import make_phantom
+
+    # the config-1 cross-section and recipe, 16 slices along the axis, built on the CPU
+    return make_phantom(16, 768, 768, 370.0, seed=0, radius_range=(6.0, 30.0), noise=7e-3, device="cpu")
+
+
+def run_cpu_oracle(ph, iters: int, threads: int) -> float:
+    from oracle import oracle
+
+    oracle.set_threads(threads)
+    u = ph.u.numpy().copy()
+    tau = tau_baseline()
+    t0 = time.perf_counter()
+    oracle.solve(ph.mapping, u, ph.ci, LAMBDA, tau, tau, iters, precision="f64", want_state=False)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(budget_s: float) -> dict:
+    ph = cpu_sample_phantom()
+    threads = os.cpu_count() or 1
+    t1 = run_cpu_oracle(ph, 1, threads)
+    iters = max(1, min(200, int(budget_s / max(t1, 1e-3))))
+    t = run_cpu_oracle(ph, iters, threads)
+    vox = ph.mapping.data_size
+    return {"value": vox * iters / t / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"FP64 oracle, OpenMP {threads} threads: 768x768 cross-section (r=370), 16 slices "
+                      f"({vox} in-mask voxels), K=3, {iters} iterations, {t:.1f} s"}
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args, dist_: Dist) -> None:
+    if dist_.rank != 0:
+        return
+    ph = cpu_sample_phantom()
+    threads = os.cpu_count() or 1
+    t1 = run_cpu_oracle(ph, 1, threads)
+    iters = max(1, int(min(args.cpu_seconds / 3.0, 20.0) / max(t1, 1e-3)))
+    for _ in range(args.warmup):
+        run_cpu_oracle(ph, 1, threads)
+    times = [run_cpu_oracle(ph, iters, threads) for _ in range(args.steps)]
+    vox = ph.mapping.data_size
+    total = sum(times)
+    value = vox * iters * args.steps / total / 1e9
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "potts_k3_768x768_r370_cpu_sample", "rows": 768, "cols": 768, "n_slices": 16,
+                   "radius": 370, "k": K_LABELS, "lambda": LAMBDA, "iters_per_step": iters},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"the reference has no CPU implementation of this path and cannot be built "
+                                   f"here; FP64 oracle port, {threads} threads, {vox} voxels x {iters} iterations "
+                                   f"per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+# ----------------------------------------------------------------------------- our arm
+def run_ours(args, dist_: Dist) -> None:
+    import numpy as np
+    import torch
+
+    from segmentctscans_b200 import potts
+    from segmentctscans_b200.phantom import config0_phantom, config1_phantom
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    dev = torch.device("cuda", dist_.local)
+    torch.cuda.set_device(dev)
+    dist_.init("nccl")
+
+    ph = (config1_phantom(seed=dist_.rank, device=dev) if args.workload == "config1"
+          else config0_phantom(seed=dist_.rank, device=dev))
+    m, u, ci = ph.mapping, ph.u, ph.ci
+    truth = ph.truth
+    del ph
+    torch.cuda.empty_cache()
+    span = m.span
+    tau = tau_baseline()
+    variant = 0 if args.variant == "fused" else 1
+    stream = torch.cuda.current_stream(dev)
+    ctx = potts.make_context(dev.index, stream=stream.cuda_stream)
+    res = torch.empty(span, dtype=torch.float32, device=dev)
+    lab = torch.empty(span, dtype=torch.uint8, device=dev)
+
+    def step():
+        return potts.solve_device(ctx, m, u.data_ptr(), ci, LAMBDA, tau, tau, args.iters, res_ptr=res.data_ptr(),
+                                  labels_ptr=lab.data_ptr(), stats=True, variant=variant,
+                                  gap_every=args.gap_every)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    dist_.barrier()
+    torch.cuda.synchronize(dev)
+
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    stats = [step() for _ in range(args.steps)]
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    dist_.barrier()
+    clk = clocks.stop()
+    t_local = e0.elapsed_time(e1) / 1000.0
+    t_max = dist_.reduce(t_local, "max")
+    vox = m.data_size
+    vox_iters_all = dist_.reduce(float(vox) * args.iters * args.steps, "sum")
+    value = vox_iters_all / t_max / 1e9
+
+    # roofline of the fused iteration kernel: algorithmic bytes / average launch time
+    loop_ms = sum(s.loop_ms for s in stats)
+    loop_launches = sum(s.loop_launches for s in stats)
+    launch_s = loop_ms / 1000.0 / max(loop_launches, 1)
+    bpv = bytes_per_voxel_iter(args.variant)
+    # the split form runs two launches per iteration
+    per_launch_bytes = bpv * vox if args.variant == "fused" else bpv * vox / 2
+    achieved = per_launch_bytes / launch_s / 1e9
+    peaks = measured_peaks()
+    tr = profiled_traffic(args.variant)
+    traffic = tr["dram_bytes_per_voxel_iter"] * vox if tr else None
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
+                "kernel": "potts::fused_*_kernel" if args.variant == "fused" else "potts::dual_kernel+primal_kernel",
+                "bytes_per_voxel_iter": bpv, "avg_launch_ms": round(launch_s * 1000, 4),
+                "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)"}
+
+    # quality figures of the last solve
+    last = stats[-1]
+    gap = last.energy_trace[-1].tolist() if last.energy_trace is not None else None
+    lab_in = lab.view(m.n_lines, m.nstride)[:, : m.n_images]
+    tru_in = truth.view(m.n_lines, m.nstride)[:, : m.n_images]
+    agree = float((lab_in == tru_in).float().mean().item())
+
+    # end to end through the host-buffer C-ABI call
+    e2e = None
+    if not args.no_e2e:
+        hu = torch.empty(span, dtype=torch.float32, pin_memory=True)
+        hu.copy_(u.cpu())
+        hres = torch.empty(span, dtype=torch.float32, pin_memory=True)
+        hlab = torch.empty(span, dtype=torch.uint8, pin_memory=True)
+        hu_np, hres_np, hlab_np = hu.numpy(), hres.numpy(), hlab.numpy()
+
+        def e2e_step():
+            potts.solve_host(ctx, m, hu_np, ci, LAMBDA, tau, tau, args.iters, res=hres_np, labels=hlab_np,
+                             variant=variant, gap_every=args.gap_every)
+
+        e2e_step()  # allocates the context's staging buffers
+        torch.cuda.synchronize(dev)
+        dist_.barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = time.perf_counter()
+        f0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        f1.record(stream)
+        torch.cuda.synchronize(dev)
+        w1 = time.perf_counter()
+        te = max(f0.elapsed_time(f1) / 1000.0, 0.0)
+        te = dist_.reduce(max(te, w1 - w0), "max")
+        same = bool(np.array_equal(hlab_np, lab.cpu().numpy()))
+        e2e = {"value": vox_iters_all / te / 1e9, "unit": UNIT, "h2d_bytes_per_step": 4 * span,
+               "d2h_bytes_per_step": 5 * span, "matches_device_run": same}
+
+    cpu = None
+    if dist_.rank == 0 and dist_.world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_seconds)
+
+    launches = sum(s.total_launches for s in stats)
+    if dist_.rank == 0:
+        out = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist_.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1000 * t_max / args.steps, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"potts_k3_{'768x768x1024_r370' if args.workload == 'config1' else '128cube_r60'}",
+                       "rows": m.rows, "cols": m.cols, "n": m.n_images, "radius": 370 if args.workload == "config1" else 60,
+                       "in_mask_voxels": vox, "k": K_LABELS, "lambda": LAMBDA, "tau": tau, "iters": args.iters,
+                       "gap_every": args.gap_every, "variant": args.variant, "storage": "f32",
+                       "parallelism": f"replica x{dist_.world}" if dist_.world > 1 else "single",
+                       "l2": "inputs larger than L2 (state ~30 GB per GPU)"},
+            "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clk, "cpu_baseline": cpu,
+            "quality": {"final_sqrt_max_dV2": last.dq_last, "energy_last": gap, "truth_agreement": round(agree, 5)},
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    dist_.close()
+
+
+def main():
+    args = parse_args()
+    d = Dist()
+    if args.impl == "reference":
+        run_reference(args, d)
+        return
+    run_ours(args, d)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,170 @@
+/*
+ * potts_b200.h — C ABI of the B200 (sm_100a) multiphase Potts segmentation solver.
+ *
+ * This library replaces the GPU path of the reference's potts-model tool:
+ * the Chambolle–Cremers–Pock primal-dual iteration of
+ * potts-model/potts-min-partition.{h,cpp} together with the minimal device
+ * runtime it runs on (cuda-context/cuda-context.cpp, include/cuda-context.h,
+ * include/cuda-details/*.h) and the cylindrical-core layout
+ * (include/layout_cylinder.h).
+ *
+ * Conventions
+ *  - Volumes use the reference's cylinder layout: index (n, row, col), n is
+ *    the contiguous axis with stride `nstride` (a multiple of 32 floats), each
+ *    column col stores rows [start_row[col], start_row[col] + rows_in_col)
+ *    consecutively from offset base[col].  offset(n, row, col) =
+ *    base[col] + (row - start_row[col]) * nstride + n
+ *    (include/layout_cylinder.h:81-84).
+ *  - Every function returns an int status (POTTS_OK = 0) and never throws;
+ *    potts_last_error() gives a message for the calling thread.
+ *  - All work is ordered on the context's stream.  A context is not
+ *    thread-safe; use one context per host thread.
+ *  - Plain pointers and sizes only; no C++ or framework types cross the ABI.
+ */
+#ifndef POTTS_B200_H
+#define POTTS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* include/cuda-context.h:7 — labels supported per solve: 2 .. POTTS_MAX_PHASES */
+#define POTTS_MAX_PHASES 6
+
+enum potts_status {
+    POTTS_OK = 0,
+    POTTS_EINVAL = 1,   /* bad argument (K, sizes, mapping, NaN parameters) */
+    POTTS_ENOMEM = 2,   /* not enough device memory (potts-min-partition.cpp:571-577) */
+    POTTS_ECUDA = 3,    /* a CUDA runtime call failed */
+    POTTS_ETIMEOUT = 4, /* a bounded device-side wait gave up */
+    POTTS_ENODEV = 5    /* no CUDA device / driver */
+};
+
+/* Host view of layout_cylinder::mapping (include/layout_cylinder.h:30-112).
+ * The tables are read during the call and not retained. */
+typedef struct potts_mapping {
+    uint32_t n_images;         /* extent 0: number of slices along the cylinder axis */
+    uint32_t rows;             /* extent 1 */
+    uint32_t cols;             /* extent 2 */
+    uint32_t nstride;          /* stride of the n axis (multiple of 32) */
+    uint32_t col_begin;        /* first column holding rows */
+    uint32_t col_end;          /* one past the last column holding rows */
+    const uint32_t *start_row; /* [cols]   first stored row of each column */
+    const uint32_t *base;      /* [cols+1] offset of each column; base[cols] = span */
+} potts_mapping;
+
+typedef struct potts_context potts_context; /* CudaContext (include/cuda-details/cuda-context-impl.h:35-65) */
+typedef struct potts_field potts_field;     /* DeviceField<float> (include/cuda-details/device-field-impl.h:12-54) */
+
+enum potts_variant {
+    POTTS_VARIANT_FUSED = 0, /* one fused stencil launch per iteration (default) */
+    POTTS_VARIANT_PLAIN = 1  /* the reference's split: a dual launch and a primal launch per iteration */
+};
+
+enum potts_storage {
+    POTTS_STORE_F32 = 0 /* state (Xi, V) stored in FP32 */
+};
+
+typedef struct potts_options {
+    int variant;      /* enum potts_variant */
+    int storage;      /* enum potts_storage */
+    int gap_every;    /* FP64 energies after every gap_every-th iteration; 0 = off */
+    int slab_w;       /* 0: plan slabs from free memory like the reference; > 0: force this slab width */
+    int track_dq;     /* 1: record max_x |V^{k+1} - V^k|^2 of every iteration on the device */
+    int sync_monitor; /* 1: reference behaviour, read the monitor back and sync after every iteration */
+} potts_options;
+
+typedef struct potts_stats {
+    int n_slabs;          /* out: slabs run */
+    int slab_w;           /* out: slab width (n-slices) */
+    int iters;            /* out: iterations per slab */
+    float dq_last;        /* out: sqrt(max |dV|^2) of the last iteration (needs track_dq) */
+    double solve_ms;      /* out: device time from init to argmax, all slabs */
+    double loop_ms;       /* out: device time of the iteration launches (fused or split), all slabs */
+    int loop_launches;    /* out: kernel launches inside loop_ms */
+    int total_launches;   /* out: kernel launches of the whole solve */
+    uint64_t state_bytes; /* out: device bytes held by the solver state */
+    float *dq_trace;      /* in, optional: [iters] max |dV|^2 per iteration of the last slab (host) */
+    double *energy_trace; /* in, optional: [3 * (iters / gap_every)] (lagrangian, dual, gap) (host) */
+} potts_stats;
+
+/* Defaults: fused, FP32, no gap, planner-chosen slabs, track_dq = 1, no per-iteration sync. */
+void potts_default_options(potts_options *opts);
+const char *potts_status_string(int status);
+const char *potts_last_error(void);
+
+/* make_context() (cuda-context/cuda-context.cpp:18-20): device `device`, a new stream. */
+int potts_context_create(int device, potts_context **out);
+/* Same, but all work goes to the caller's cudaStream_t `stream` (not owned). */
+int potts_context_create_on_stream(int device, void *stream, potts_context **out);
+void potts_context_destroy(potts_context *ctx);
+int potts_context_synchronize(potts_context *ctx);
+/* device_memory() (cuda-context/cuda-context.cpp:22-42): free bytes + bytes cached by this context. */
+int potts_device_memory(potts_context *ctx, size_t *available, size_t *total);
+
+/* DeviceField(mapping, stream, mr) (device-field-impl.h:24-33): uninitialised voxels. */
+int potts_field_create(potts_context *ctx, const potts_mapping *map, potts_field **out);
+/* upload() (cuda-context/cuda-context.cpp:49-57): copies `span` = base[cols] floats. */
+int potts_field_upload(potts_context *ctx, const potts_mapping *map, const float *host, potts_field **out);
+/* download() (cuda-context/cuda-context.cpp:59-77): synchronous; span must match. */
+int potts_field_download(potts_context *ctx, const potts_field *field, float *host, uint64_t span);
+float *potts_field_data(potts_field *field);
+uint64_t potts_field_span(const potts_field *field);
+void potts_field_destroy(potts_field *field);
+
+/*
+ * potts_min_partition<K> (potts-model/potts-min-partition.h:8-16,
+ * potts-model/potts-min-partition.cpp:540-679).
+ *   g        device field u in [0,1] (borrowed, not modified)
+ *   cpu_map  host mapping of g (borrowed)
+ *   ci       K labels in the normalised units of u (host array)
+ *   lambda   data weight; tau1 primal step; tau2 dual step
+ *   iters    iterations per slab (also the slab halo)
+ *   result   out: new field with the mapping of g holding ci[argmax_i V_i]
+ * opts / stats may be NULL.  Returns POTTS_ENOMEM where the reference prints
+ * "Not enough memory" and returns an empty pointer.
+ */
+int potts_min_partition(potts_context *ctx, const potts_field *g, const potts_mapping *cpu_map, int K,
+                        const float *ci, float lambda, float tau1, float tau2, int iters,
+                        const potts_options *opts, potts_field **result, potts_stats *stats);
+
+/*
+ * Device-pointer form of the same solve.  d_u and every output are device
+ * pointers laid out with `map` (span = base[cols] voxels per plane); each
+ * output may be NULL:
+ *   d_res     span floats: ci[argmax]                        (update_kernel)
+ *   d_labels  span bytes:  argmax index
+ *   d_V       (K-1) planes of span floats: relaxed V_0..V_{K-2} (V_{K-1} = 1 - sum)
+ *   d_Xi      3(K-1) planes of span floats: dual field, plane 3*i + axis
+ *             (axis 0 = n, 1 = row, 2 = col)
+ * Voxels outside the mask and padding (n >= n_images) are not written.
+ */
+int potts_solve_device(potts_context *ctx, const potts_mapping *map, const float *d_u, int K, const float *ci,
+                       float lambda, float tau1, float tau2, int iters, const potts_options *opts, float *d_res,
+                       uint8_t *d_labels, float *d_V, float *d_Xi, potts_stats *stats);
+
+/*
+ * Host-buffer form (what potts-model.cpp does around the call: upload, solve,
+ * download).  h_u is span floats on the host (pinned memory is faster); the
+ * outputs h_res (span floats) and h_labels (span bytes) may be NULL.  Blocks
+ * until the results are on the host.
+ */
+int potts_solve_host(potts_context *ctx, const potts_mapping *map, const float *h_u, int K, const float *ci,
+                     float lambda, float tau1, float tau2, int iters, const potts_options *opts, float *h_res,
+                     uint8_t *h_labels, potts_stats *stats);
+
+/* Mask constructor of layout_cylinder::mapping_storage (include/layout_cylinder.h:152-195):
+ * fills start_row[cols] and base[cols+1], returns the span (base[cols]). */
+uint64_t potts_cylinder_mapping(uint32_t rows, uint32_t cols, double xc, double yc, double r, uint32_t nstride,
+                                uint32_t *start_row, uint32_t *base, uint32_t *col_begin, uint32_t *col_end);
+/* Field<float>::get_stride (include/field.h:37-40): n rounded up to 32. */
+uint32_t potts_get_stride(uint32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* POTTS_B200_H */

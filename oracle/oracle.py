@@ -1,0 +1,195 @@
+"""ctypes wrapper of the CPU oracle (test infrastructure only).
+
+Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of bench.py
+use this module, as the checker.  The restated algorithm lives in
+``potts_oracle.c`` (FP64 and FP32 builds) and ``cylinder_oracle.c``; see their
+headers for the reference lines each function follows.  Parity unpinned: the
+reference has no tests or golden vectors for this path and cannot be built
+here.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from .build import LIB_PATH, build_oracle
+
+
+class OCyl(ctypes.Structure):
+    _fields_ = [
+        ("n_images", ctypes.c_uint32), ("rows", ctypes.c_uint32), ("cols", ctypes.c_uint32),
+        ("nstride", ctypes.c_uint32), ("col_begin", ctypes.c_uint32), ("col_end", ctypes.c_uint32),
+        ("start_row", ctypes.POINTER(ctypes.c_uint32)), ("base", ctypes.POINTER(ctypes.c_uint32)),
+    ]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build_oracle()
+        _lib = ctypes.CDLL(str(LIB_PATH))
+    return _lib
+
+
+def _ptr(a, ct):
+    return a.ctypes.data_as(ctypes.POINTER(ct)) if a is not None else None
+
+
+def _real(precision: str):
+    if precision == "f64":
+        return np.float64, ctypes.c_double
+    if precision == "f32":
+        return np.float32, ctypes.c_float
+    raise ValueError(precision)
+
+
+def set_threads(n: int) -> None:
+    lib().oracle_set_threads(int(n))
+
+
+def max_threads() -> int:
+    return int(lib().oracle_max_threads())
+
+
+def ocyl(m) -> OCyl:
+    sr = np.ascontiguousarray(m.start_row, dtype=np.uint32)
+    bs = np.ascontiguousarray(m.base, dtype=np.uint32)
+    c = OCyl(m.n_images, m.rows, m.cols, m.nstride, m.col_begin, m.col_end, _ptr(sr, ctypes.c_uint32),
+             _ptr(bs, ctypes.c_uint32))
+    c._keep = (sr, bs)
+    return c
+
+
+def cylinder_mask(rows: int, cols: int, xc: float, yc: float, r: float, nstride: int):
+    """(start_row, base, col_begin, col_end, span) per include/layout_cylinder.h:152-195."""
+    sr = np.zeros(cols, np.uint32)
+    bs = np.zeros(cols + 1, np.uint32)
+    cb, ce = ctypes.c_uint32(), ctypes.c_uint32()
+    f = lib().oracle_cylinder_mask
+    f.restype = ctypes.c_uint64
+    f.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                  ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
+                  ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]
+    span = f(rows, cols, xc, yc, r, nstride, _ptr(sr, ctypes.c_uint32), _ptr(bs, ctypes.c_uint32),
+             ctypes.byref(cb), ctypes.byref(ce))
+    return sr, bs, int(cb.value), int(ce.value), int(span)
+
+
+def project_simplex(q: np.ndarray, precision: str = "f64") -> np.ndarray:
+    dt, ct = _real(precision)
+    out = np.ascontiguousarray(np.array(q, dtype=dt))
+    f = getattr(lib(), f"oracle_project_simplex_{precision}")
+    f.argtypes = [ctypes.POINTER(ct), ctypes.c_int]
+    f(_ptr(out, ct), int(out.size))
+    return out
+
+
+def project_K(q: np.ndarray, precision: str = "f64") -> tuple[np.ndarray, int]:
+    """q: [K, 3] -> (projected [K, 3], sweeps)."""
+    dt, ct = _real(precision)
+    out = np.ascontiguousarray(np.array(q, dtype=dt).reshape(-1, 3))
+    f = getattr(lib(), f"oracle_project_K_{precision}")
+    f.argtypes = [ctypes.POINTER(ct), ctypes.c_int]
+    f.restype = ctypes.c_int
+    sw = f(_ptr(out, ct), int(out.shape[0]))
+    return out, int(sw)
+
+
+@dataclass
+class OracleResult:
+    res: np.ndarray
+    labels: np.ndarray
+    V: Optional[np.ndarray]
+    Xi: Optional[np.ndarray]
+    dq_trace: np.ndarray
+    energy_trace: Optional[np.ndarray]
+    sweep_hist: np.ndarray
+
+
+def solve(m, u: np.ndarray, ci, lam: float, tau1: float, tau2: float, iters: int, *, precision: str = "f64",
+          slab_w: int = 0, want_state: bool = True, gap_every: int = 0) -> OracleResult:
+    """The whole solve (potts-model/potts-min-partition.cpp:540-679) on the CPU."""
+    dt, ct = _real(precision)
+    K = len(ci)
+    span = int(m.base[m.cols])
+    c = np.ascontiguousarray(np.asarray(ci, np.float32))
+    u = np.ascontiguousarray(u, dtype=np.float32)
+    if u.size != span:
+        raise ValueError("u size != span")
+    res = np.zeros(span, np.float32)
+    labels = np.zeros(span, np.uint8)
+    V = np.zeros((K - 1, span), dt) if want_state else None
+    Xi = np.zeros((3 * (K - 1), span), dt) if want_state else None
+    dq = np.zeros(max(iters, 1), np.float32)
+    ne = iters // gap_every if gap_every > 0 else 0
+    en = np.zeros((max(ne, 1), 3), np.float64) if ne > 0 else None
+    hist = np.zeros(21, np.int32)
+    f = getattr(lib(), f"oracle_solve_{precision}")
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.POINTER(OCyl), ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.POINTER(ctypes.c_float),
+                  ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                  ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ct),
+                  ctypes.POINTER(ct), ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                  ctypes.POINTER(ctypes.c_int)]
+    oc = ocyl(m)
+    rc = f(ctypes.byref(oc), _ptr(u, ctypes.c_float), K, _ptr(c, ctypes.c_float), float(lam), float(tau1),
+           float(tau2), int(iters), int(slab_w), _ptr(res, ctypes.c_float), _ptr(labels, ctypes.c_uint8),
+           _ptr(V, ct), _ptr(Xi, ct), _ptr(dq, ctypes.c_float), int(gap_every), _ptr(en, ctypes.c_double),
+           _ptr(hist, ctypes.c_int))
+    if rc != 0:
+        raise RuntimeError("oracle_solve failed (bad arguments or slab planner)")
+    return OracleResult(res, labels, V, Xi, dq[:iters], en, hist)
+
+
+def grad_step(m, K: int, xi: np.ndarray, Vb: np.ndarray, tau2: float, precision: str = "f64") -> np.ndarray:
+    dt, ct = _real(precision)
+    xi = np.ascontiguousarray(xi, dtype=dt).copy()
+    Vb = np.ascontiguousarray(Vb, dtype=dt)
+    f = getattr(lib(), f"oracle_grad_step_{precision}")
+    f.argtypes = [ctypes.POINTER(OCyl), ctypes.c_int, ctypes.POINTER(ct), ctypes.POINTER(ct), ctypes.c_float]
+    oc = ocyl(m)
+    f(ctypes.byref(oc), K, _ptr(xi, ct), _ptr(Vb, ct), float(tau2))
+    return xi
+
+
+def div_step(m, K: int, xi, V, u, ci, lam, tau1, precision: str = "f64"):
+    """One primal step: returns (V_new, Vbar_new, max |dV|^2)."""
+    dt, ct = _real(precision)
+    xi = np.ascontiguousarray(xi, dtype=dt)
+    V = np.ascontiguousarray(V, dtype=dt).copy()
+    Vb = np.zeros_like(V)
+    u = np.ascontiguousarray(u, dtype=np.float32)
+    c = np.ascontiguousarray(np.asarray(ci, np.float32))
+    f = getattr(lib(), f"oracle_div_step_{precision}")
+    f.restype = ct
+    f.argtypes = [ctypes.POINTER(OCyl), ctypes.c_int, ctypes.POINTER(ct), ctypes.POINTER(ct), ctypes.POINTER(ct),
+                  ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), ctypes.c_float, ctypes.c_float]
+    oc = ocyl(m)
+    dq = f(ctypes.byref(oc), K, _ptr(xi, ct), _ptr(V, ct), _ptr(Vb, ct), _ptr(u, ctypes.c_float),
+           _ptr(c, ctypes.c_float), float(lam), float(tau1))
+    return V, Vb, float(dq)
+
+
+def energies(m, K: int, xi, V, u, ci, lam, precision: str = "f64") -> np.ndarray:
+    """(lagrangian, dual, gap) in FP64."""
+    dt, ct = _real(precision)
+    xi = np.ascontiguousarray(xi, dtype=dt)
+    V = np.ascontiguousarray(V, dtype=dt)
+    u = np.ascontiguousarray(u, dtype=np.float32)
+    c = np.ascontiguousarray(np.asarray(ci, np.float32))
+    out = np.zeros(3, np.float64)
+    f = getattr(lib(), f"oracle_energies_{precision}")
+    f.argtypes = [ctypes.POINTER(OCyl), ctypes.c_int, ctypes.POINTER(ct), ctypes.POINTER(ct),
+                  ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), ctypes.c_float,
+                  ctypes.POINTER(ctypes.c_double)]
+    oc = ocyl(m)
+    f(ctypes.byref(oc), K, _ptr(xi, ct), _ptr(V, ct), _ptr(u, ctypes.c_float), _ptr(c, ctypes.c_float), float(lam),
+      _ptr(out, ctypes.c_double))
+    return out

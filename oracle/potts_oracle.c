@@ -1,0 +1,528 @@
+/*
+ * CPU oracle for the multiphase Potts primal-dual solve (test infrastructure only).
+ *
+ * This file is the correctness checker of the project, not part of the product:
+ * only tests/, the smoke check and the CPU-baseline leg of bench.py load it.
+ * It restates, plainly and per voxel, the Chambolle-Cremers-Pock iteration of
+ * the reference solver:
+ *
+ *   init_v_kernel   potts-model/potts-min-partition.cpp:56-94
+ *   grad_kernel     potts-model/potts-min-partition.cpp:96-247   (dual step + Dykstra)
+ *   project_simplex potts-model/potts-min-partition.cpp:292-347
+ *   div_kernel      potts-model/potts-min-partition.cpp:349-488  (primal step)
+ *   update_kernel   potts-model/potts-min-partition.cpp:491-538  (argmax)
+ *   host driver     potts-model/potts-min-partition.cpp:540-679  (slabs + halo)
+ *   cylinder layout include/layout_cylinder.h:81-97 (offsets, row ranges)
+ *
+ * Parity unpinned: the reference ships no tests, golden vectors or fixtures for
+ * this path and cannot be built in this environment (it needs clang-CUDA,
+ * Boost.Hana, mdspan, range-v3 and CCCL 3 launch/buffer APIs), so this
+ * restatement is checked against mathematical properties (simplex KKT,
+ * projection feasibility, grad/div adjointness) rather than reference outputs.
+ *
+ * The file is compiled twice: REAL=double (the FP64 oracle) and REAL=float
+ * (an FP32 mode).  Where the reference's clang build would contract a multiply
+ * and an add into one fused multiply-add, this restatement writes FMA()
+ * explicitly, and it is compiled with -ffp-contract=off so that no other
+ * contraction happens.  In FP32 mode every operation is therefore an IEEE
+ * single-precision operation with a fixed order.
+ */
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifndef REAL
+#define REAL double
+#endif
+#ifndef SFX
+#define SFX f64
+#endif
+
+#define CAT2(a, b) a##_##b
+#define CAT(a, b) CAT2(a, b)
+#define NAME(x) CAT(x, SFX)
+
+#if defined(ORACLE_REAL_IS_FLOAT)
+#define FMA(a, b, c) fmaf((a), (b), (c))
+#define SQRT(x) sqrtf(x)
+#define FABS(x) fabsf(x)
+#define RMAX FLT_MAX
+#else
+#define FMA(a, b, c) fma((a), (b), (c))
+#define SQRT(x) sqrt(x)
+#define FABS(x) fabs(x)
+#define RMAX DBL_MAX
+#endif
+
+#define KMAX 6
+
+/* Host copy of layout_cylinder::mapping (include/layout_cylinder.h:30-112). */
+typedef struct {
+    uint32_t n_images, rows, cols;
+    uint32_t nstride, col_begin, col_end;
+    const uint32_t *start_row; /* cols entries   */
+    const uint32_t *base;      /* cols+1 entries */
+} ocyl;
+
+static inline int64_t row_begin(const ocyl *m, uint32_t col) { return m->start_row[col]; }
+static inline int64_t row_end(const ocyl *m, uint32_t col)
+{
+    return (int64_t)m->start_row[col] + (int64_t)(m->base[col + 1] - m->base[col]) / m->nstride;
+}
+/* layout_cylinder.h:81-84 */
+static inline int64_t offset(const ocyl *m, int64_t n, int64_t row, uint32_t col)
+{
+    return (int64_t)m->base[col] + (row - (int64_t)m->start_row[col]) * m->nstride + n;
+}
+static inline int row_in(const ocyl *m, uint32_t col, int64_t row)
+{
+    return row_begin(m, col) <= row && row < row_end(m, col);
+}
+
+/* std::max / cuda::std::max(a, b) as the reference uses it: (a < b) ? b : a */
+static inline REAL rmax(REAL a, REAL b) { return (a < b) ? b : a; }
+
+/* ---------------------------------------------------------------------------
+ * Projection onto the simplex, potts-min-partition.cpp:292-347.
+ * The reference sorts with sorting networks; any correct sort yields the same
+ * sorted values, so a plain insertion sort is used here.
+ * ------------------------------------------------------------------------- */
+void NAME(oracle_project_simplex)(REAL *q, int K)
+{
+    REAL u[KMAX];
+    for (int i = 0; i < K; ++i) u[i] = q[i];
+    for (int i = 1; i < K; ++i) {            /* descending */
+        REAL x = u[i];
+        int j = i - 1;
+        while (j >= 0 && u[j] < x) { u[j + 1] = u[j]; --j; }
+        u[j + 1] = x;
+    }
+    REAL sum = 0, rho_sum = 0;
+    int rho = 0;
+    for (int i = 0; i < K; ++i) {
+        sum += u[i];
+        REAL theta = (sum - (REAL)1) / (REAL)(i + 1);
+        if (u[i] > theta) { rho = i + 1; rho_sum = sum; }
+    }
+    REAL theta = (rho_sum - (REAL)1) / (REAL)rho;
+    for (int i = 0; i < K; ++i) q[i] = rmax(q[i] - theta, (REAL)0);
+}
+
+/* ---------------------------------------------------------------------------
+ * Dykstra projection onto K = {|q_i - q_j| <= 1, i < j},
+ * potts-min-partition.cpp:202-238.  q holds K vectors of 3 components,
+ * q[3*i + axis].  Returns the number of sweeps run.
+ * ------------------------------------------------------------------------- */
+int NAME(oracle_project_K)(REAL *q, int K)
+{
+    REAL P[KMAX * (KMAX - 1) / 2][3];
+    memset(P, 0, sizeof(P));
+    int sweep;
+    for (sweep = 0; sweep < 20; ++sweep) {
+        REAL max_d = -RMAX;
+        int p = 0; /* pair index in lexicographic (i1, i2) order, :209 */
+        for (int i1 = 0; i1 < K - 1; ++i1) {
+            for (int i2 = i1 + 1; i2 < K; ++i2, ++p) {
+                REAL qh[3], qhh[3], d[3];
+                for (int a = 0; a < 3; ++a) qh[a] = q[3 * i2 + a] - q[3 * i1 + a] + P[p][a];
+                REAL s = qh[0] * qh[0];
+                s = FMA(qh[1], qh[1], s);
+                s = FMA(qh[2], qh[2], s);
+                REAL l = SQRT(s);
+                for (int a = 0; a < 3; ++a) qhh[a] = (l > (REAL)1) ? ((l - (REAL)1) * qh[a]) / l : (REAL)0;
+                for (int a = 0; a < 3; ++a) d[a] = (REAL)0.5 * (qhh[a] - P[p][a]);
+                REAL dd = d[0] * d[0];
+                dd = FMA(d[1], d[1], dd);
+                dd = FMA(d[2], d[2], dd);
+                REAL dn = SQRT(dd);
+                max_d = rmax(dn, max_d);
+                for (int a = 0; a < 3; ++a) {
+                    q[3 * i1 + a] += d[a];
+                    q[3 * i2 + a] -= d[a];
+                    P[p][a] = qhh[a];
+                }
+            }
+        }
+        /* `1e-6 > max_δ` compares against the double literal 1e-6 (:235) */
+        if (1e-6 > (double)max_d) { ++sweep; break; }
+    }
+    return sweep;
+}
+
+/* ---------------------------------------------------------------------------
+ * Solver state for one slab [n_lo, n_hi): arrays are indexed by the input
+ * mapping (same offsets as u); only n in [n_lo, n_hi) is touched.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+    const ocyl *m;
+    int K;
+    int64_t span;
+    REAL *xi;  /* 3(K-1) planes of span */
+    REAL *V;   /* K-1 planes */
+    REAL *Vb;  /* K-1 planes */
+} ostate;
+
+/* init_v_kernel, potts-min-partition.cpp:56-94: V = V_bar = one-hot of the
+ * nearest label (strict <, first wins). */
+static void init_v(ostate *st, const float *u, const REAL *c, int n_lo, int n_hi)
+{
+    const ocyl *m = st->m;
+    const int K = st->K;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t col = m->col_begin; col < m->col_end; ++col) {
+        for (int64_t row = row_begin(m, col); row < row_end(m, col); ++row) {
+            for (int64_t n = n_lo; n < n_hi; ++n) {
+                int64_t o = offset(m, n, row, col);
+                REAL v = (REAL)u[o];
+                REAL best = RMAX;
+                int cluster = 0;
+                for (int k = 0; k < K; ++k) {
+                    REAL d = FABS(c[k] - v);
+                    if (d < best) { best = d; cluster = k; }
+                }
+                for (int i = 0; i < K - 1; ++i) {
+                    REAL x = (i == cluster) ? (REAL)1 : (REAL)0;
+                    st->V[i * st->span + o] = x;
+                    st->Vb[i * st->span + o] = x;
+                }
+            }
+        }
+    }
+}
+
+/* grad_kernel, potts-min-partition.cpp:96-247 (returns nothing; Xi updated in place). */
+static void grad_step(ostate *st, REAL tau2, int n_lo, int n_hi, int *sweep_hist)
+{
+    const ocyl *m = st->m;
+    const int K = st->K;
+    const int64_t S = st->span;
+    int64_t hist[21];
+    memset(hist, 0, sizeof(hist));
+#pragma omp parallel
+    {
+        int64_t lh[21];
+        memset(lh, 0, sizeof(lh));
+#pragma omp for schedule(dynamic, 4)
+        for (int64_t col = m->col_begin; col < m->col_end; ++col) {
+            for (int64_t row = row_begin(m, col); row < row_end(m, col); ++row) {
+                const int has_r = row_end(m, col) - 1 > row;
+                const int has_c = (int64_t)m->col_end - 1 > col && row_in(m, (uint32_t)(col + 1), row);
+                for (int64_t n = n_lo; n < n_hi; ++n) {
+                    const int has_n = n_hi - 1 > n;
+                    const int64_t o = offset(m, n, row, col);
+                    const int64_t on = has_n ? offset(m, n + 1, row, col) : 0;
+                    const int64_t orr = has_r ? offset(m, n, row + 1, col) : 0;
+                    const int64_t oc = has_c ? offset(m, n, row, (uint32_t)(col + 1)) : 0;
+                    REAL q[3 * KMAX];
+                    REAL vk = 1, vkn = 1, vkr = 1, vkc = 1;
+                    REAL xk[3] = {0, 0, 0};
+                    for (int i = 0; i < K; ++i) {
+                        REAL vi, g[3] = {0, 0, 0}, xi_i[3];
+                        if (i < K - 1) { vi = st->Vb[i * S + o]; vk -= vi; } else vi = vk;
+                        if (has_n) {
+                            REAL w;
+                            if (i < K - 1) { w = st->Vb[i * S + on]; vkn -= w; } else w = vkn;
+                            g[0] = w - vi;
+                        }
+                        if (has_r) {
+                            REAL w;
+                            if (i < K - 1) { w = st->Vb[i * S + orr]; vkr -= w; } else w = vkr;
+                            g[1] = w - vi;
+                        }
+                        if (has_c) {
+                            REAL w;
+                            if (i < K - 1) { w = st->Vb[i * S + oc]; vkc -= w; } else w = vkc;
+                            g[2] = w - vi;
+                        }
+                        if (i < K - 1) {
+                            for (int a = 0; a < 3; ++a) { xi_i[a] = st->xi[(3 * i + a) * S + o]; xk[a] -= xi_i[a]; }
+                        } else {
+                            for (int a = 0; a < 3; ++a) xi_i[a] = xk[a];
+                        }
+                        /* q *= tau2; q += xi  (contracted to one FMA) */
+                        for (int a = 0; a < 3; ++a) q[3 * i + a] = FMA(g[a], tau2, xi_i[a]);
+                    }
+                    int sw = NAME(oracle_project_K)(q, K);
+                    lh[sw] += 1;
+                    for (int i = 0; i < K - 1; ++i)
+                        for (int a = 0; a < 3; ++a) st->xi[(3 * i + a) * S + o] = q[3 * i + a];
+                }
+            }
+        }
+#pragma omp critical
+        for (int i = 0; i < 21; ++i) hist[i] += lh[i];
+    }
+    if (sweep_hist)
+        for (int i = 0; i < 21; ++i) sweep_hist[i] += (int)hist[i];
+}
+
+/* div_kernel, potts-min-partition.cpp:349-488.  Returns max_x |V^{k+1}-V^k|^2. */
+static REAL div_step(ostate *st, const float *u, const REAL *c, REAL lam, REAL tau1, int n_lo, int n_hi)
+{
+    const ocyl *m = st->m;
+    const int K = st->K;
+    const int64_t S = st->span;
+    REAL dq_max = 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(max : dq_max)
+    for (int64_t col = m->col_begin; col < m->col_end; ++col) {
+        for (int64_t row = row_begin(m, col); row < row_end(m, col); ++row) {
+            const int has_r = row_end(m, col) - 1 > row;
+            const int prv_r = row_begin(m, col) < row;
+            const int has_c = (int64_t)m->col_end - 1 > col && row_in(m, (uint32_t)(col + 1), row);
+            const int prv_c = (int64_t)m->col_begin < col && row_in(m, (uint32_t)(col - 1), row);
+            for (int64_t n = n_lo; n < n_hi; ++n) {
+                const int has_n = n_hi - 1 > n;
+                const int prv_n = n_lo < n;
+                const int64_t o = offset(m, n, row, col);
+                const int64_t pn = prv_n ? offset(m, n - 1, row, col) : 0;
+                const int64_t pr = prv_r ? offset(m, n, row - 1, col) : 0;
+                const int64_t pc = prv_c ? offset(m, n, row, (uint32_t)(col - 1)) : 0;
+                const REAL g = (REAL)u[o];
+                REAL q[KMAX], v[KMAX];
+                REAL vk = 1;
+                REAL xk[3] = {0, 0, 0};
+                REAL xkn = 0, xkr = 0, xkc = 0;
+                for (int i = 0; i < K; ++i) {
+                    REAL xi_i[3], div = 0, w;
+                    if (i < K - 1) {
+                        for (int a = 0; a < 3; ++a) { xi_i[a] = st->xi[(3 * i + a) * S + o]; xk[a] -= xi_i[a]; }
+                    } else {
+                        for (int a = 0; a < 3; ++a) xi_i[a] = xk[a];
+                    }
+                    if (prv_n) {
+                        if (i < K - 1) { w = st->xi[(3 * i + 0) * S + pn]; xkn -= w; } else w = xkn;
+                        div -= w;
+                    }
+                    if (has_n) div += xi_i[0];
+                    if (prv_r) {
+                        if (i < K - 1) { w = st->xi[(3 * i + 1) * S + pr]; xkr -= w; } else w = xkr;
+                        div -= w;
+                    }
+                    if (has_r) div += xi_i[1];
+                    if (prv_c) {
+                        if (i < K - 1) { w = st->xi[(3 * i + 2) * S + pc]; xkc -= w; } else w = xkc;
+                        div -= w;
+                    }
+                    if (has_c) div += xi_i[2];
+                    REAL vi;
+                    if (i < K - 1) { vi = st->V[i * S + o]; vk -= vi; } else vi = vk;
+                    v[i] = vi;
+                    /* q = v + tau1 * (div - lam * sqr(g - c_i)) */
+                    REAL dlt = g - c[i];
+                    REAL d2 = dlt * dlt;
+                    REAL wv = FMA(-lam, d2, div);
+                    q[i] = FMA(tau1, wv, vi);
+                }
+                NAME(oracle_project_simplex)(q, K);
+                REAL dq = 0;
+                for (int i = 0; i < K; ++i) {
+                    REAL e = q[i] - v[i];
+                    dq = (i == 0) ? e * e : FMA(e, e, dq);
+                }
+                for (int i = 0; i < K - 1; ++i) {
+                    st->Vb[i * S + o] = (REAL)2 * q[i] - v[i];
+                    st->V[i * S + o] = q[i];
+                }
+                if (dq > dq_max) dq_max = dq;
+            }
+        }
+    }
+    return dq_max;
+}
+
+/* update_kernel, potts-min-partition.cpp:491-538: argmax (strict >, v starts at 0). */
+static void update(const ostate *st, const float *c, int n_lo, int n_hi, float *res, uint8_t *labels)
+{
+    const ocyl *m = st->m;
+    const int K = st->K;
+    const int64_t S = st->span;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t col = m->col_begin; col < m->col_end; ++col) {
+        for (int64_t row = row_begin(m, col); row < row_end(m, col); ++row) {
+            for (int64_t n = n_lo; n < n_hi; ++n) {
+                const int64_t o = offset(m, n, row, col);
+                REAL best = 0, vk = 1;
+                int lab = 0;
+                for (int i = 0; i < K; ++i) {
+                    REAL vi;
+                    if (i < K - 1) { vi = st->V[i * S + o]; vk -= vi; } else vi = vk;
+                    if (vi > best) { best = vi; lab = i; }
+                }
+                if (res) res[o] = c[lab];
+                if (labels) labels[o] = (uint8_t)lab;
+            }
+        }
+    }
+}
+
+/* ---------------------------------------------------------------------------
+ * FP64 energies of a state (V, Xi) over the voxels of [n_lo, n_hi):
+ *   lagrangian = sum_x sum_i V_i (G_i - div Xi_i)
+ *   dual       = sum_x min_i (G_i - div Xi_i)
+ *   gap        = lagrangian - dual  (>= 0 for V on the simplex)
+ * with G_i = lam (u - c_i)^2.  The reference computes no energy; this is the
+ * diagnostic reported every few iterations.  Sums are per column, then added
+ * in column order.
+ * ------------------------------------------------------------------------- */
+static void energies(const ostate *st, const float *u, const REAL *c, REAL lam, int n_lo, int n_hi, double out[3])
+{
+    const ocyl *m = st->m;
+    const int K = st->K;
+    const int64_t S = st->span;
+    const int64_t ncol = (int64_t)m->col_end - m->col_begin;
+    double *part = (double *)calloc((size_t)(2 * (ncol > 0 ? ncol : 1)), sizeof(double));
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t col = m->col_begin; col < m->col_end; ++col) {
+        double sl = 0, sd = 0;
+        for (int64_t row = row_begin(m, col); row < row_end(m, col); ++row) {
+            const int has_r = row_end(m, col) - 1 > row;
+            const int prv_r = row_begin(m, col) < row;
+            const int has_c = (int64_t)m->col_end - 1 > col && row_in(m, (uint32_t)(col + 1), row);
+            const int prv_c = (int64_t)m->col_begin < col && row_in(m, (uint32_t)(col - 1), row);
+            for (int64_t n = n_lo; n < n_hi; ++n) {
+                const int has_n = n_hi - 1 > n;
+                const int prv_n = n_lo < n;
+                const int64_t o = offset(m, n, row, col);
+                double dv[KMAX + 1], xk[3] = {0, 0, 0}, xkn = 0, xkr = 0, xkc = 0, vk = 1, lag = 0, mn = DBL_MAX;
+                for (int i = 0; i < K; ++i) {
+                    double x[3], w, div = 0, vi;
+                    if (i < K - 1) {
+                        for (int a = 0; a < 3; ++a) { x[a] = (double)st->xi[(3 * i + a) * S + o]; xk[a] -= x[a]; }
+                    } else {
+                        for (int a = 0; a < 3; ++a) x[a] = xk[a];
+                    }
+                    if (prv_n) {
+                        if (i < K - 1) { w = (double)st->xi[(3 * i) * S + offset(m, n - 1, row, col)]; xkn -= w; } else w = xkn;
+                        div -= w;
+                    }
+                    if (has_n) div += x[0];
+                    if (prv_r) {
+                        if (i < K - 1) { w = (double)st->xi[(3 * i + 1) * S + offset(m, n, row - 1, col)]; xkr -= w; } else w = xkr;
+                        div -= w;
+                    }
+                    if (has_r) div += x[1];
+                    if (prv_c) {
+                        if (i < K - 1) { w = (double)st->xi[(3 * i + 2) * S + offset(m, n, row, (uint32_t)(col - 1))]; xkc -= w; } else w = xkc;
+                        div -= w;
+                    }
+                    if (has_c) div += x[2];
+                    if (i < K - 1) { vi = (double)st->V[i * S + o]; vk -= vi; } else vi = vk;
+                    double dl = (double)u[o] - (double)c[i];
+                    double e = (double)lam * dl * dl - div;
+                    dv[i] = e;
+                    lag += vi * e;
+                    if (e < mn) mn = e;
+                }
+                sl += lag;
+                sd += mn;
+            }
+        }
+        part[2 * (col - m->col_begin)] = sl;
+        part[2 * (col - m->col_begin) + 1] = sd;
+    }
+    double L = 0, D = 0;
+    for (int64_t i = 0; i < ncol; ++i) { L += part[2 * i]; D += part[2 * i + 1]; }
+    free(part);
+    out[0] = L;
+    out[1] = D;
+    out[2] = L - D;
+}
+
+/* ---------------------------------------------------------------------------
+ * Whole solve, potts-min-partition.cpp:540-679.
+ *
+ * slab_w <= 0 or >= n_images: one slab over the whole volume.  Otherwise the
+ * reference's planner: halo = iters, res_w = slab_w - 2*halo, slabs start at
+ * i*res_w, the result of each slab is written without its halo (:627-675).
+ *
+ * Outputs (each optional): res = c[argmax] (span floats, input mapping),
+ * labels = argmax index (span bytes), V_out / Xi_out = final state
+ * ((K-1)*span and 3(K-1)*span REALs; single-slab runs only), dq_trace = the
+ * squared max |dV|^2 of every iteration of the last slab, energy_trace =
+ * (lagrangian, dual, gap) after iterations it with (it+1) % gap_every == 0,
+ * sweep_hist = histogram of Dykstra sweep counts (21 ints).
+ *
+ * Returns 0, or -1 on bad arguments / allocation failure / planner failure.
+ * ------------------------------------------------------------------------- */
+int NAME(oracle_solve)(const ocyl *m, const float *u, int K, const float *c_f, float lam_f, float tau1_f,
+                       float tau2_f, int iters, int slab_w, float *res, uint8_t *labels, REAL *V_out, REAL *Xi_out,
+                       float *dq_trace, int gap_every, double *energy_trace, int *sweep_hist)
+{
+    if (!m || !u || K < 2 || K > KMAX || iters < 0) return -1;
+    const int n = (int)m->n_images;
+    const int64_t span = (int64_t)m->base[m->cols];
+    REAL c[KMAX];
+    for (int i = 0; i < K; ++i) c[i] = (REAL)c_f[i];
+    const REAL lam = (REAL)lam_f, tau1 = (REAL)tau1_f, tau2 = (REAL)tau2_f;
+
+    ostate st;
+    st.m = m;
+    st.K = K;
+    st.span = span;
+    const size_t ns = (size_t)(span > 0 ? span : 1);
+    st.xi = (REAL *)calloc(ns * 3 * (size_t)(K - 1), sizeof(REAL));
+    st.V = (REAL *)calloc(ns * (size_t)(K - 1), sizeof(REAL));
+    st.Vb = (REAL *)calloc(ns * (size_t)(K - 1), sizeof(REAL));
+    if (!st.xi || !st.V || !st.Vb) { free(st.xi); free(st.V); free(st.Vb); return -1; }
+
+    int halo = iters, sw = slab_w, n_slabs = 1, res_w = n;
+    if (sw <= 0 || sw >= n) {
+        sw = n;
+    } else {
+        res_w = sw - 2 * halo;
+        if (res_w <= 0) { free(st.xi); free(st.V); free(st.Vb); return -1; }
+        n_slabs = 1 + (n - sw + res_w - 1) / res_w;
+    }
+    for (int s = 0; s < n_slabs; ++s) {
+        const int s0 = s * res_w;
+        const int s1 = (s0 + sw < n) ? s0 + sw : n;
+        init_v(&st, u, c, s0, s1);
+        memset(st.xi, 0, ns * 3 * (size_t)(K - 1) * sizeof(REAL));
+        for (int it = 0; it < iters; ++it) {
+            grad_step(&st, tau2, s0, s1, sweep_hist);
+            REAL dq = div_step(&st, u, c, lam, tau1, s0, s1);
+            if (dq_trace) dq_trace[it] = (float)dq;
+            if (energy_trace && gap_every > 0 && (it + 1) % gap_every == 0)
+                energies(&st, u, c, lam, s0, s1, energy_trace + 3 * ((it + 1) / gap_every - 1));
+        }
+        const int r0 = (s0 == 0) ? s0 : s0 + halo;
+        const int r1 = (s1 == n) ? s1 : s1 - halo;
+        update(&st, c_f, r0, r1, res, labels);
+    }
+    if (n_slabs == 1) {
+        if (V_out) memcpy(V_out, st.V, ns * (size_t)(K - 1) * sizeof(REAL));
+        if (Xi_out) memcpy(Xi_out, st.xi, ns * 3 * (size_t)(K - 1) * sizeof(REAL));
+    }
+    free(st.xi);
+    free(st.V);
+    free(st.Vb);
+    return 0;
+}
+
+/* Single steps on caller-owned state (whole volume as one slab), for tests of
+ * the adjoint identity and of individual kernels. */
+void NAME(oracle_grad_step)(const ocyl *m, int K, REAL *xi, const REAL *Vb, float tau2)
+{
+    ostate st = {m, K, (int64_t)m->base[m->cols], xi, NULL, (REAL *)Vb};
+    grad_step(&st, (REAL)tau2, 0, (int)m->n_images, NULL);
+}
+
+REAL NAME(oracle_div_step)(const ocyl *m, int K, const REAL *xi, REAL *V, REAL *Vb, const float *u, const float *c_f,
+                           float lam, float tau1)
+{
+    REAL c[KMAX];
+    for (int i = 0; i < K; ++i) c[i] = (REAL)c_f[i];
+    ostate st = {m, K, (int64_t)m->base[m->cols], (REAL *)xi, V, Vb};
+    return div_step(&st, u, c, (REAL)lam, (REAL)tau1, 0, (int)m->n_images);
+}
+
+void NAME(oracle_energies)(const ocyl *m, int K, const REAL *xi, const REAL *V, const float *u, const float *c_f,
+                           float lam, double out[3])
+{
+    REAL c[KMAX];
+    for (int i = 0; i < K; ++i) c[i] = (REAL)c_f[i];
+    ostate st = {m, K, (int64_t)m->base[m->cols], (REAL *)xi, (REAL *)V, NULL};
+    energies(&st, u, c, (REAL)lam, 0, (int)m->n_images, out);
+}

@@ -1,0 +1,121 @@
+"""ctypes binding of the native library ``libpotts_b200.so`` (include/potts_b200.h).
+
+The library is built in-tree by ``segmentctscans_b200.build``.  Loading fails
+loudly when it is missing: there is no CPU fallback for the solver.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+from .build import LIB_PATH
+
+POTTS_OK, POTTS_EINVAL, POTTS_ENOMEM, POTTS_ECUDA, POTTS_ETIMEOUT, POTTS_ENODEV = range(6)
+VARIANT_FUSED, VARIANT_PLAIN = 0, 1
+STORE_F32 = 0
+MAX_PHASES = 6
+
+
+class PottsMapping(ctypes.Structure):
+    _fields_ = [
+        ("n_images", ctypes.c_uint32), ("rows", ctypes.c_uint32), ("cols", ctypes.c_uint32),
+        ("nstride", ctypes.c_uint32), ("col_begin", ctypes.c_uint32), ("col_end", ctypes.c_uint32),
+        ("start_row", ctypes.POINTER(ctypes.c_uint32)), ("base", ctypes.POINTER(ctypes.c_uint32)),
+    ]
+
+
+class PottsOptions(ctypes.Structure):
+    _fields_ = [
+        ("variant", ctypes.c_int), ("storage", ctypes.c_int), ("gap_every", ctypes.c_int),
+        ("slab_w", ctypes.c_int), ("track_dq", ctypes.c_int), ("sync_monitor", ctypes.c_int),
+    ]
+
+
+class PottsStats(ctypes.Structure):
+    _fields_ = [
+        ("n_slabs", ctypes.c_int), ("slab_w", ctypes.c_int), ("iters", ctypes.c_int),
+        ("dq_last", ctypes.c_float), ("solve_ms", ctypes.c_double), ("loop_ms", ctypes.c_double),
+        ("loop_launches", ctypes.c_int), ("total_launches", ctypes.c_int), ("state_bytes", ctypes.c_uint64),
+        ("dq_trace", ctypes.POINTER(ctypes.c_float)), ("energy_trace", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_F = ctypes.c_float
+_U32 = ctypes.c_uint32
+_U64 = ctypes.c_uint64
+_FP = ctypes.POINTER(ctypes.c_float)
+_MP = ctypes.POINTER(PottsMapping)
+_OP = ctypes.POINTER(PottsOptions)
+_SP = ctypes.POINTER(PottsStats)
+
+# name -> (restype, argtypes); every entry point declared in include/potts_b200.h
+SIGNATURES = {
+    "potts_default_options": (None, [_OP]),
+    "potts_status_string": (ctypes.c_char_p, [_I]),
+    "potts_last_error": (ctypes.c_char_p, []),
+    "potts_context_create": (_I, [_I, ctypes.POINTER(_P)]),
+    "potts_context_create_on_stream": (_I, [_I, _P, ctypes.POINTER(_P)]),
+    "potts_context_destroy": (None, [_P]),
+    "potts_context_synchronize": (_I, [_P]),
+    "potts_device_memory": (_I, [_P, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]),
+    "potts_field_create": (_I, [_P, _MP, ctypes.POINTER(_P)]),
+    "potts_field_upload": (_I, [_P, _MP, _FP, ctypes.POINTER(_P)]),
+    "potts_field_download": (_I, [_P, _P, _FP, _U64]),
+    "potts_field_data": (_P, [_P]),
+    "potts_field_span": (_U64, [_P]),
+    "potts_field_destroy": (None, [_P]),
+    "potts_min_partition": (_I, [_P, _P, _MP, _I, _FP, _F, _F, _F, _I, _OP, ctypes.POINTER(_P), _SP]),
+    "potts_solve_device": (_I, [_P, _MP, _P, _I, _FP, _F, _F, _F, _I, _OP, _P, _P, _P, _P, _SP]),
+    "potts_solve_host": (_I, [_P, _MP, _P, _I, _FP, _F, _F, _F, _I, _OP, _P, _P, _SP]),
+    "potts_cylinder_mapping": (_U64, [_U32, _U32, ctypes.c_double, ctypes.c_double, ctypes.c_double, _U32,
+                                      ctypes.POINTER(_U32), ctypes.POINTER(_U32), ctypes.POINTER(_U32),
+                                      ctypes.POINTER(_U32)]),
+    "potts_get_stride": (_U32, [_U32]),
+}
+
+_lib = None
+
+
+class PottsError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+def lib_path() -> Path:
+    return LIB_PATH
+
+
+def host_lib() -> ctypes.CDLL:
+    """Load the library (no CUDA call is made by loading it)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(
+                f"native library {LIB_PATH} is missing; build it with `python -m segmentctscans_b200.build`")
+        lib = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != POTTS_OK:
+        lib = host_lib()
+        msg = lib.potts_last_error().decode(errors="replace")
+        raise PottsError(status, f"{lib.potts_status_string(status).decode()}: {msg}")
+
+
+def default_options(**kw) -> PottsOptions:
+    o = PottsOptions()
+    host_lib().potts_default_options(ctypes.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise TypeError(f"unknown option {k}")
+        setattr(o, k, int(v))
+    return o

@@ -1,0 +1,800 @@
+// C-ABI implementation of the B200 Potts solver: device context, fields,
+// slab planner and the iteration driver (potts-model/potts-min-partition.cpp:540-679).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/potts_b200.h"
+#include "geometry.cuh"
+#include "kernels_fused.cuh"
+#include "kernels_plain.cuh"
+#include "voxel.cuh"
+
+using potts::DykstraThresholds;
+using potts::Geometry;
+using potts::PhaseParams;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+#define POTTS_CUDA(call)                                                                               \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                         \
+            return fail(e_ == cudaErrorMemoryAllocation ? POTTS_ENOMEM : POTTS_ECUDA,                  \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                           \
+    } while (0)
+
+#define POTTS_TRY(expr)              \
+    do {                             \
+        int s_ = (expr);             \
+        if (s_ != POTTS_OK) return s_; \
+    } while (0)
+
+inline float bits_to_float(uint32_t b)
+{
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f;
+}
+
+// Bisection over the bit patterns of non-negative floats (which order like
+// the floats) for the two Dykstra thresholds; host sqrtf is IEEE like the
+// device's __fsqrt_rn.
+DykstraThresholds compute_thresholds()
+{
+    DykstraThresholds t;
+    {   // largest s with sqrtf(s) <= 1
+        uint32_t lo = 0, hi = 0x7f800000u;
+        while (hi - lo > 1) {
+            uint32_t mid = lo + (hi - lo) / 2;
+            if (std::sqrt(bits_to_float(mid)) > 1.0f) hi = mid; else lo = mid;
+        }
+        t.len_gt_one = bits_to_float(lo);
+    }
+    {   // smallest m with (double)sqrtf(m) >= 1e-6
+        uint32_t lo = 0, hi = 0x7f800000u;
+        while (hi - lo > 1) {
+            uint32_t mid = lo + (hi - lo) / 2;
+            if ((double)std::sqrt(bits_to_float(mid)) < 1e-6) lo = mid; else hi = mid;
+        }
+        t.exit_below = bits_to_float(hi);
+    }
+    return t;
+}
+
+uint32_t get_stride(uint32_t n) { return ((n + 31u) / 32u) * 32u; }
+uint32_t prev_stride(uint64_t n) { return (uint32_t)std::min<uint64_t>((n / 32u) * 32u, 0x7fffffe0u); }
+
+// Validated host copy of a mapping with its line table.
+struct MappingCopy {
+    potts_mapping m{};
+    std::vector<uint32_t> start_row, base;
+    std::vector<int4> lines;
+    int64_t n_lines = 0;
+    uint64_t span = 0;
+
+    void rebind()
+    {
+        m.start_row = start_row.data();
+        m.base = base.data();
+    }
+};
+
+int64_t row_end_of(const potts_mapping &m, uint32_t col)
+{
+    return (int64_t)m.start_row[col] + (int64_t)(m.base[col + 1] - m.base[col]) / m.nstride;
+}
+
+bool row_in(const potts_mapping &m, uint32_t col, int64_t row)
+{
+    return (int64_t)m.start_row[col] <= row && row < row_end_of(m, col);
+}
+
+int validate_mapping(const potts_mapping *map)
+{
+    if (!map || !map->start_row || !map->base) return fail(POTTS_EINVAL, "mapping or its tables is NULL");
+    const potts_mapping &m = *map;
+    if (m.nstride == 0 || m.nstride % 4 != 0 || m.nstride < m.n_images)
+        return fail(POTTS_EINVAL, "nstride must be a multiple of 4 and >= n_images");
+    if (m.n_images == 0) return fail(POTTS_EINVAL, "n_images is 0");
+    if (m.col_end > m.cols || (m.col_begin > m.col_end && m.col_end != 0))
+        return fail(POTTS_EINVAL, "col_begin/col_end out of range");
+    if (m.rows > 65535 || m.cols > 65535) return fail(POTTS_EINVAL, "rows and cols are limited to 65535");
+    for (uint32_t c = 0; c < m.cols; ++c) {
+        if (m.base[c + 1] < m.base[c] || m.base[c] % m.nstride != 0 || (m.base[c + 1] - m.base[c]) % m.nstride != 0)
+            return fail(POTTS_EINVAL, "base[] must be non-decreasing multiples of nstride");
+        const uint32_t cnt = (m.base[c + 1] - m.base[c]) / m.nstride;
+        if (cnt > 0 && ((uint64_t)m.start_row[c] + cnt > m.rows))
+            return fail(POTTS_EINVAL, "a column's rows exceed the row extent");
+        if (cnt > 0 && (c < m.col_begin || c >= m.col_end))
+            return fail(POTTS_EINVAL, "a column outside [col_begin, col_end) holds rows");
+    }
+    if (m.base[0] != 0) return fail(POTTS_EINVAL, "base[0] must be 0");
+    return POTTS_OK;
+}
+
+void build_lines(MappingCopy &mc)
+{
+    const potts_mapping &m = mc.m;
+    mc.span = m.base[m.cols];
+    mc.n_lines = (int64_t)(mc.span / m.nstride);
+    mc.lines.assign((size_t)mc.n_lines, make_int4(-1, -1, 0, 0));
+    for (uint32_t col = m.col_begin; col < m.col_end; ++col) {
+        const int64_t rb = m.start_row[col], re = row_end_of(m, col);
+        const int64_t first = m.base[col] / m.nstride;
+        for (int64_t row = rb; row < re; ++row) {
+            int4 li;
+            li.x = (col + 1 < m.col_end && row_in(m, col + 1, row))
+                       ? (int32_t)(m.base[col + 1] / m.nstride + (row - m.start_row[col + 1]))
+                       : -1;
+            li.y = (col > m.col_begin && row_in(m, col - 1, row))
+                       ? (int32_t)(m.base[col - 1] / m.nstride + (row - m.start_row[col - 1]))
+                       : -1;
+            li.z = (int32_t)((row + 1 < re ? potts::kHasNextRow : 0u) | (row > rb ? potts::kHasPrevRow : 0u));
+            li.w = (int32_t)((col << 16) | (uint32_t)row);
+            mc.lines[(size_t)(first + row - rb)] = li;
+        }
+    }
+}
+
+int copy_mapping(const potts_mapping *map, MappingCopy &mc)
+{
+    POTTS_TRY(validate_mapping(map));
+    mc.m = *map;
+    mc.start_row.assign(map->start_row, map->start_row + map->cols);
+    mc.base.assign(map->base, map->base + map->cols + 1);
+    mc.rebind();
+    build_lines(mc);
+    return POTTS_OK;
+}
+
+bool same_mapping(const MappingCopy &a, const potts_mapping &b)
+{
+    if (a.m.n_images != b.n_images || a.m.rows != b.rows || a.m.cols != b.cols || a.m.nstride != b.nstride ||
+        a.m.col_begin != b.col_begin || a.m.col_end != b.col_end)
+        return false;
+    return std::memcmp(a.start_row.data(), b.start_row, sizeof(uint32_t) * b.cols) == 0 &&
+           std::memcmp(a.base.data(), b.base, sizeof(uint32_t) * (b.cols + 1)) == 0;
+}
+
+// Grow-only device buffer owned by a context.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct potts_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    DykstraThresholds thr{};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    MappingCopy mapping;  // last mapping whose line table is on the device
+    bool mapping_valid = false;
+    DevBuf lines, state, dq, energy, partial, host_u, host_res, host_labels;
+    float *pinned_dq = nullptr;
+    // Event pairs around runs of consecutive iteration launches (energy
+    // evaluations and slab set-up fall outside them), and launch counters.
+    std::vector<cudaEvent_t> seg_ev;
+    int seg_used = 0;
+    bool seg_open = false;
+    int loop_launches = 0, total_launches = 0;
+};
+
+struct potts_field {
+    potts_context *ctx = nullptr;
+    float *d = nullptr;
+    MappingCopy mapping;
+};
+
+namespace {
+
+int seg_begin(potts_context *ctx)
+{
+    if (ctx->seg_open) return POTTS_OK;
+    if ((int)ctx->seg_ev.size() < 2 * (ctx->seg_used + 1)) {
+        for (int i = 0; i < 2; ++i) {
+            cudaEvent_t e;
+            POTTS_CUDA(cudaEventCreate(&e));
+            ctx->seg_ev.push_back(e);
+        }
+    }
+    POTTS_CUDA(cudaEventRecord(ctx->seg_ev[2 * ctx->seg_used], ctx->stream));
+    ctx->seg_open = true;
+    return POTTS_OK;
+}
+
+int seg_end(potts_context *ctx)
+{
+    if (!ctx->seg_open) return POTTS_OK;
+    POTTS_CUDA(cudaEventRecord(ctx->seg_ev[2 * ctx->seg_used + 1], ctx->stream));
+    ctx->seg_open = false;
+    ctx->seg_used += 1;
+    return POTTS_OK;
+}
+
+int seg_total_ms(potts_context *ctx, double *ms)
+{
+    *ms = 0.0;
+    for (int i = 0; i < ctx->seg_used; ++i) {
+        float t = 0.0f;
+        POTTS_CUDA(cudaEventElapsedTime(&t, ctx->seg_ev[2 * i], ctx->seg_ev[2 * i + 1]));
+        *ms += t;
+    }
+    return POTTS_OK;
+}
+
+int ensure(potts_context *ctx, DevBuf &b, size_t bytes)
+{
+    if (b.bytes >= bytes && b.p) return POTTS_OK;
+    if (b.p) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(b.p);
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+    if (bytes == 0) return POTTS_OK;
+    POTTS_CUDA(cudaMalloc(&b.p, bytes));
+    b.bytes = bytes;
+    return POTTS_OK;
+}
+
+size_t cached_bytes(const potts_context *ctx)
+{
+    return ctx->state.bytes + ctx->partial.bytes + ctx->host_u.bytes + ctx->host_res.bytes + ctx->host_labels.bytes;
+}
+
+int upload_lines(potts_context *ctx, const potts_mapping *map)
+{
+    if (ctx->mapping_valid && same_mapping(ctx->mapping, *map)) return POTTS_OK;
+    ctx->mapping_valid = false;
+    POTTS_TRY(copy_mapping(map, ctx->mapping));
+    const size_t bytes = sizeof(int4) * (size_t)std::max<int64_t>(ctx->mapping.n_lines, 1);
+    POTTS_TRY(ensure(ctx, ctx->lines, bytes));
+    if (ctx->mapping.n_lines > 0)
+        POTTS_CUDA(cudaMemcpyAsync(ctx->lines.p, ctx->mapping.lines.data(), sizeof(int4) * ctx->mapping.n_lines,
+                                   cudaMemcpyHostToDevice, ctx->stream));
+    POTTS_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->mapping_valid = true;
+    return POTTS_OK;
+}
+
+// Where the state of one slab lives.
+struct SlabState {
+    float *xi[2];  // 3(K-1) planes each (ping-pong for the fused form)
+    float *v[2];   // K-1 planes each (v[1] is Vbar in the split form)
+};
+
+int state_planes(int K, int variant)
+{
+    return variant == POTTS_VARIANT_PLAIN ? 5 * (K - 1) : 8 * (K - 1);
+}
+
+struct Outputs {
+    float *res;
+    uint8_t *labels;
+    float *V;
+    float *Xi;
+};
+
+inline unsigned plain_blocks(const Geometry &g, int n_begin, int n_end)
+{
+    const int chunks = (n_end - n_begin + potts::kPlainThreads - 1) / potts::kPlainThreads;
+    return (unsigned)(g.n_lines * chunks);
+}
+
+template <int K>
+int run_energy(potts_context *ctx, const Geometry &g, const float *xi, const float *V, const float *d_u,
+               const PhaseParams<K> &pp, double *out)
+{
+    POTTS_TRY(seg_end(ctx));
+    const unsigned nb = plain_blocks(g, 0, g.ns);
+    ctx->total_launches += 2;
+    potts::energy_kernel<K><<<nb, potts::kPlainThreads, 0, ctx->stream>>>(g, xi, V, d_u, pp,
+                                                                          (double2 *)ctx->partial.p);
+    potts::energy_finish<<<1, 1024, 0, ctx->stream>>>((const double2 *)ctx->partial.p, (int64_t)nb, out);
+    POTTS_CUDA(cudaGetLastError());
+    return POTTS_OK;
+}
+
+template <int K>
+int monitor_sync(potts_context *ctx, int it)
+{
+    POTTS_CUDA(cudaMemcpyAsync(ctx->pinned_dq, (float *)ctx->dq.p + it, sizeof(float), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+    POTTS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return POTTS_OK;
+}
+
+// One slab: init, iters iterations, argmax of [res_begin, res_end).
+template <int K>
+int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const PhaseParams<K> &pp, float tau2,
+             int iters, const potts_options &o, const SlabState &st, int res_begin, int res_end, const Outputs &out,
+             int64_t plane_out)
+{
+    const unsigned nb = plain_blocks(g, 0, g.ns);
+    const size_t xi_bytes = sizeof(float) * 3 * (K - 1) * (size_t)g.plane_w;
+    float *dq = o.track_dq ? (float *)ctx->dq.p : nullptr;
+    double *energy = (double *)ctx->energy.p;
+    const int ge = o.gap_every;
+    cudaStream_t s = ctx->stream;
+    if (dq && iters > 0) POTTS_CUDA(cudaMemsetAsync(dq, 0, sizeof(float) * iters, s));
+
+    int cur = 0;
+    if (o.variant == POTTS_VARIANT_PLAIN) {
+        float *xi = st.xi[0], *V = st.v[0], *Vb = st.v[1];
+        potts::init_kernel<K><<<nb, potts::kPlainThreads, 0, s>>>(g, d_u, V, Vb, pp);
+        ctx->total_launches += 1;
+        POTTS_CUDA(cudaMemsetAsync(xi, 0, xi_bytes, s));
+        for (int it = 0; it < iters; ++it) {
+            POTTS_TRY(seg_begin(ctx));
+            potts::dual_kernel<K><<<nb, potts::kPlainThreads, 0, s>>>(g, xi, Vb, tau2, ctx->thr);
+            potts::primal_kernel<K><<<nb, potts::kPlainThreads, 0, s>>>(g, xi, V, Vb, d_u, pp, dq ? dq + it : nullptr);
+            ctx->loop_launches += 2;
+            ctx->total_launches += 2;
+            if (ge > 0 && (it + 1) % ge == 0) POTTS_TRY(run_energy<K>(ctx, g, xi, V, d_u, pp, energy + 3 * ((it + 1) / ge - 1)));
+            if (o.sync_monitor && dq) POTTS_TRY(monitor_sync<K>(ctx, it));
+        }
+        POTTS_TRY(seg_end(ctx));
+        POTTS_CUDA(cudaGetLastError());
+    } else {
+        // Fused schedule: a dual step gives Xi^1 from V^0 (= Vbar^0); launch m
+        // (m = 1 .. iters-1) turns (Xi^m, V^{m-1}) into (Xi^{m+1}, V^m); a final
+        // primal step gives V^iters from Xi^iters.
+        potts::init_kernel<K><<<nb, potts::kPlainThreads, 0, s>>>(g, d_u, st.v[0], nullptr, pp);
+        ctx->total_launches += 1;
+        POTTS_CUDA(cudaMemsetAsync(st.xi[0], 0, xi_bytes, s));
+        if (iters > 0) {
+            potts::dual_kernel<K><<<nb, potts::kPlainThreads, 0, s>>>(g, st.xi[0], st.v[0], tau2, ctx->thr);
+            ctx->total_launches += 1;
+        }
+        for (int m = 1; m < iters; ++m) {
+            const int nxt = cur ^ 1;
+            POTTS_TRY(seg_begin(ctx));
+            ctx->loop_launches += 1;
+            ctx->total_launches += 1;
+            POTTS_CUDA(potts::launch_fused<K>(g, st.xi[cur], st.v[cur], st.xi[nxt], st.v[nxt], d_u, pp, tau2, ctx->thr,
+                                             dq ? dq + (m - 1) : nullptr, s));
+            if (ge > 0 && m % ge == 0) POTTS_TRY(run_energy<K>(ctx, g, st.xi[cur], st.v[nxt], d_u, pp, energy + 3 * (m / ge - 1)));
+            if (o.sync_monitor && dq) POTTS_TRY(monitor_sync<K>(ctx, m - 1));
+            cur = nxt;
+        }
+        POTTS_TRY(seg_end(ctx));
+        if (iters > 0) {
+            ctx->total_launches += 1;
+            potts::primal_kernel<K><<<nb, potts::kPlainThreads, 0, s>>>(g, st.xi[cur], st.v[cur], nullptr, d_u, pp,
+                                                                        dq ? dq + (iters - 1) : nullptr);
+            if (ge > 0 && iters % ge == 0) POTTS_TRY(run_energy<K>(ctx, g, st.xi[cur], st.v[cur], d_u, pp, energy + 3 * (iters / ge - 1)));
+            if (o.sync_monitor && dq) POTTS_TRY(monitor_sync<K>(ctx, iters - 1));
+        }
+        POTTS_CUDA(cudaGetLastError());
+    }
+    if (res_end > res_begin) {
+        const unsigned nbu = plain_blocks(g, res_begin, res_end);
+        ctx->total_launches += 1;
+        const float *Vf = o.variant == POTTS_VARIANT_PLAIN ? st.v[0] : st.v[cur];
+        const float *Xf = o.variant == POTTS_VARIANT_PLAIN ? st.xi[0] : st.xi[cur];
+        potts::update_kernel<K><<<nbu, potts::kPlainThreads, 0, s>>>(g, Vf, Xf, pp, res_begin, res_end, out.res,
+                                                                      out.labels, out.V, out.Xi, plane_out);
+        POTTS_CUDA(cudaGetLastError());
+    }
+    return POTTS_OK;
+}
+
+template <int K>
+int solve_k(potts_context *ctx, const float *d_u, const float *ci, float lam, float tau1, float tau2, int iters,
+            const potts_options &o, const Outputs &out, potts_stats *stats)
+{
+    const MappingCopy &mc = ctx->mapping;
+    const int n = (int)mc.m.n_images;
+    const int planes = state_planes(K, o.variant);
+
+    // Slab planner (potts-min-partition.cpp:560-577): as many n-slices as the
+    // free memory holds, halo = iters on each side of a slab.
+    size_t free_b = 0, total_b = 0;
+    POTTS_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t margin = size_t(512) << 20;
+    const size_t avail = free_b + ctx->state.bytes > margin ? free_b + ctx->state.bytes - margin : 0;
+    const uint64_t bytes_per_slice = sizeof(float) * (uint64_t)planes * (uint64_t)std::max<int64_t>(mc.n_lines, 1);
+    int slab_w = o.slab_w > 0 ? o.slab_w : (int)std::min<uint64_t>(prev_stride(avail / bytes_per_slice), 0x7fffffe0u);
+    const int halo = iters;
+    int res_w = n, n_slabs = 1;
+    if (n <= slab_w) {
+        slab_w = n;
+    } else {
+        res_w = slab_w - 2 * halo;
+        if (res_w <= 0)
+            return fail(POTTS_ENOMEM, "Not enough memory. Reduce the mask radius or the number of iterations.");
+        n_slabs = 1 + (n - slab_w + res_w - 1) / res_w;
+    }
+
+    const int nstride_w = (int)get_stride((uint32_t)slab_w);
+    const int64_t plane_w = mc.n_lines * (int64_t)nstride_w;
+    const size_t state_bytes = sizeof(float) * (size_t)planes * (size_t)std::max<int64_t>(plane_w, 1);
+    POTTS_TRY(ensure(ctx, ctx->state, state_bytes));
+    POTTS_TRY(ensure(ctx, ctx->dq, sizeof(float) * (size_t)std::max(iters, 1)));
+    const int n_energy = o.gap_every > 0 ? iters / o.gap_every : 0;
+    POTTS_TRY(ensure(ctx, ctx->energy, sizeof(double) * 3 * (size_t)std::max(n_energy, 1)));
+    if (n_energy > 0) {
+        const int chunks = (slab_w + potts::kPlainThreads - 1) / potts::kPlainThreads;
+        POTTS_TRY(ensure(ctx, ctx->partial, sizeof(double2) * (size_t)std::max<int64_t>(mc.n_lines * chunks, 1)));
+    }
+
+    float *base = (float *)ctx->state.p;
+    SlabState st;
+    const size_t xi_planes = 3 * (K - 1), v_planes = K - 1;
+    st.xi[0] = base;
+    if (o.variant == POTTS_VARIANT_PLAIN) {
+        st.v[0] = base + xi_planes * plane_w;
+        st.v[1] = st.v[0] + v_planes * plane_w;
+        st.xi[1] = st.xi[0];
+    } else {
+        st.xi[1] = base + xi_planes * plane_w;
+        st.v[0] = st.xi[1] + xi_planes * plane_w;
+        st.v[1] = st.v[0] + v_planes * plane_w;
+    }
+
+    PhaseParams<K> pp;
+    for (int i = 0; i < K; ++i) pp.c[i] = ci[i];
+    pp.lam = lam;
+    pp.tau1 = tau1;
+
+    Geometry g;
+    g.lines = (const int4 *)ctx->lines.p;
+    g.n_lines = mc.n_lines;
+    g.plane_w = plane_w;
+    g.nstride_w = nstride_w;
+    g.nstride_in = (int)mc.m.nstride;
+
+    ctx->seg_used = 0;
+    ctx->seg_open = false;
+    ctx->loop_launches = ctx->total_launches = 0;
+    POTTS_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (int sl = 0; sl < n_slabs; ++sl) {
+        const int s0 = sl * res_w;
+        const int s1 = std::min(n, s0 + slab_w);
+        g.slab_start = s0;
+        g.ns = s1 - s0;
+        const int r0 = (s0 == 0) ? s0 : s0 + halo;
+        const int r1 = (s1 == n) ? s1 : s1 - halo;
+        if (mc.n_lines > 0)
+            POTTS_TRY(run_slab<K>(ctx, g, d_u, pp, tau2, iters, o, st, r0 - s0, r1 - s0, out, (int64_t)mc.span));
+    }
+    POTTS_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+
+    if (stats) {
+        POTTS_CUDA(cudaStreamSynchronize(ctx->stream));
+        float ms = 0.0f;
+        POTTS_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        stats->n_slabs = n_slabs;
+        stats->slab_w = slab_w;
+        stats->iters = iters;
+        stats->solve_ms = ms;
+        POTTS_TRY(seg_total_ms(ctx, &stats->loop_ms));
+        stats->loop_launches = ctx->loop_launches;
+        stats->total_launches = ctx->total_launches;
+        stats->state_bytes = state_bytes;
+        stats->dq_last = 0.0f;
+        if (o.track_dq && iters > 0) {
+            std::vector<float> tr((size_t)iters);
+            POTTS_CUDA(cudaMemcpy(tr.data(), ctx->dq.p, sizeof(float) * iters, cudaMemcpyDeviceToHost));
+            stats->dq_last = std::sqrt(tr.back());
+            if (stats->dq_trace) std::memcpy(stats->dq_trace, tr.data(), sizeof(float) * iters);
+        }
+        if (stats->energy_trace && n_energy > 0)
+            POTTS_CUDA(cudaMemcpy(stats->energy_trace, ctx->energy.p, sizeof(double) * 3 * n_energy,
+                                  cudaMemcpyDeviceToHost));
+    }
+    return POTTS_OK;
+}
+
+int check_params(int K, const float *ci, float lam, float tau1, float tau2, int iters, const potts_options &o)
+{
+    if (K < 2 || K > POTTS_MAX_PHASES) return fail(POTTS_EINVAL, "K must be in [2, 6]");
+    if (!ci) return fail(POTTS_EINVAL, "ci is NULL");
+    for (int i = 0; i < K; ++i)
+        if (!std::isfinite(ci[i])) return fail(POTTS_EINVAL, "labels must be finite");
+    if (!std::isfinite(lam) || !std::isfinite(tau1) || !std::isfinite(tau2))
+        return fail(POTTS_EINVAL, "lambda, tau1 and tau2 must be finite");
+    if (iters < 0) return fail(POTTS_EINVAL, "iters must be >= 0");
+    if (o.variant != POTTS_VARIANT_FUSED && o.variant != POTTS_VARIANT_PLAIN)
+        return fail(POTTS_EINVAL, "unknown variant");
+    if (o.storage != POTTS_STORE_F32) return fail(POTTS_EINVAL, "unknown storage");
+    if (o.gap_every < 0 || o.slab_w < 0) return fail(POTTS_EINVAL, "gap_every and slab_w must be >= 0");
+    return POTTS_OK;
+}
+
+int solve_dispatch(potts_context *ctx, const potts_mapping *map, const float *d_u, int K, const float *ci,
+                   float lam, float tau1, float tau2, int iters, const potts_options *opts, const Outputs &out,
+                   potts_stats *stats)
+{
+    if (!ctx) return fail(POTTS_EINVAL, "context is NULL");
+    potts_options o;
+    potts_default_options(&o);
+    if (opts) o = *opts;
+    POTTS_TRY(check_params(K, ci, lam, tau1, tau2, iters, o));
+    if (!d_u) return fail(POTTS_EINVAL, "u is NULL");
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    POTTS_TRY(upload_lines(ctx, map));
+    switch (K) {
+    case 2: return solve_k<2>(ctx, d_u, ci, lam, tau1, tau2, iters, o, out, stats);
+    case 3: return solve_k<3>(ctx, d_u, ci, lam, tau1, tau2, iters, o, out, stats);
+    case 4: return solve_k<4>(ctx, d_u, ci, lam, tau1, tau2, iters, o, out, stats);
+    case 5: return solve_k<5>(ctx, d_u, ci, lam, tau1, tau2, iters, o, out, stats);
+    case 6: return solve_k<6>(ctx, d_u, ci, lam, tau1, tau2, iters, o, out, stats);
+    }
+    return fail(POTTS_EINVAL, "K must be in [2, 6]");
+}
+
+int context_init(int device, void *stream, potts_context **out)
+{
+    if (!out) return fail(POTTS_EINVAL, "out is NULL");
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(POTTS_ENODEV, "no CUDA device");
+    }
+    if (device < 0 || device >= count) return fail(POTTS_EINVAL, "device index out of range");
+    POTTS_CUDA(cudaSetDevice(device));
+    auto *ctx = new potts_context();
+    ctx->device = device;
+    ctx->thr = compute_thresholds();
+    if (stream) {
+        ctx->stream = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete ctx;
+            return fail(POTTS_ECUDA, "cudaStreamCreate failed");
+        }
+        ctx->own_stream = true;
+    }
+    if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+        cudaMallocHost(&ctx->pinned_dq, sizeof(float)) != cudaSuccess) {
+        potts_context_destroy(ctx);
+        return fail(POTTS_ECUDA, "event/pinned allocation failed");
+    }
+    *out = ctx;
+    return POTTS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void potts_default_options(potts_options *o)
+{
+    if (!o) return;
+    o->variant = POTTS_VARIANT_FUSED;
+    o->storage = POTTS_STORE_F32;
+    o->gap_every = 0;
+    o->slab_w = 0;
+    o->track_dq = 1;
+    o->sync_monitor = 0;
+}
+
+const char *potts_status_string(int s)
+{
+    switch (s) {
+    case POTTS_OK: return "ok";
+    case POTTS_EINVAL: return "invalid argument";
+    case POTTS_ENOMEM: return "out of device memory";
+    case POTTS_ECUDA: return "CUDA error";
+    case POTTS_ETIMEOUT: return "device wait timed out";
+    case POTTS_ENODEV: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+const char *potts_last_error(void) { return g_last_error.c_str(); }
+
+int potts_context_create(int device, potts_context **out) { return context_init(device, nullptr, out); }
+
+int potts_context_create_on_stream(int device, void *stream, potts_context **out)
+{
+    if (!stream) return fail(POTTS_EINVAL, "stream is NULL");
+    return context_init(device, stream, out);
+}
+
+void potts_context_destroy(potts_context *ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (DevBuf *b : {&ctx->lines, &ctx->state, &ctx->dq, &ctx->energy, &ctx->partial, &ctx->host_u,
+                      &ctx->host_res, &ctx->host_labels})
+        if (b->p) cudaFree(b->p);
+    if (ctx->pinned_dq) cudaFreeHost(ctx->pinned_dq);
+    for (cudaEvent_t e : ctx->seg_ev) cudaEventDestroy(e);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+int potts_context_synchronize(potts_context *ctx)
+{
+    if (!ctx) return fail(POTTS_EINVAL, "context is NULL");
+    POTTS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return POTTS_OK;
+}
+
+int potts_device_memory(potts_context *ctx, size_t *available, size_t *total)
+{
+    if (!ctx || !available || !total) return fail(POTTS_EINVAL, "NULL argument");
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    size_t f = 0, t = 0;
+    POTTS_CUDA(cudaMemGetInfo(&f, &t));
+    *available = f + cached_bytes(ctx);
+    *total = t;
+    return POTTS_OK;
+}
+
+int potts_field_create(potts_context *ctx, const potts_mapping *map, potts_field **out)
+{
+    if (!ctx || !out) return fail(POTTS_EINVAL, "NULL argument");
+    *out = nullptr;
+    auto *f = new potts_field();
+    int s = copy_mapping(map, f->mapping);
+    if (s != POTTS_OK) {
+        delete f;
+        return s;
+    }
+    f->ctx = ctx;
+    cudaSetDevice(ctx->device);
+    const size_t bytes = sizeof(float) * (size_t)std::max<uint64_t>(f->mapping.span, 1);
+    cudaError_t e = cudaMalloc(&f->d, bytes);
+    if (e != cudaSuccess) {
+        delete f;
+        return fail(e == cudaErrorMemoryAllocation ? POTTS_ENOMEM : POTTS_ECUDA, cudaGetErrorString(e));
+    }
+    *out = f;
+    return POTTS_OK;
+}
+
+int potts_field_upload(potts_context *ctx, const potts_mapping *map, const float *host, potts_field **out)
+{
+    if (!host) return fail(POTTS_EINVAL, "host is NULL");
+    POTTS_TRY(potts_field_create(ctx, map, out));
+    potts_field *f = *out;
+    cudaError_t e = cudaMemcpyAsync(f->d, host, sizeof(float) * f->mapping.span, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        potts_field_destroy(f);
+        *out = nullptr;
+        return fail(POTTS_ECUDA, cudaGetErrorString(e));
+    }
+    return POTTS_OK;
+}
+
+int potts_field_download(potts_context *ctx, const potts_field *f, float *host, uint64_t span)
+{
+    if (!ctx || !f || !host) return fail(POTTS_EINVAL, "NULL argument");
+    if (span != f->mapping.span) return fail(POTTS_EINVAL, "Host and device images have different sizes.");
+    POTTS_CUDA(cudaMemcpyAsync(host, f->d, sizeof(float) * span, cudaMemcpyDeviceToHost, ctx->stream));
+    POTTS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return POTTS_OK;
+}
+
+float *potts_field_data(potts_field *f) { return f ? f->d : nullptr; }
+uint64_t potts_field_span(const potts_field *f) { return f ? f->mapping.span : 0; }
+
+void potts_field_destroy(potts_field *f)
+{
+    if (!f) return;
+    if (f->d) {
+        if (f->ctx) cudaStreamSynchronize(f->ctx->stream);
+        cudaFree(f->d);
+    }
+    delete f;
+}
+
+int potts_solve_device(potts_context *ctx, const potts_mapping *map, const float *d_u, int K, const float *ci,
+                       float lambda, float tau1, float tau2, int iters, const potts_options *opts, float *d_res,
+                       uint8_t *d_labels, float *d_V, float *d_Xi, potts_stats *stats)
+{
+    Outputs out{d_res, d_labels, d_V, d_Xi};
+    return solve_dispatch(ctx, map, d_u, K, ci, lambda, tau1, tau2, iters, opts, out, stats);
+}
+
+int potts_min_partition(potts_context *ctx, const potts_field *g, const potts_mapping *cpu_map, int K,
+                        const float *ci, float lambda, float tau1, float tau2, int iters,
+                        const potts_options *opts, potts_field **result, potts_stats *stats)
+{
+    if (!ctx || !g || !result) return fail(POTTS_EINVAL, "NULL argument");
+    *result = nullptr;
+    const potts_mapping *map = cpu_map ? cpu_map : &g->mapping.m;
+    if (cpu_map && (cpu_map->base == nullptr || cpu_map->base[cpu_map->cols] != g->mapping.span))
+        return fail(POTTS_EINVAL, "cpu_map does not describe g");
+    potts_field *res = nullptr;
+    POTTS_TRY(potts_field_create(ctx, map, &res));
+    cudaError_t e = cudaMemsetAsync(res->d, 0, sizeof(float) * res->mapping.span, ctx->stream);
+    if (e != cudaSuccess) {
+        potts_field_destroy(res);
+        return fail(POTTS_ECUDA, cudaGetErrorString(e));
+    }
+    Outputs out{res->d, nullptr, nullptr, nullptr};
+    int s = solve_dispatch(ctx, map, g->d, K, ci, lambda, tau1, tau2, iters, opts, out, stats);
+    if (s != POTTS_OK) {
+        potts_field_destroy(res);
+        return s;
+    }
+    *result = res;
+    return POTTS_OK;
+}
+
+int potts_solve_host(potts_context *ctx, const potts_mapping *map, const float *h_u, int K, const float *ci,
+                     float lambda, float tau1, float tau2, int iters, const potts_options *opts, float *h_res,
+                     uint8_t *h_labels, potts_stats *stats)
+{
+    if (!ctx || !map || !h_u) return fail(POTTS_EINVAL, "NULL argument");
+    POTTS_TRY(validate_mapping(map));
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    const uint64_t span = map->base[map->cols];
+    POTTS_TRY(ensure(ctx, ctx->host_u, sizeof(float) * std::max<uint64_t>(span, 1)));
+    if (h_res) POTTS_TRY(ensure(ctx, ctx->host_res, sizeof(float) * std::max<uint64_t>(span, 1)));
+    if (h_labels) POTTS_TRY(ensure(ctx, ctx->host_labels, std::max<uint64_t>(span, 1)));
+    POTTS_CUDA(cudaMemcpyAsync(ctx->host_u.p, h_u, sizeof(float) * span, cudaMemcpyHostToDevice, ctx->stream));
+    Outputs out{h_res ? (float *)ctx->host_res.p : nullptr, h_labels ? (uint8_t *)ctx->host_labels.p : nullptr,
+                nullptr, nullptr};
+    POTTS_TRY(solve_dispatch(ctx, map, (const float *)ctx->host_u.p, K, ci, lambda, tau1, tau2, iters, opts, out,
+                             stats));
+    if (h_res)
+        POTTS_CUDA(cudaMemcpyAsync(h_res, ctx->host_res.p, sizeof(float) * span, cudaMemcpyDeviceToHost, ctx->stream));
+    if (h_labels)
+        POTTS_CUDA(cudaMemcpyAsync(h_labels, ctx->host_labels.p, span, cudaMemcpyDeviceToHost, ctx->stream));
+    POTTS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return POTTS_OK;
+}
+
+uint64_t potts_cylinder_mapping(uint32_t rows, uint32_t cols, double xc, double yc, double r, uint32_t nstride,
+                                uint32_t *start_row, uint32_t *base, uint32_t *col_begin, uint32_t *col_end)
+{
+    // include/layout_cylinder.h:152-195: a row is kept iff it lies strictly
+    // inside the circle; columns are stored in order.
+    const double r2 = r * r;
+    uint64_t off = 0;
+    uint32_t cb = ~0u, ce = 0;
+    for (uint32_t col = 0; col < cols; ++col) {
+        const double dx = (double)col - xc;
+        const double d2 = r2 - dx * dx;
+        base[col] = (uint32_t)off;
+        start_row[col] = ~0u;
+        if (!(d2 > 0.0)) continue;
+        const double d = std::sqrt(d2);
+        double lo = std::ceil(yc - d);
+        if (yc - d == lo) lo += 1.0;  // on the circle: outside
+        double hi = std::floor(yc + d);
+        if (yc + d == hi) hi -= 1.0;
+        lo = std::max(0.0, lo);
+        hi = std::min((double)rows - 1.0, hi);
+        if (lo > hi) continue;
+        if (cb == ~0u) cb = col, ce = col;
+        ce = col + 1;
+        start_row[col] = (uint32_t)lo;
+        off += (uint64_t)((uint32_t)hi - (uint32_t)lo + 1) * nstride;
+    }
+    base[cols] = (uint32_t)off;
+    if (col_begin) *col_begin = cb;
+    if (col_end) *col_end = ce;
+    return off;
+}
+
+uint32_t potts_get_stride(uint32_t n) { return get_stride(n); }
+
+}  // extern "C"

@@ -1,0 +1,270 @@
+"""Host API mirroring the reference's Potts entry points.
+
+Reference interface (C++):
+  make_context()                                   cuda-context/cuda-context.cpp:18-20
+  upload(ctx, span) / download(ctx, field, span)   cuda-context/cuda-context.cpp:49-77
+  device_memory(ctx)                               cuda-context/cuda-context.cpp:22-42
+  potts_min_partition<K>(ctx, g, cpu_map, ci, 𝜆, 𝜏1, 𝜏2, iters)
+                                                   potts-model/potts-min-partition.h:8-16
+
+Each call goes through the C ABI of ``libpotts_b200.so``; errors raise
+``PottsError`` (the reference throws ``cuda::cuda_error`` and returns an empty
+pointer when memory runs out, potts-min-partition.cpp:571-577).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _native
+from ._native import PottsError, check
+from .layout import CylinderMapping
+
+MAX_PHASES = _native.MAX_PHASES
+
+
+def reference_tau() -> float:
+    """Step size of the reference CLI: 0.99 * sqrt(1/12) (potts-model/potts-model.cpp:141)."""
+    return float(np.float32(0.99) * np.sqrt(np.float32(1.0) / np.float32(12.0)))
+
+
+class CudaContext:
+    """One device and one stream (include/cuda-details/cuda-context-impl.h:35-65)."""
+
+    def __init__(self, device: int = 0, stream: Optional[int] = None):
+        lib = _native.host_lib()
+        h = ctypes.c_void_p()
+        if stream is None:
+            check(lib.potts_context_create(int(device), ctypes.byref(h)))
+        else:
+            check(lib.potts_context_create_on_stream(int(device), ctypes.c_void_p(int(stream)), ctypes.byref(h)))
+        self._h = h
+        self.device = int(device)
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        if self._h is None:
+            raise RuntimeError("context is closed")
+        return self._h
+
+    def synchronize(self) -> None:
+        check(_native.host_lib().potts_context_synchronize(self.handle))
+
+    def device_memory(self) -> tuple[int, int]:
+        a, t = ctypes.c_size_t(), ctypes.c_size_t()
+        check(_native.host_lib().potts_device_memory(self.handle, ctypes.byref(a), ctypes.byref(t)))
+        return int(a.value), int(t.value)
+
+    def close(self) -> None:
+        if self._h is not None:
+            _native.host_lib().potts_context_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def make_context(device: int = 0, stream: Optional[int] = None) -> CudaContext:
+    """make_context(): a context on `device`; `stream` is an optional cudaStream_t handle to share."""
+    return CudaContext(device, stream)
+
+
+class DeviceField:
+    """DeviceField<float> (include/cuda-details/device-field-impl.h:12-54): device voxels + mapping."""
+
+    def __init__(self, ctx: CudaContext, mapping: CylinderMapping, handle: ctypes.c_void_p):
+        self.ctx = ctx
+        self.mapping = mapping
+        self._h = handle
+
+    @property
+    def handle(self):
+        return self._h
+
+    def data_ptr(self) -> int:
+        return int(_native.host_lib().potts_field_data(self._h) or 0)
+
+    @property
+    def span(self) -> int:
+        return int(_native.host_lib().potts_field_span(self._h))
+
+    def free(self) -> None:
+        if self._h is not None:
+            _native.host_lib().potts_field_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def upload(ctx: CudaContext, mapping: CylinderMapping, host: np.ndarray) -> DeviceField:
+    host = np.ascontiguousarray(host, dtype=np.float32)
+    if host.size != mapping.span:
+        raise ValueError(f"host array has {host.size} floats, mapping span is {mapping.span}")
+    h = ctypes.c_void_p()
+    check(_native.host_lib().potts_field_upload(ctx.handle, ctypes.byref(mapping.as_c()),
+                                                host.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                                ctypes.byref(h)))
+    return DeviceField(ctx, mapping, h)
+
+
+def download(ctx: CudaContext, fld: DeviceField, out: Optional[np.ndarray] = None) -> np.ndarray:
+    span = fld.span
+    if out is None:
+        out = np.empty(span, dtype=np.float32)
+    if out.dtype != np.float32 or not out.flags.c_contiguous:
+        raise ValueError("out must be a contiguous float32 array")
+    check(_native.host_lib().potts_field_download(ctx.handle, fld.handle,
+                                                  out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                                  ctypes.c_uint64(out.size)))
+    return out
+
+
+def device_memory(ctx: CudaContext) -> tuple[int, int]:
+    return ctx.device_memory()
+
+
+def _ci_array(ci: Sequence[float]) -> np.ndarray:
+    c = np.ascontiguousarray(np.asarray(ci, dtype=np.float32))
+    if c.ndim != 1 or not (2 <= c.size <= MAX_PHASES):
+        raise ValueError(f"need 2..{MAX_PHASES} labels, got {c.size}")
+    return c
+
+
+@dataclass
+class SolveStats:
+    n_slabs: int
+    slab_w: int
+    iters: int
+    dq_last: float
+    solve_ms: float
+    loop_ms: float
+    loop_launches: int
+    total_launches: int
+    state_bytes: int
+    dq_trace: Optional[np.ndarray] = None       # [iters] max |dV|^2 per iteration (last slab)
+    energy_trace: Optional[np.ndarray] = None   # [iters // gap_every, 3] (lagrangian, dual, gap)
+
+
+def _make_stats(iters: int, gap_every: int, want_traces: bool):
+    st = _native.PottsStats()
+    dq = en = None
+    if want_traces and iters > 0:
+        dq = np.zeros(iters, dtype=np.float32)
+        st.dq_trace = dq.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        if gap_every > 0 and iters // gap_every > 0:
+            en = np.zeros((iters // gap_every, 3), dtype=np.float64)
+            st.energy_trace = en.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    return st, dq, en
+
+
+def _stats_out(st, dq, en) -> SolveStats:
+    return SolveStats(st.n_slabs, st.slab_w, st.iters, float(st.dq_last), float(st.solve_ms), float(st.loop_ms),
+                      int(st.loop_launches), int(st.total_launches), int(st.state_bytes), dq, en)
+
+
+def potts_min_partition(ctx: CudaContext, g: DeviceField, cpu_map: CylinderMapping, ci: Sequence[float],
+                        lam: float, tau1: float, tau2: float, iters: int, *, stats: bool = False,
+                        **options) -> DeviceField | tuple[DeviceField, SolveStats]:
+    """potts_min_partition<K> (potts-model/potts-min-partition.h:8-16): a new field holding
+    ci[argmax_i V_i] for every in-mask voxel of g."""
+    c = _ci_array(ci)
+    opts = _native.default_options(**options)
+    st, dq, en = _make_stats(iters, opts.gap_every, stats)
+    h = ctypes.c_void_p()
+    check(_native.host_lib().potts_min_partition(
+        ctx.handle, g.handle, ctypes.byref(cpu_map.as_c()), int(c.size),
+        c.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(lam), float(tau1), float(tau2), int(iters),
+        ctypes.byref(opts), ctypes.byref(h), ctypes.byref(st)))
+    res = DeviceField(ctx, cpu_map, h)
+    return (res, _stats_out(st, dq, en)) if stats else res
+
+
+def solve_device(ctx: CudaContext, mapping: CylinderMapping, u_ptr: int, ci: Sequence[float], lam: float,
+                 tau1: float, tau2: float, iters: int, *, res_ptr: int = 0, labels_ptr: int = 0, V_ptr: int = 0,
+                 Xi_ptr: int = 0, stats: bool = True, **options) -> Optional[SolveStats]:
+    """Device-pointer solve (potts_solve_device): inputs/outputs are raw device addresses laid out
+    with `mapping`; any output address may be 0.  With stats=False nothing waits for the GPU."""
+    c = _ci_array(ci)
+    opts = _native.default_options(**options)
+    st, dq, en = _make_stats(iters, opts.gap_every, stats)
+    check(_native.host_lib().potts_solve_device(
+        ctx.handle, ctypes.byref(mapping.as_c()), ctypes.c_void_p(int(u_ptr)), int(c.size),
+        c.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(lam), float(tau1), float(tau2), int(iters),
+        ctypes.byref(opts), ctypes.c_void_p(int(res_ptr)), ctypes.c_void_p(int(labels_ptr)),
+        ctypes.c_void_p(int(V_ptr)), ctypes.c_void_p(int(Xi_ptr)), ctypes.byref(st) if stats else None))
+    return _stats_out(st, dq, en) if stats else None
+
+
+def solve_host(ctx: CudaContext, mapping: CylinderMapping, u: np.ndarray, ci: Sequence[float], lam: float,
+               tau1: float, tau2: float, iters: int, *, res: Optional[np.ndarray] = None,
+               labels: Optional[np.ndarray] = None, stats: bool = False, **options) -> Optional[SolveStats]:
+    """Host-buffer solve (potts_solve_host): copies u in, solves, copies res/labels out; blocks."""
+    c = _ci_array(ci)
+    if u.dtype != np.float32 or not u.flags.c_contiguous or u.size != mapping.span:
+        raise ValueError("u must be a contiguous float32 array of mapping.span values")
+    for arr, dt in ((res, np.float32), (labels, np.uint8)):
+        if arr is not None and (arr.dtype != dt or not arr.flags.c_contiguous or arr.size != mapping.span):
+            raise ValueError("outputs must be contiguous arrays of mapping.span values")
+    opts = _native.default_options(**options)
+    st, dq, en = _make_stats(iters, opts.gap_every, stats)
+    check(_native.host_lib().potts_solve_host(
+        ctx.handle, ctypes.byref(mapping.as_c()), ctypes.c_void_p(u.ctypes.data), int(c.size),
+        c.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(lam), float(tau1), float(tau2), int(iters),
+        ctypes.byref(opts), ctypes.c_void_p(res.ctypes.data if res is not None else 0),
+        ctypes.c_void_p(labels.ctypes.data if labels is not None else 0), ctypes.byref(st) if stats else None))
+    return _stats_out(st, dq, en) if stats else None
+
+
+@dataclass
+class PottsResult:
+    labels: np.ndarray            # uint8 span: argmax index
+    res: np.ndarray               # float32 span: ci[argmax]
+    V: Optional[np.ndarray]       # float32 [K-1, span]
+    Xi: Optional[np.ndarray]      # float32 [3(K-1), span]
+    stats: SolveStats = field(default=None)
+
+
+def solve(mapping: CylinderMapping, u: np.ndarray, ci: Sequence[float], lam: float, tau1: float, tau2: float,
+          iters: int, *, ctx: Optional[CudaContext] = None, want_state: bool = True, **options) -> PottsResult:
+    """Convenience: solve a host volume on the GPU (through torch device buffers) and return host arrays."""
+    import torch
+
+    c = _ci_array(ci)
+    K = c.size
+    own = ctx is None
+    if own:
+        ctx = make_context(0, stream=torch.cuda.current_stream().cuda_stream)
+    try:
+        dev = torch.device("cuda", ctx.device)
+        span = mapping.span
+        du = torch.from_numpy(np.ascontiguousarray(u, dtype=np.float32)).to(dev)
+        dres = torch.zeros(span, dtype=torch.float32, device=dev)
+        dlab = torch.zeros(span, dtype=torch.uint8, device=dev)
+        dV = torch.zeros((K - 1, span), dtype=torch.float32, device=dev) if want_state else None
+        dX = torch.zeros((3 * (K - 1), span), dtype=torch.float32, device=dev) if want_state else None
+        st = solve_device(ctx, mapping, du.data_ptr(), c, lam, tau1, tau2, iters, res_ptr=dres.data_ptr(),
+                          labels_ptr=dlab.data_ptr(), V_ptr=dV.data_ptr() if dV is not None else 0,
+                          Xi_ptr=dX.data_ptr() if dX is not None else 0, stats=True, **options)
+        torch.cuda.synchronize(dev)
+        return PottsResult(dlab.cpu().numpy(), dres.cpu().numpy(),
+                           dV.cpu().numpy() if dV is not None else None,
+                           dX.cpu().numpy() if dX is not None else None, st)
+    finally:
+        if own:
+            ctx.close()
