@@ -41,6 +41,7 @@ METRIC = "Potts PD Gvox-iter/s at k=3, %HBM peak; BF16-store vs FP32 at ≤1e-4 
 UNIT = "Gvox-iter/s"
 K_LABELS = 3
 LAMBDA = 30.0
+RADIUS = {"config1": 370.0, "config0": 60.0, "mid": 180.0}
 
 
 def parse_args():
@@ -52,10 +53,15 @@ def parse_args():
     p.add_argument("--iters", type=int, default=1000)
     p.add_argument("--gap-every", type=int, default=50)
     p.add_argument("--variant", choices=["fused", "plain"], default="fused")
-    p.add_argument("--workload", choices=["config1", "config0"], default="config1")
+    p.add_argument("--workload", choices=["config1", "config0", "mid"], default="config1",
+                   help="config1: 768x768x1024 r=370 (the benchmark); config0: 128^3 r=60; "
+                        "mid: 384x384x256 r=180 (profiling size, state > L2)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
+    p.add_argument("--tile-rows", type=int, default=0, help="fused tile rows (0 = library default)")
+    p.add_argument("--tile-slices", type=int, default=0, help="fused tile slices (0 = library default)")
+    p.add_argument("--segment", type=int, default=0, help="columns per fused work item (0 = library default)")
     return p.parse_args()
 
 
@@ -260,7 +266,7 @@ def run_ours(args, dist_: Dist) -> None:
     import torch
 
     from segmentctscans_b200 import potts
-    from segmentctscans_b200.phantom import config0_phantom, config1_phantom
+    from segmentctscans_b200.phantom import config0_phantom, config1_phantom, make_phantom
 
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device")
@@ -268,8 +274,12 @@ def run_ours(args, dist_: Dist) -> None:
     torch.cuda.set_device(dev)
     dist_.init("nccl")
 
-    ph = (config1_phantom(seed=dist_.rank, device=dev) if args.workload == "config1"
-          else config0_phantom(seed=dist_.rank, device=dev))
+    if args.workload == "config1":
+        ph = config1_phantom(seed=dist_.rank, device=dev)
+    elif args.workload == "config0":
+        ph = config0_phantom(seed=dist_.rank, device=dev)
+    else:
+        ph = make_phantom(256, 384, 384, 180.0, seed=dist_.rank, radius_range=(6.0, 30.0), noise=7e-3, device=dev)
     m, u, ci = ph.mapping, ph.u, ph.ci
     truth = ph.truth
     del ph
@@ -282,10 +292,12 @@ def run_ours(args, dist_: Dist) -> None:
     res = torch.empty(span, dtype=torch.float32, device=dev)
     lab = torch.empty(span, dtype=torch.uint8, device=dev)
 
+    tile_opts = {"tile_rows": args.tile_rows, "tile_slices": args.tile_slices, "segment_cols": args.segment}
+
     def step():
         return potts.solve_device(ctx, m, u.data_ptr(), ci, LAMBDA, tau, tau, args.iters, res_ptr=res.data_ptr(),
                                   labels_ptr=lab.data_ptr(), stats=True, variant=variant,
-                                  gap_every=args.gap_every)
+                                  gap_every=args.gap_every, **tile_opts)
 
     for _ in range(args.warmup):
         step()
@@ -321,7 +333,7 @@ def run_ours(args, dist_: Dist) -> None:
     traffic = tr["dram_bytes_per_voxel_iter"] * vox if tr else None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
-                "kernel": "potts::fused_*_kernel" if args.variant == "fused" else "potts::dual_kernel+primal_kernel",
+                "kernel": "potts::fused_tiled_kernel" if args.variant == "fused" else "potts::dual_kernel+primal_kernel",
                 "bytes_per_voxel_iter": bpv, "avg_launch_ms": round(launch_s * 1000, 4),
                 "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)"}
 
@@ -343,7 +355,7 @@ def run_ours(args, dist_: Dist) -> None:
 
         def e2e_step():
             potts.solve_host(ctx, m, hu_np, ci, LAMBDA, tau, tau, args.iters, res=hres_np, labels=hlab_np,
-                             variant=variant, gap_every=args.gap_every)
+                             variant=variant, gap_every=args.gap_every, **tile_opts)
 
         e2e_step()  # allocates the context's staging buffers
         torch.cuda.synchronize(dev)
@@ -372,10 +384,11 @@ def run_ours(args, dist_: Dist) -> None:
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist_.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1000 * t_max / args.steps, 2), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"potts_k3_{'768x768x1024_r370' if args.workload == 'config1' else '128cube_r60'}",
-                       "rows": m.rows, "cols": m.cols, "n": m.n_images, "radius": 370 if args.workload == "config1" else 60,
+            "config": {"workload": f"potts_k3_{m.rows}x{m.cols}x{m.n_images}_r{RADIUS[args.workload]:g}",
+                       "rows": m.rows, "cols": m.cols, "n": m.n_images, "radius": RADIUS[args.workload],
                        "in_mask_voxels": vox, "k": K_LABELS, "lambda": LAMBDA, "tau": tau, "iters": args.iters,
                        "gap_every": args.gap_every, "variant": args.variant, "storage": "f32",
+                       "tile": [args.tile_rows, args.tile_slices, args.segment],
                        "parallelism": f"replica x{dist_.world}" if dist_.world > 1 else "single",
                        "l2": "inputs larger than L2 (state ~30 GB per GPU)"},
             "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clk, "cpu_baseline": cpu,

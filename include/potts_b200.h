@@ -75,6 +75,9 @@ typedef struct potts_options {
     int slab_w;       /* 0: plan slabs from free memory like the reference; > 0: force this slab width */
     int track_dq;     /* 1: record max_x |V^{k+1} - V^k|^2 of every iteration on the device */
     int sync_monitor; /* 1: reference behaviour, read the monitor back and sync after every iteration */
+    int tile_rows;    /* fused form: rows per tile (0 = default for K) */
+    int tile_slices;  /* fused form: slices (n) per tile (0 = default for K) */
+    int segment_cols; /* fused form: columns one tile marches over (0 = 32) */
 } potts_options;
 
 typedef struct potts_stats {
@@ -98,7 +101,7 @@ const char *potts_last_error(void);
 
 /* make_context() (cuda-context/cuda-context.cpp:18-20): device `device`, a new stream. */
 int potts_context_create(int device, potts_context **out);
-/* Same, but all work goes to the caller's cudaStream_t `stream` (not owned). */
+/* Same, but all work goes to the caller's cudaStream_t `stream` (not owned; NULL = the default stream). */
 int potts_context_create_on_stream(int device, void *stream, potts_context **out);
 void potts_context_destroy(potts_context *ctx);
 int potts_context_synchronize(potts_context *ctx);

@@ -1,5 +1,6 @@
 // C-ABI implementation of the B200 Potts solver: device context, fields,
 // slab planner and the iteration driver (potts-model/potts-min-partition.cpp:540-679).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -11,8 +12,8 @@
 
 #include "../../include/potts_b200.h"
 #include "geometry.cuh"
-#include "kernels_fused.cuh"
 #include "kernels_plain.cuh"
+#include "kernels_tiled.cuh"
 #include "voxel.cuh"
 
 using potts::DykstraThresholds;
@@ -186,8 +187,14 @@ struct potts_context {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     MappingCopy mapping;  // last mapping whose line table is on the device
     bool mapping_valid = false;
-    DevBuf lines, state, dq, energy, partial, host_u, host_res, host_labels;
+    DevBuf lines, state, dq, energy, partial, host_u, host_res, host_labels, ustage, err;
     float *pinned_dq = nullptr;
+    // tiled-kernel tables: per column (depends on the mapping) and the work
+    // items of the last (slab extent, tile shape) planned
+    DevBuf cols, work;
+    bool cols_valid = false;
+    int work_key[5] = {-1, -1, -1, -1, -1};
+    int n_work = 0;
     // Event pairs around runs of consecutive iteration launches (energy
     // evaluations and slab set-up fall outside them), and launch counters.
     std::vector<cudaEvent_t> seg_ev;
@@ -197,7 +204,7 @@ struct potts_context {
 };
 
 struct potts_field {
-    potts_context *ctx = nullptr;
+    int device = 0;  // fields may outlive the context that made them
     float *d = nullptr;
     MappingCopy mapping;
 };
@@ -256,13 +263,16 @@ int ensure(potts_context *ctx, DevBuf &b, size_t bytes)
 
 size_t cached_bytes(const potts_context *ctx)
 {
-    return ctx->state.bytes + ctx->partial.bytes + ctx->host_u.bytes + ctx->host_res.bytes + ctx->host_labels.bytes;
+    return ctx->state.bytes + ctx->partial.bytes + ctx->host_u.bytes + ctx->host_res.bytes + ctx->host_labels.bytes +
+           ctx->ustage.bytes;
 }
 
 int upload_lines(potts_context *ctx, const potts_mapping *map)
 {
     if (ctx->mapping_valid && same_mapping(ctx->mapping, *map)) return POTTS_OK;
     ctx->mapping_valid = false;
+    ctx->cols_valid = false;
+    ctx->work_key[0] = -1;
     POTTS_TRY(copy_mapping(map, ctx->mapping));
     const size_t bytes = sizeof(int4) * (size_t)std::max<int64_t>(ctx->mapping.n_lines, 1);
     POTTS_TRY(ensure(ctx, ctx->lines, bytes));
@@ -312,12 +322,243 @@ int run_energy(potts_context *ctx, const Geometry &g, const float *xi, const flo
     return POTTS_OK;
 }
 
+// Waits for the stream and reports a bounded device-side wait that gave up.
+int check_device_error(potts_context *ctx)
+{
+    int e = 0;
+    POTTS_CUDA(cudaMemcpyAsync(&e, ctx->err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    POTTS_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (e != 0) return fail(POTTS_ETIMEOUT, "a device-side wait for a tile load gave up");
+    return POTTS_OK;
+}
+
 template <int K>
 int monitor_sync(potts_context *ctx, int it)
 {
     POTTS_CUDA(cudaMemcpyAsync(ctx->pinned_dq, (float *)ctx->dq.p + it, sizeof(float), cudaMemcpyDeviceToHost,
                                ctx->stream));
     POTTS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return POTTS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Tiled fused kernel: tensor maps, per-column table, work items.
+// ---------------------------------------------------------------------------
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// A float tensor of `rank` dims (dims[0] contiguous), strides in bytes of dims 1.., box per dim.
+int encode_map(CUtensorMap *m, const float *base, int rank, const uint64_t *dims, const uint64_t *strides,
+               const uint32_t *box)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return fail(POTTS_ECUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    cuuint64_t gd[3], gs[2];
+    cuuint32_t bd[3], es[3] = {1, 1, 1};
+    for (int i = 0; i < rank; ++i) {
+        gd[i] = dims[i];
+        bd[i] = box[i];
+    }
+    for (int i = 0; i + 1 < rank; ++i) gs[i] = strides[i];
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank, const_cast<float *>(base), gd, gs, bd, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(POTTS_ECUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return POTTS_OK;
+}
+
+struct TileChoice {
+    int rows, slices, segment;
+};
+
+// Tile shapes compiled per K (rows x slices); the first entry is the default.
+template <int K>
+struct TileShapes;
+template <> struct TileShapes<2> { static constexpr int n = 2; static constexpr int r[n] = {8, 8}, t[n] = {128, 64}; };
+template <> struct TileShapes<3> { static constexpr int n = 4; static constexpr int r[n] = {8, 8, 16, 4}, t[n] = {128, 64, 64, 128}; };
+template <> struct TileShapes<4> { static constexpr int n = 2; static constexpr int r[n] = {8, 4}, t[n] = {64, 128}; };
+template <> struct TileShapes<5> { static constexpr int n = 1; static constexpr int r[n] = {4}, t[n] = {64}; };
+template <> struct TileShapes<6> { static constexpr int n = 1; static constexpr int r[n] = {4}, t[n] = {64}; };
+
+template <int K>
+int choose_tile(const potts_options &o, TileChoice *tc)
+{
+    tc->rows = TileShapes<K>::r[0];
+    tc->slices = TileShapes<K>::t[0];
+    tc->segment = o.segment_cols > 0 ? o.segment_cols : 32;
+    if (o.tile_rows > 0 || o.tile_slices > 0) {
+        for (int i = 0; i < TileShapes<K>::n; ++i)
+            if ((o.tile_rows <= 0 || o.tile_rows == TileShapes<K>::r[i]) &&
+                (o.tile_slices <= 0 || o.tile_slices == TileShapes<K>::t[i])) {
+                tc->rows = TileShapes<K>::r[i];
+                tc->slices = TileShapes<K>::t[i];
+                return POTTS_OK;
+            }
+        return fail(POTTS_EINVAL, "tile_rows x tile_slices is not a compiled tile shape for this K");
+    }
+    return POTTS_OK;
+}
+
+// Per-column table and work items (x = first row, y = first slice, z/w = column range).
+int plan_tiles(potts_context *ctx, int ns, const TileChoice &tc)
+{
+    const MappingCopy &mc = ctx->mapping;
+    const potts_mapping &m = mc.m;
+    if (!ctx->cols_valid) {
+        std::vector<int4> cols(std::max<uint32_t>(m.cols, 1), make_int4(0, 0, 0, 0));
+        for (uint32_t c = 0; c < m.cols; ++c) {
+            const int64_t cnt = (int64_t)(m.base[c + 1] - m.base[c]) / m.nstride;
+            cols[c].x = (int)(m.base[c] / m.nstride);
+            cols[c].y = cnt > 0 ? (int)m.start_row[c] : 0;
+            cols[c].z = cnt > 0 ? (int)(m.start_row[c] + cnt) : 0;
+        }
+        POTTS_TRY(ensure(ctx, ctx->cols, sizeof(int4) * cols.size()));
+        POTTS_CUDA(cudaMemcpy(ctx->cols.p, cols.data(), sizeof(int4) * cols.size(), cudaMemcpyHostToDevice));
+        ctx->cols_valid = true;
+    }
+    const int key[5] = {ns, tc.rows, tc.slices, tc.segment, (int)mc.n_lines};
+    if (std::equal(key, key + 5, ctx->work_key)) return POTTS_OK;
+    int row_lo = INT32_MAX, row_hi = 0;
+    for (uint32_t c = m.col_begin; c < m.col_end; ++c) {
+        const int64_t cnt = (int64_t)(m.base[c + 1] - m.base[c]) / m.nstride;
+        if (cnt <= 0) continue;
+        row_lo = std::min<int>(row_lo, (int)m.start_row[c]);
+        row_hi = std::max<int>(row_hi, (int)(m.start_row[c] + cnt));
+    }
+    struct Item {
+        int ca, r0, n0, cb;
+    };
+    std::vector<Item> items;
+    const int tiles = (ns + tc.slices - 1) / tc.slices;
+    for (int r0 = row_lo; r0 < row_hi; r0 += tc.rows) {
+        int run = -1;
+        for (int c = (int)m.col_begin; c <= (int)m.col_end; ++c) {
+            bool active = false;
+            if (c < (int)m.col_end) {
+                const int64_t cnt = (int64_t)(m.base[c + 1] - m.base[c]) / m.nstride;
+                active = cnt > 0 && (int)m.start_row[c] < r0 + tc.rows && (int)(m.start_row[c] + cnt) > r0;
+            }
+            if (active && run < 0) run = c;
+            if (!active && run >= 0) {
+                for (int ca = run; ca < c; ca += tc.segment)
+                    for (int t = 0; t < tiles; ++t) items.push_back({ca, r0, t * tc.slices, std::min(c, ca + tc.segment)});
+                run = -1;
+            }
+        }
+    }
+    // items sharing columns run together, so halo rows of neighbouring tiles meet in L2
+    std::sort(items.begin(), items.end(), [](const Item &a, const Item &b) {
+        if (a.ca != b.ca) return a.ca < b.ca;
+        if (a.n0 != b.n0) return a.n0 < b.n0;
+        return a.r0 < b.r0;
+    });
+    std::vector<int4> work(std::max<size_t>(items.size(), 1));
+    for (size_t i = 0; i < items.size(); ++i) work[i] = make_int4(items[i].r0, items[i].n0, items[i].ca, items[i].cb);
+    POTTS_TRY(ensure(ctx, ctx->work, sizeof(int4) * work.size()));
+    POTTS_CUDA(cudaMemcpy(ctx->work.p, work.data(), sizeof(int4) * work.size(), cudaMemcpyHostToDevice));
+    std::copy(key, key + 5, ctx->work_key);
+    ctx->n_work = (int)items.size();
+    return POTTS_OK;
+}
+
+struct FusedPlan {
+    CUtensorMap xi[2], v[2], u;
+    potts::TiledParams tp;
+    int n_work = 0;
+    TileChoice tile{};
+};
+
+template <int K, int R, int NT>
+int launch_tiled_shape(potts_context *ctx, const FusedPlan &fp, int in, float *Xout, float *Vout,
+                       const PhaseParams<K> &pp, float tau2, float *dq)
+{
+    using S = potts::TileShape<K, R, NT>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        POTTS_CUDA(cudaFuncSetAttribute(potts::fused_tiled_kernel<K, R, NT>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM_ALLOC));
+        attr_set = true;
+    }
+    if (fp.n_work == 0) return POTTS_OK;
+    potts::fused_tiled_kernel<K, R, NT><<<fp.n_work, S::THREADS, S::SMEM_ALLOC, ctx->stream>>>(
+        fp.xi[in], fp.v[in], fp.u, fp.tp, Xout, Vout, pp, tau2, ctx->thr, dq, (int *)ctx->err.p);
+    POTTS_CUDA(cudaGetLastError());
+    return POTTS_OK;
+}
+
+template <int K, int I = 0>
+int launch_tiled(potts_context *ctx, const FusedPlan &fp, int in, float *Xout, float *Vout, const PhaseParams<K> &pp,
+                 float tau2, float *dq)
+{
+    if constexpr (I < TileShapes<K>::n) {
+        constexpr int R = TileShapes<K>::r[I], NT = TileShapes<K>::t[I];
+        if (fp.tile.rows == R && fp.tile.slices == NT)
+            return launch_tiled_shape<K, R, NT>(ctx, fp, in, Xout, Vout, pp, tau2, dq);
+        return launch_tiled<K, I + 1>(ctx, fp, in, Xout, Vout, pp, tau2, dq);
+    } else {
+        return fail(POTTS_EINVAL, "no compiled tile shape matches");
+    }
+}
+
+template <int K>
+int prepare_fused(potts_context *ctx, const Geometry &g, const float *const xi[2], const float *const v[2],
+                  const float *d_u, const potts_options &o, FusedPlan *fp)
+{
+    POTTS_TRY(choose_tile<K>(o, &fp->tile));
+    const int R = fp->tile.rows, NT = fp->tile.slices;
+    POTTS_TRY(plan_tiles(ctx, g.ns, fp->tile));
+    fp->n_work = ctx->n_work;
+    const uint64_t L = (uint64_t)g.n_lines;
+    for (int b = 0; b < 2; ++b) {
+        const uint64_t dx[3] = {(uint64_t)g.nstride_w, L, (uint64_t)(3 * (K - 1))};
+        const uint64_t sx[2] = {(uint64_t)g.nstride_w * 4, (uint64_t)g.plane_w * 4};
+        const uint32_t bx[3] = {(uint32_t)(NT + 8), (uint32_t)(R + 2), (uint32_t)(3 * (K - 1))};
+        POTTS_TRY(encode_map(&fp->xi[b], xi[b], 3, dx, sx, bx));
+        const uint64_t dv[3] = {(uint64_t)g.nstride_w, L, (uint64_t)(K - 1)};
+        const uint32_t bv[3] = {(uint32_t)(NT + 4), (uint32_t)(R + 1), (uint32_t)(K - 1)};
+        POTTS_TRY(encode_map(&fp->v[b], v[b], 3, dv, sx, bv));
+    }
+    // u: read in place when the slab starts on a 16-byte boundary, else staged
+    const float *ubase = d_u;
+    uint64_t ustride = (uint64_t)g.nstride_in;
+    int ux0 = g.slab_start;
+    if (g.slab_start % 4 != 0) {
+        POTTS_TRY(ensure(ctx, ctx->ustage, sizeof(float) * (size_t)g.plane_w));
+        const int chunks = (g.ns + potts::kPlainThreads - 1) / potts::kPlainThreads;
+        potts::stage_u_kernel<<<(unsigned)(g.n_lines * chunks), potts::kPlainThreads, 0, ctx->stream>>>(
+            g, d_u, (float *)ctx->ustage.p);
+        ctx->total_launches += 1;
+        POTTS_CUDA(cudaGetLastError());
+        ubase = (const float *)ctx->ustage.p;
+        ustride = (uint64_t)g.nstride_w;
+        ux0 = 0;
+    }
+    const uint64_t du[2] = {ustride, L};
+    const uint64_t su[1] = {ustride * 4};
+    const uint32_t bu[2] = {(uint32_t)(NT + 4), (uint32_t)(R + 1)};
+    POTTS_TRY(encode_map(&fp->u, ubase, 2, du, su, bu));
+    fp->tp.cols = (const int4 *)ctx->cols.p;
+    fp->tp.work = (const int4 *)ctx->work.p;
+    fp->tp.col_begin = (int)ctx->mapping.m.col_begin;
+    fp->tp.col_end = (int)ctx->mapping.m.col_end;
+    fp->tp.ns = g.ns;
+    fp->tp.nstride_w = g.nstride_w;
+    fp->tp.plane_w = g.plane_w;
+    fp->tp.u_x0 = ux0;
     return POTTS_OK;
 }
 
@@ -356,6 +597,9 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
         // Fused schedule: a dual step gives Xi^1 from V^0 (= Vbar^0); launch m
         // (m = 1 .. iters-1) turns (Xi^m, V^{m-1}) into (Xi^{m+1}, V^m); a final
         // primal step gives V^iters from Xi^iters.
+        FusedPlan fp;
+        const float *xs[2] = {st.xi[0], st.xi[1]}, *vs[2] = {st.v[0], st.v[1]};
+        if (iters > 1) POTTS_TRY(prepare_fused<K>(ctx, g, xs, vs, d_u, o, &fp));
         potts::init_kernel<K><<<nb, potts::kPlainThreads, 0, s>>>(g, d_u, st.v[0], nullptr, pp);
         ctx->total_launches += 1;
         POTTS_CUDA(cudaMemsetAsync(st.xi[0], 0, xi_bytes, s));
@@ -368,8 +612,7 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
             POTTS_TRY(seg_begin(ctx));
             ctx->loop_launches += 1;
             ctx->total_launches += 1;
-            POTTS_CUDA(potts::launch_fused<K>(g, st.xi[cur], st.v[cur], st.xi[nxt], st.v[nxt], d_u, pp, tau2, ctx->thr,
-                                             dq ? dq + (m - 1) : nullptr, s));
+            POTTS_TRY(launch_tiled<K>(ctx, fp, cur, st.xi[nxt], st.v[nxt], pp, tau2, dq ? dq + (m - 1) : nullptr));
             if (ge > 0 && m % ge == 0) POTTS_TRY(run_energy<K>(ctx, g, st.xi[cur], st.v[nxt], d_u, pp, energy + 3 * (m / ge - 1)));
             if (o.sync_monitor && dq) POTTS_TRY(monitor_sync<K>(ctx, m - 1));
             cur = nxt;
@@ -464,6 +707,8 @@ int solve_k(potts_context *ctx, const float *d_u, const float *ci, float lam, fl
     ctx->seg_used = 0;
     ctx->seg_open = false;
     ctx->loop_launches = ctx->total_launches = 0;
+    POTTS_TRY(ensure(ctx, ctx->err, sizeof(int)));
+    POTTS_CUDA(cudaMemsetAsync(ctx->err.p, 0, sizeof(int), ctx->stream));
     POTTS_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
     for (int sl = 0; sl < n_slabs; ++sl) {
         const int s0 = sl * res_w;
@@ -477,8 +722,8 @@ int solve_k(potts_context *ctx, const float *d_u, const float *ci, float lam, fl
     }
     POTTS_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
 
+    if (stats || o.sync_monitor) POTTS_TRY(check_device_error(ctx));
     if (stats) {
-        POTTS_CUDA(cudaStreamSynchronize(ctx->stream));
         float ms = 0.0f;
         POTTS_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
         stats->n_slabs = n_slabs;
@@ -516,6 +761,8 @@ int check_params(int K, const float *ci, float lam, float tau1, float tau2, int 
         return fail(POTTS_EINVAL, "unknown variant");
     if (o.storage != POTTS_STORE_F32) return fail(POTTS_EINVAL, "unknown storage");
     if (o.gap_every < 0 || o.slab_w < 0) return fail(POTTS_EINVAL, "gap_every and slab_w must be >= 0");
+    if (o.tile_rows < 0 || o.tile_slices < 0 || o.segment_cols < 0)
+        return fail(POTTS_EINVAL, "tile options must be >= 0");
     return POTTS_OK;
 }
 
@@ -541,7 +788,7 @@ int solve_dispatch(potts_context *ctx, const potts_mapping *map, const float *d_
     return fail(POTTS_EINVAL, "K must be in [2, 6]");
 }
 
-int context_init(int device, void *stream, potts_context **out)
+int context_init(int device, void *stream, bool use_stream, potts_context **out)
 {
     if (!out) return fail(POTTS_EINVAL, "out is NULL");
     *out = nullptr;
@@ -555,8 +802,8 @@ int context_init(int device, void *stream, potts_context **out)
     auto *ctx = new potts_context();
     ctx->device = device;
     ctx->thr = compute_thresholds();
-    if (stream) {
-        ctx->stream = (cudaStream_t)stream;
+    if (use_stream) {
+        ctx->stream = (cudaStream_t)stream;  // NULL: the device's default stream
     } else {
         if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
             delete ctx;
@@ -586,6 +833,9 @@ void potts_default_options(potts_options *o)
     o->slab_w = 0;
     o->track_dq = 1;
     o->sync_monitor = 0;
+    o->tile_rows = 0;
+    o->tile_slices = 0;
+    o->segment_cols = 0;
 }
 
 const char *potts_status_string(int s)
@@ -603,12 +853,11 @@ const char *potts_status_string(int s)
 
 const char *potts_last_error(void) { return g_last_error.c_str(); }
 
-int potts_context_create(int device, potts_context **out) { return context_init(device, nullptr, out); }
+int potts_context_create(int device, potts_context **out) { return context_init(device, nullptr, false, out); }
 
 int potts_context_create_on_stream(int device, void *stream, potts_context **out)
 {
-    if (!stream) return fail(POTTS_EINVAL, "stream is NULL");
-    return context_init(device, stream, out);
+    return context_init(device, stream, true, out);
 }
 
 void potts_context_destroy(potts_context *ctx)
@@ -617,7 +866,7 @@ void potts_context_destroy(potts_context *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (DevBuf *b : {&ctx->lines, &ctx->state, &ctx->dq, &ctx->energy, &ctx->partial, &ctx->host_u,
-                      &ctx->host_res, &ctx->host_labels})
+                      &ctx->host_res, &ctx->host_labels, &ctx->ustage, &ctx->err, &ctx->cols, &ctx->work})
         if (b->p) cudaFree(b->p);
     if (ctx->pinned_dq) cudaFreeHost(ctx->pinned_dq);
     for (cudaEvent_t e : ctx->seg_ev) cudaEventDestroy(e);
@@ -655,7 +904,7 @@ int potts_field_create(potts_context *ctx, const potts_mapping *map, potts_field
         delete f;
         return s;
     }
-    f->ctx = ctx;
+    f->device = ctx->device;
     cudaSetDevice(ctx->device);
     const size_t bytes = sizeof(float) * (size_t)std::max<uint64_t>(f->mapping.span, 1);
     cudaError_t e = cudaMalloc(&f->d, bytes);
@@ -698,8 +947,8 @@ void potts_field_destroy(potts_field *f)
 {
     if (!f) return;
     if (f->d) {
-        if (f->ctx) cudaStreamSynchronize(f->ctx->stream);
-        cudaFree(f->d);
+        cudaSetDevice(f->device);
+        cudaFree(f->d);  // waits for work on the device that may still use it
     }
     delete f;
 }

@@ -30,59 +30,64 @@ __device__ __forceinline__ float fmax_ref(float a, float b) { return (a < b) ? b
 // Dual step at one voxel (potts-model/potts-min-partition.cpp:96-247):
 //   q = Xi + tau2 * grad+(Vbar), then Dykstra projection onto
 //   K = {|q_i - q_j| <= 1 for all i < j} with at most 20 sweeps.
+// It is split in three parts so that the tiled kernel can gather the voxels
+// that need the full projection loop before running it:
+//   dual_build_q      q from Xi and Vbar at x and its forward neighbours
+//   dual_first_sweep_is_identity
+//                     true when the first sweep changes nothing (no pair is
+//                     longer than 1: every correction is zero, max|delta| = 0
+//                     and the loop exits after one sweep)
+//   dual_project      the full loop (from zero corrections); returns sweeps
 // xi[3*i + axis] holds the stored K-1 labels; vb* are Vbar at x and at the
 // forward neighbours along n, row, col; h* say whether that neighbour exists.
-// Returns the number of sweeps run.
 // ---------------------------------------------------------------------------
 template <int K>
-__device__ __forceinline__ int dual_voxel(float (&xo)[3 * (K - 1)], const float (&xi)[3 * (K - 1)],
-                                          const float (&vb)[K - 1], const float (&vbn)[K - 1],
-                                          const float (&vbr)[K - 1], const float (&vbc)[K - 1], bool hn, bool hr,
-                                          bool hc, float tau2, DykstraThresholds thr)
+__device__ __forceinline__ void dual_build_q(float (&q)[K][3], const float (&xi)[3 * (K - 1)],
+                                             const float (&vb)[K - 1], const float (&vbn)[K - 1],
+                                             const float (&vbr)[K - 1], const float (&vbc)[K - 1], bool hn, bool hr,
+                                             bool hc, float tau2)
 {
-    float q[K][3];
-    {
-        float vk = 1.0f, vkn = 1.0f, vkr = 1.0f, vkc = 1.0f;
-        float xk0 = 0.0f, xk1 = 0.0f, xk2 = 0.0f;
+    float vk = 1.0f, vkn = 1.0f, vkr = 1.0f, vkc = 1.0f;
+    float xk0 = 0.0f, xk1 = 0.0f, xk2 = 0.0f;
 #pragma unroll
-        for (int i = 0; i < K; ++i) {
-            float vi, wn, wr, wc, x0, x1, x2;
-            if (i < K - 1) {
-                vi = vb[i];
-                vk = vk - vi;
-                wn = vbn[i];
-                vkn = vkn - wn;
-                wr = vbr[i];
-                vkr = vkr - wr;
-                wc = vbc[i];
-                vkc = vkc - wc;
-                x0 = xi[3 * i];
-                x1 = xi[3 * i + 1];
-                x2 = xi[3 * i + 2];
-                xk0 = xk0 - x0;
-                xk1 = xk1 - x1;
-                xk2 = xk2 - x2;
-            } else {
-                vi = vk;
-                wn = vkn;
-                wr = vkr;
-                wc = vkc;
-                x0 = xk0;
-                x1 = xk1;
-                x2 = xk2;
-            }
-            const float g0 = hn ? (wn - vi) : 0.0f;
-            const float g1 = hr ? (wr - vi) : 0.0f;
-            const float g2 = hc ? (wc - vi) : 0.0f;
-            q[i][0] = fmaf(g0, tau2, x0);
-            q[i][1] = fmaf(g1, tau2, x1);
-            q[i][2] = fmaf(g2, tau2, x2);
+    for (int i = 0; i < K; ++i) {
+        float vi, wn, wr, wc, x0, x1, x2;
+        if (i < K - 1) {
+            vi = vb[i];
+            vk = vk - vi;
+            wn = vbn[i];
+            vkn = vkn - wn;
+            wr = vbr[i];
+            vkr = vkr - wr;
+            wc = vbc[i];
+            vkc = vkc - wc;
+            x0 = xi[3 * i];
+            x1 = xi[3 * i + 1];
+            x2 = xi[3 * i + 2];
+            xk0 = xk0 - x0;
+            xk1 = xk1 - x1;
+            xk2 = xk2 - x2;
+        } else {
+            vi = vk;
+            wn = vkn;
+            wr = vkr;
+            wc = vkc;
+            x0 = xk0;
+            x1 = xk1;
+            x2 = xk2;
         }
+        const float g0 = hn ? (wn - vi) : 0.0f;
+        const float g1 = hr ? (wr - vi) : 0.0f;
+        const float g2 = hc ? (wc - vi) : 0.0f;
+        q[i][0] = fmaf(g0, tau2, x0);
+        q[i][1] = fmaf(g1, tau2, x1);
+        q[i][2] = fmaf(g2, tau2, x2);
     }
+}
 
-    // Fast path: in the first sweep every correction P is zero.  If no pair
-    // has |q_i2 - q_i1| > 1, every step is zero, the sweep ends with
-    // max|delta| = 0 and the loop exits; q is already the result.
+template <int K>
+__device__ __forceinline__ bool dual_first_sweep_is_identity(const float (&q)[K][3], DykstraThresholds thr)
+{
     bool any_long = false;
 #pragma unroll
     for (int i1 = 0; i1 < K - 1; ++i1) {
@@ -97,61 +102,84 @@ __device__ __forceinline__ int dual_voxel(float (&xo)[3 * (K - 1)], const float 
             any_long |= (s > thr.len_gt_one);
         }
     }
-    int sweeps = 1;
-    if (any_long) {
-        constexpr int kPairs = K * (K - 1) / 2;
-        float P[kPairs][3];
+    return !any_long;
+}
+
+template <int K>
+__device__ __forceinline__ int dual_project(float (&q)[K][3], DykstraThresholds thr)
+{
+    constexpr int kPairs = K * (K - 1) / 2;
+    float P[kPairs][3];
 #pragma unroll
-        for (int p = 0; p < kPairs; ++p) P[p][0] = P[p][1] = P[p][2] = 0.0f;
-        for (sweeps = 1; sweeps <= 20; ++sweeps) {
-            float max_dd = 0.0f;
-            int p = 0;
+    for (int p = 0; p < kPairs; ++p) P[p][0] = P[p][1] = P[p][2] = 0.0f;
+    int sweeps;
+    for (sweeps = 1; sweeps <= 20; ++sweeps) {
+        float max_dd = 0.0f;
+        int p = 0;
 #pragma unroll
-            for (int i1 = 0; i1 < K - 1; ++i1) {
+        for (int i1 = 0; i1 < K - 1; ++i1) {
 #pragma unroll
-                for (int i2 = i1 + 1; i2 < K; ++i2, ++p) {
-                    const float h0 = (q[i2][0] - q[i1][0]) + P[p][0];
-                    const float h1 = (q[i2][1] - q[i1][1]) + P[p][1];
-                    const float h2 = (q[i2][2] - q[i1][2]) + P[p][2];
-                    float s = h0 * h0;
-                    s = fmaf(h1, h1, s);
-                    s = fmaf(h2, h2, s);
-                    float n0 = 0.0f, n1 = 0.0f, n2 = 0.0f;
-                    if (s > thr.len_gt_one) {
-                        const float l = __fsqrt_rn(s);
-                        const float lm1 = l - 1.0f;
-                        n0 = __fdiv_rn(lm1 * h0, l);
-                        n1 = __fdiv_rn(lm1 * h1, l);
-                        n2 = __fdiv_rn(lm1 * h2, l);
-                    }
-                    const float d0 = 0.5f * (n0 - P[p][0]);
-                    const float d1 = 0.5f * (n1 - P[p][1]);
-                    const float d2 = 0.5f * (n2 - P[p][2]);
-                    float dd = d0 * d0;
-                    dd = fmaf(d1, d1, dd);
-                    dd = fmaf(d2, d2, dd);
-                    max_dd = fmax_ref(dd, max_dd);
-                    q[i1][0] = q[i1][0] + d0;
-                    q[i1][1] = q[i1][1] + d1;
-                    q[i1][2] = q[i1][2] + d2;
-                    q[i2][0] = q[i2][0] - d0;
-                    q[i2][1] = q[i2][1] - d1;
-                    q[i2][2] = q[i2][2] - d2;
-                    P[p][0] = n0;
-                    P[p][1] = n1;
-                    P[p][2] = n2;
+            for (int i2 = i1 + 1; i2 < K; ++i2, ++p) {
+                const float h0 = (q[i2][0] - q[i1][0]) + P[p][0];
+                const float h1 = (q[i2][1] - q[i1][1]) + P[p][1];
+                const float h2 = (q[i2][2] - q[i1][2]) + P[p][2];
+                float s = h0 * h0;
+                s = fmaf(h1, h1, s);
+                s = fmaf(h2, h2, s);
+                float n0 = 0.0f, n1 = 0.0f, n2 = 0.0f;
+                if (s > thr.len_gt_one) {
+                    const float l = __fsqrt_rn(s);
+                    const float lm1 = l - 1.0f;
+                    n0 = __fdiv_rn(lm1 * h0, l);
+                    n1 = __fdiv_rn(lm1 * h1, l);
+                    n2 = __fdiv_rn(lm1 * h2, l);
                 }
+                const float d0 = 0.5f * (n0 - P[p][0]);
+                const float d1 = 0.5f * (n1 - P[p][1]);
+                const float d2 = 0.5f * (n2 - P[p][2]);
+                float dd = d0 * d0;
+                dd = fmaf(d1, d1, dd);
+                dd = fmaf(d2, d2, dd);
+                max_dd = fmax_ref(dd, max_dd);
+                q[i1][0] = q[i1][0] + d0;
+                q[i1][1] = q[i1][1] + d1;
+                q[i1][2] = q[i1][2] + d2;
+                q[i2][0] = q[i2][0] - d0;
+                q[i2][1] = q[i2][1] - d1;
+                q[i2][2] = q[i2][2] - d2;
+                P[p][0] = n0;
+                P[p][1] = n1;
+                P[p][2] = n2;
             }
-            if (max_dd < thr.exit_below) break;
         }
-        if (sweeps > 20) sweeps = 20;
+        if (max_dd < thr.exit_below) break;
     }
+    return sweeps > 20 ? 20 : sweeps;
+}
+
+template <int K>
+__device__ __forceinline__ void dual_store(float (&xo)[3 * (K - 1)], const float (&q)[K][3])
+{
 #pragma unroll
     for (int i = 0; i < K - 1; ++i) {
         xo[3 * i] = q[i][0];
         xo[3 * i + 1] = q[i][1];
         xo[3 * i + 2] = q[i][2];
     }
+}
+
+// The whole dual step at one voxel; returns the number of sweeps.
+template <int K>
+__device__ __forceinline__ int dual_voxel(float (&xo)[3 * (K - 1)], const float (&xi)[3 * (K - 1)],
+                                          const float (&vb)[K - 1], const float (&vbn)[K - 1],
+                                          const float (&vbr)[K - 1], const float (&vbc)[K - 1], bool hn, bool hr,
+                                          bool hc, float tau2, DykstraThresholds thr)
+{
+    float q[K][3];
+    dual_build_q<K>(q, xi, vb, vbn, vbr, vbc, hn, hr, hc, tau2);
+    int sweeps = 1;
+    if (!dual_first_sweep_is_identity<K>(q, thr)) sweeps = dual_project<K>(q, thr);
+    dual_store<K>(xo, q);
     return sweeps;
 }
 

@@ -181,3 +181,35 @@ def test_errors_are_reported(cuda_device):
         # the context stays usable after errors
         res = potts.potts_min_partition(ctx, g, m, ci, 30.0, TAU, TAU, 3)
         assert res.span == m.span
+
+
+TILE_SHAPES = {2: [(8, 128), (8, 64)], 3: [(8, 128), (8, 64), (16, 64), (4, 128)], 4: [(8, 64), (4, 128)],
+               5: [(4, 64)], 6: [(4, 64)]}
+
+
+@pytest.mark.parametrize("K", [2, 3, 4, 5, 6])
+def test_every_tile_shape_and_segment_length(cuda_device, oracle_mod, K):
+    """Partial n-tiles (n = 150), the n/row halos, segment starts and ends (1, 3 and 32 columns)."""
+    m, u, ci = random_volume(150, 37, 35, 16.3, K, seed=20 + K)
+    o = oracle_mod.solve(m, u, ci, 30.0, TAU, TAU, 9, precision="f32")
+    for rows, slices in TILE_SHAPES[K]:
+        for seg in (1, 3, 32):
+            g = gpu_solve(m, u, ci, 30.0, TAU, TAU, 9, variant=0, tile_rows=rows, tile_slices=slices,
+                          segment_cols=seg)
+            assert_same(m, g, o)
+
+
+def test_unaligned_slab_starts_stage_u(cuda_device, oracle_mod):
+    """iters = 7, slab_w = 40: slabs start at 0, 26, 52, 78 (u staged when not 16-byte aligned)."""
+    m, u, ci = random_volume(100, 16, 16, 7.1, 3, seed=30)
+    g = gpu_solve(m, u, ci, 30.0, TAU, TAU, 7, variant=0, slab_w=40, want_state=False)
+    o = oracle_mod.solve(m, u, ci, 30.0, TAU, TAU, 7, precision="f32", slab_w=40, want_state=False)
+    assert g.stats.n_slabs == 4
+    assert_same(m, g, o, what=("labels", "res"))
+
+
+def test_unknown_tile_shape_is_rejected(cuda_device):
+    m, u, ci = random_volume(16, 10, 10, 4.4, 3, seed=31)
+    with pytest.raises(PottsError) as e:
+        gpu_solve(m, u, ci, 30.0, TAU, TAU, 5, variant=0, tile_rows=5, tile_slices=40)
+    assert e.value.status == 1
