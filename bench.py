@@ -62,6 +62,7 @@ def parse_args():
     p.add_argument("--tile-rows", type=int, default=0, help="fused tile rows (0 = library default)")
     p.add_argument("--tile-slices", type=int, default=0, help="fused tile slices (0 = library default)")
     p.add_argument("--segment", type=int, default=0, help="columns per fused work item (0 = library default)")
+    p.add_argument("--tile-vpt", type=int, default=0, help="fused slices per thread (0 = library default)")
     return p.parse_args()
 
 
@@ -292,7 +293,8 @@ def run_ours(args, dist_: Dist) -> None:
     res = torch.empty(span, dtype=torch.float32, device=dev)
     lab = torch.empty(span, dtype=torch.uint8, device=dev)
 
-    tile_opts = {"tile_rows": args.tile_rows, "tile_slices": args.tile_slices, "segment_cols": args.segment}
+    tile_opts = {"tile_rows": args.tile_rows, "tile_slices": args.tile_slices, "segment_cols": args.segment,
+                 "tile_vpt": args.tile_vpt}
 
     def step():
         return potts.solve_device(ctx, m, u.data_ptr(), ci, LAMBDA, tau, tau, args.iters, res_ptr=res.data_ptr(),
@@ -388,7 +390,7 @@ def run_ours(args, dist_: Dist) -> None:
                        "rows": m.rows, "cols": m.cols, "n": m.n_images, "radius": RADIUS[args.workload],
                        "in_mask_voxels": vox, "k": K_LABELS, "lambda": LAMBDA, "tau": tau, "iters": args.iters,
                        "gap_every": args.gap_every, "variant": args.variant, "storage": "f32",
-                       "tile": [args.tile_rows, args.tile_slices, args.segment],
+                       "tile": [args.tile_rows, args.tile_slices, args.tile_vpt, args.segment],
                        "parallelism": f"replica x{dist_.world}" if dist_.world > 1 else "single",
                        "l2": "inputs larger than L2 (state ~30 GB per GPU)"},
             "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clk, "cpu_baseline": cpu,

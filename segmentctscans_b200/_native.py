@@ -29,6 +29,7 @@ class PottsOptions(ctypes.Structure):
         ("variant", ctypes.c_int), ("storage", ctypes.c_int), ("gap_every", ctypes.c_int),
         ("slab_w", ctypes.c_int), ("track_dq", ctypes.c_int), ("sync_monitor", ctypes.c_int),
         ("tile_rows", ctypes.c_int), ("tile_slices", ctypes.c_int), ("segment_cols", ctypes.c_int),
+        ("tile_vpt", ctypes.c_int),
     ]
 
 

@@ -29,11 +29,13 @@
 // therefore run up to two planes apart instead of waiting for the slowest one
 // at every plane.
 //
-// Dykstra's full loop is needed only where some pair |q_i - q_j| exceeds 1;
-// elsewhere its first sweep is the identity.  Stage B tests this per voxel,
-// gathers the warp's voxels that need the loop into a shared-memory queue and
-// runs the loop on them with all 32 lanes busy, so the common voxels do not
-// wait for the warp's slowest lane.
+// Dykstra's full loop is needed only where some pair |q_i - q_j| exceeds 1
+// (a few percent of the voxels); elsewhere its first sweep is the identity.
+// Stage B tests this per voxel and appends the voxels that need the loop to a
+// per-warp ring queue in shared memory that persists across planes; whenever
+// 32 have gathered, each lane runs the loop on one of them and writes the
+// result to global memory itself (nothing reads Xi^{m+1} during the launch).
+// So the common voxels never wait for a partly idle warp.
 //
 // HBM traffic per voxel and iteration: Xi and V read and written once, u read
 // once (8(K-1)+1 floats: 68 bytes at K = 3); halo rows/slices and the
@@ -65,18 +67,19 @@ struct TiledParams {
     int u_x0;       // n offset of the slab in the u tensor map
 };
 
-template <int K, int R, int NT>
+template <int K, int R, int NT, int VPT>
 struct TileShape {
     static constexpr int D = 3;  // ring depth (planes)
-    static constexpr int C3 = 3 * (K - 1), C1 = K - 1, Q = NT / 4;
+    static constexpr int C3 = 3 * (K - 1), C1 = K - 1, Q = NT / VPT;  // Q threads per tile row
     static constexpr int NX = NT + 8;  // Xi box: slices n0-4 .. n0+NT+3
     static constexpr int NV = NT + 4;  // V/u/Vbar box: slices n0 .. n0+NT+3
     static constexpr int MAIN = R * Q;
     static constexpr int MAIN_WARPS = MAIN / 32;
-    static constexpr int HALO_WARP = MAIN_WARPS, PRODUCER_WARP = MAIN_WARPS + 1;
-    static constexpr int THREADS = MAIN + 64;
-    static constexpr int QSTRIDE = (3 * K) | 1;  // queue entry stride (odd: no bank conflicts)
-    static constexpr int QCAP = 4 * 32;           // a warp's voxels per plane
+    static constexpr int HALO_WARPS = (Q + 31) / 32;  // the high halo row (and the slice n0+NT)
+    static constexpr int PRODUCER_WARP = MAIN_WARPS + HALO_WARPS;
+    static constexpr int THREADS = MAIN + 32 * HALO_WARPS + 32;
+    static constexpr int QSTRIDE = (3 * K + 1) | 1;  // queue entry: q (3K floats) + state offset; odd stride
+    static constexpr int QCAP = 64;                    // ring of one pass (32) + one gather round (32)
     static constexpr int XI_BYTES = C3 * (R + 2) * NX * 4;
     static constexpr int V_BYTES = C1 * (R + 1) * NV * 4;
     static constexpr int U_BYTES = (R + 1) * NV * 4;
@@ -87,152 +90,197 @@ struct TileShape {
     static constexpr int OFF_U = OFF_V + D * V_SLOT;
     static constexpr int OFF_VB = OFF_U + D * U_SLOT;
     static constexpr int OFF_Q = OFF_VB + D * V_SLOT;
-    static constexpr int OFF_BAR = OFF_Q + al(MAIN_WARPS * QCAP * QSTRIDE * 4);
+    static constexpr int MAX_SEGMENT = 64;  // columns per work item
+    static constexpr int OFF_COLS = OFF_Q + al(MAIN_WARPS * QCAP * QSTRIDE * 4);
+    static constexpr int OFF_BAR = OFF_COLS + al((MAX_SEGMENT + 3) * 16);
     static constexpr int SMEM = OFF_BAR + 3 * D * 8 + 16;
     static constexpr int SMEM_ALLOC = SMEM + 128;  // room to align the base to 128 bytes
-    static_assert(NT % 4 == 0 && Q <= 32 && R + 1 <= 32, "tile shape");
+    static_assert((VPT == 2 || VPT == 4) && NT % VPT == 0 && R + 1 <= 32, "tile shape");
     static_assert(MAIN % 32 == 0, "row threads fill whole warps");
     static_assert(SMEM_ALLOC <= 227 * 1024, "shared memory of one block");
 };
 
-__device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
-__device__ __forceinline__ void sts4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
-__device__ __forceinline__ void f4_to(float (&a)[4], float4 v)
+// VPT consecutive floats of shared or global memory as one vector access.
+template <int VPT>
+__device__ __forceinline__ void ldv(float (&a)[VPT], const float *p)
 {
-    a[0] = v.x;
-    a[1] = v.y;
-    a[2] = v.z;
-    a[3] = v.w;
+    if constexpr (VPT == 4) {
+        const float4 v = *reinterpret_cast<const float4 *>(p);
+        a[0] = v.x, a[1] = v.y, a[2] = v.z, a[3] = v.w;
+    } else {
+        const float2 v = *reinterpret_cast<const float2 *>(p);
+        a[0] = v.x, a[1] = v.y;
+    }
+}
+template <int VPT>
+__device__ __forceinline__ void stv(float *p, const float (&a)[VPT])
+{
+    if constexpr (VPT == 4)
+        *reinterpret_cast<float4 *>(p) = make_float4(a[0], a[1], a[2], a[3]);
+    else
+        *reinterpret_cast<float2 *>(p) = make_float2(a[0], a[1]);
 }
 
 __device__ __forceinline__ bool row_in_col(int4 ci, int row) { return row >= ci.y && row < ci.z; }
 
-template <int K, int R, int NT>
+template <int K, int R, int NT, int VPT>
 struct TiledSmem {
-    using S = TileShape<K, R, NT>;
+    using S = TileShape<K, R, NT, VPT>;
     uint8_t *base;
 
-    __device__ __forceinline__ float *xi_slot(int p) const
+    __device__ __forceinline__ float *xi_slot(int slot) const
     {
-        return reinterpret_cast<float *>(base + S::OFF_XI + (p % S::D) * S::XI_SLOT);
+        return reinterpret_cast<float *>(base + S::OFF_XI + slot * S::XI_SLOT);
     }
-    __device__ __forceinline__ float *v_slot(int p) const
+    __device__ __forceinline__ float *v_slot(int slot) const
     {
-        return reinterpret_cast<float *>(base + S::OFF_V + (p % S::D) * S::V_SLOT);
+        return reinterpret_cast<float *>(base + S::OFF_V + slot * S::V_SLOT);
     }
-    __device__ __forceinline__ float *u_slot(int p) const
+    __device__ __forceinline__ float *u_slot(int slot) const
     {
-        return reinterpret_cast<float *>(base + S::OFF_U + (p % S::D) * S::U_SLOT);
+        return reinterpret_cast<float *>(base + S::OFF_U + slot * S::U_SLOT);
     }
-    __device__ __forceinline__ float *vb_plane(int p) const
+    __device__ __forceinline__ float *vb_plane(int slot) const
     {
-        return reinterpret_cast<float *>(base + S::OFF_VB + (p % S::D) * S::V_SLOT);
+        return reinterpret_cast<float *>(base + S::OFF_VB + slot * S::V_SLOT);
     }
     __device__ __forceinline__ float *queue(int warp) const
     {
         return reinterpret_cast<float *>(base + S::OFF_Q) + warp * S::QCAP * S::QSTRIDE;
     }
-    __device__ __forceinline__ uint64_t *full(int p) const
+    __device__ __forceinline__ uint64_t *full(int slot) const
     {
-        return reinterpret_cast<uint64_t *>(base + S::OFF_BAR) + (p % S::D);
+        return reinterpret_cast<uint64_t *>(base + S::OFF_BAR) + slot;
     }
-    __device__ __forceinline__ uint64_t *ready(int p) const
+    __device__ __forceinline__ uint64_t *ready(int slot) const
     {
-        return reinterpret_cast<uint64_t *>(base + S::OFF_BAR) + S::D + (p % S::D);
+        return reinterpret_cast<uint64_t *>(base + S::OFF_BAR) + S::D + slot;
     }
-    __device__ __forceinline__ uint64_t *empty(int p) const
+    __device__ __forceinline__ uint64_t *empty(int slot) const
     {
-        return reinterpret_cast<uint64_t *>(base + S::OFF_BAR) + 2 * S::D + (p % S::D);
+        return reinterpret_cast<uint64_t *>(base + S::OFF_BAR) + 2 * S::D + slot;
     }
+    // column table entries of planes ca-1 .. cb+1: index c - ca + 1; an entry
+    // outside [col_begin, col_end) is all zeros (no rows)
+    __device__ __forceinline__ int4 *cols() const { return reinterpret_cast<int4 *>(base + S::OFF_COLS); }
     __device__ __forceinline__ volatile int *abort_flag() const
     {
         return reinterpret_cast<volatile int *>(base + S::OFF_BAR + 3 * S::D * 8);
     }
-    // phase parity of ring position p's use of its slot's barriers
-    __device__ __forceinline__ static uint32_t parity(int p) { return (uint32_t)((p / S::D) & 1); }
     // element (comp, box row, box slice) of an Xi plane / a V-shaped plane
     __device__ __forceinline__ static int xi_at(int comp, int rr, int nn) { return (comp * (R + 2) + rr) * S::NX + nn; }
     __device__ __forceinline__ static int v_at(int comp, int rr, int nn) { return (comp * (R + 1) + rr) * S::NV + nn; }
 };
 
-// Stage A for 4 consecutive slices n0+4q .. n0+4q+3 of tile row rr (row r0+rr).
-// Planes are indexed by "ring position" p = c - ca + 1 (plane ca-1 is p = 0).
-template <int K, int R, int NT>
-__device__ __forceinline__ void stage_a_quad(const TiledSmem<K, R, NT> &sm, const TiledParams &tp,
-                                             const PhaseParams<K> &pp, int p, int c, int r0, int rr, int n0, int q,
-                                             bool store_v, float *__restrict__ Vout, float &dqmax)
+// Stage A for VPT consecutive slices n0+VPT*q .. of tile row rr (row r0+rr).
+// Planes are indexed by "ring position" p = c - ca + 1 (plane ca-1 is p = 0);
+// sc and sp are the ring slots of planes p and p-1.
+template <int K, int R, int NT, int VPT>
+__device__ __forceinline__ void stage_a_chunk(const TiledSmem<K, R, NT, VPT> &sm, const TiledParams &tp,
+                                              const PhaseParams<K> &pp, int p, int sc, int sp, int r0, int rr,
+                                              int n0, int q, bool store_v, float *__restrict__ Vout, float &dqmax)
 {
-    using S = TileShape<K, R, NT>;
-    using T = TiledSmem<K, R, NT>;
+    using S = TileShape<K, R, NT, VPT>;
+    using T = TiledSmem<K, R, NT, VPT>;
     const int row = r0 + rr;
-    float *vb = sm.vb_plane(p);
-    const int4 ci = tp.cols[c];
-    const int nb = n0 + 4 * q;
+    float *vb = sm.vb_plane(sc);
+    const int4 ci = sm.cols()[p];
+    const int off = VPT * q;  // offset of the chunk in the V-shaped boxes
+    const int nb = n0 + off;
     if (!row_in_col(ci, row) || nb >= tp.ns) {
+        float z[VPT];
 #pragma unroll
-        for (int i = 0; i < K - 1; ++i) sts4(vb + T::v_at(i, rr, 4 * q), make_float4(0, 0, 0, 0));
+        for (int j = 0; j < VPT; ++j) z[j] = 0.0f;
+#pragma unroll
+        for (int i = 0; i < K - 1; ++i) stv<VPT>(vb + T::v_at(i, rr, off), z);
         return;
     }
     const bool pr = row > ci.y, hr = row + 1 < ci.z;
-    const bool pc = c - 1 >= tp.col_begin && row_in_col(tp.cols[c - 1], row);
-    const bool hc = c + 1 < tp.col_end && row_in_col(tp.cols[c + 1], row);
-    const float *xs = sm.xi_slot(p), *xp = sm.xi_slot(p - 1);
-    const float *vs = sm.v_slot(p), *us = sm.u_slot(p);
+    const bool pc = row_in_col(sm.cols()[p - 1], row);
+    const bool hc = row_in_col(sm.cols()[p + 1], row);
+    const float *xs = sm.xi_slot(sc), *xp = sm.xi_slot(sp);
+    const float *vs = sm.v_slot(sc), *us = sm.u_slot(sc);
 
-    float x[S::C3][4], xn[K - 1][4], xr[K - 1][4], xc[K - 1][4], v[K - 1][4], u[4];
+    float onew[K - 1][VPT], obar[K - 1][VPT];
+    if constexpr (VPT == 2) {
+        // both slices with paired FP32 instructions
+        const float2 *xs2 = reinterpret_cast<const float2 *>(xs);
+        float2 x[S::C3], xin[K - 1], xr[K - 1], xc[K - 1], v[K - 1], vn[K - 1], vbar[K - 1];
 #pragma unroll
-    for (int comp = 0; comp < S::C3; ++comp) f4_to(x[comp], lds4(xs + T::xi_at(comp, rr + 1, 4 * q + 4)));
-#pragma unroll
-    for (int i = 0; i < K - 1; ++i) {
-        f4_to(xn[i], lds4(xs + T::xi_at(3 * i, rr + 1, 4 * q)));  // slices nb-4 .. nb-1
-        f4_to(xr[i], lds4(xs + T::xi_at(3 * i + 1, rr, 4 * q + 4)));
-        f4_to(xc[i], lds4(xp + T::xi_at(3 * i + 2, rr + 1, 4 * q + 4)));
-        f4_to(v[i], lds4(vs + T::v_at(i, rr, 4 * q)));
-    }
-    f4_to(u, lds4(us + T::v_at(0, rr, 4 * q)));
-
-    float onew[K - 1][4], obar[K - 1][4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int n = nb + j;
-        float xi_j[S::C3], xin_j[K - 1], xir_j[K - 1], xic_j[K - 1], v_j[K - 1], vn[K - 1], vbar[K - 1];
-#pragma unroll
-        for (int comp = 0; comp < S::C3; ++comp) xi_j[comp] = x[comp][j];
+        for (int comp = 0; comp < S::C3; ++comp) x[comp] = xs2[T::xi_at(comp, rr + 1, off + 4) / 2];
 #pragma unroll
         for (int i = 0; i < K - 1; ++i) {
-            xin_j[i] = (j == 0) ? xn[i][3] : x[3 * i][j - 1];
-            xir_j[i] = xr[i][j];
-            xic_j[i] = xc[i][j];
-            v_j[i] = v[i][j];
+            const float2 before = xs2[T::xi_at(3 * i, rr + 1, off + 2) / 2];  // slices nb-2, nb-1
+            xin[i] = f2(before.y, x[3 * i].x);
+            xr[i] = xs2[T::xi_at(3 * i + 1, rr, off + 4) / 2];
+            xc[i] = reinterpret_cast<const float2 *>(xp)[T::xi_at(3 * i + 2, rr + 1, off + 4) / 2];
+            v[i] = reinterpret_cast<const float2 *>(vs)[T::v_at(i, rr, off) / 2];
         }
-        float d = 0.0f;
-        if (n < tp.ns) {
-            d = primal_voxel<K>(vn, vbar, v_j, xi_j, xin_j, xir_j, xic_j, n > 0, n + 1 < tp.ns, pr, hr, pc, hc, u[j],
-                                pp.c, pp.lam, pp.tau1);
-        } else {
-#pragma unroll
-            for (int i = 0; i < K - 1; ++i) vn[i] = vbar[i] = 0.0f;
-        }
-        if (store_v) dqmax = fmaxf(dqmax, d);
+        const float2 u2 = reinterpret_cast<const float2 *>(us)[T::v_at(0, rr, off) / 2];
+        const bool second = nb + 1 < tp.ns;
+        const float fr = pr ? 1.0f : 0.0f, gr = hr ? 1.0f : 0.0f, fc = pc ? 1.0f : 0.0f, gc = hc ? 1.0f : 0.0f;
+        const float2 d = primal_pair<K>(vn, vbar, v, x, xin, xr, xc, f2(nb > 0 ? 1.0f : 0.0f, 1.0f),
+                                        f2(second ? 1.0f : 0.0f, nb + 2 < tp.ns ? 1.0f : 0.0f), f2(fr), f2(gr),
+                                        f2(fc), f2(gc), u2, pp.c, pp.lam, pp.tau1);
+        if (store_v) dqmax = fmaxf(dqmax, second ? fmaxf(d.x, d.y) : d.x);
 #pragma unroll
         for (int i = 0; i < K - 1; ++i) {
-            onew[i][j] = vn[i];
-            obar[i][j] = vbar[i];
+            onew[i][0] = vn[i].x;
+            obar[i][0] = vbar[i].x;
+            onew[i][1] = second ? vn[i].y : 0.0f;
+            obar[i][1] = second ? vbar[i].y : 0.0f;
+        }
+    } else {
+        float x[S::C3][VPT], xn[K - 1][VPT], xr[K - 1][VPT], xc[K - 1][VPT], v[K - 1][VPT], u[VPT];
+#pragma unroll
+        for (int comp = 0; comp < S::C3; ++comp) ldv<VPT>(x[comp], xs + T::xi_at(comp, rr + 1, off + 4));
+#pragma unroll
+        for (int i = 0; i < K - 1; ++i) {
+            ldv<VPT>(xn[i], xs + T::xi_at(3 * i, rr + 1, off + 4 - VPT));  // the chunk before: slices nb-VPT .. nb-1
+            ldv<VPT>(xr[i], xs + T::xi_at(3 * i + 1, rr, off + 4));
+            ldv<VPT>(xc[i], xp + T::xi_at(3 * i + 2, rr + 1, off + 4));
+            ldv<VPT>(v[i], vs + T::v_at(i, rr, off));
+        }
+        ldv<VPT>(u, us + T::v_at(0, rr, off));
+#pragma unroll
+        for (int j = 0; j < VPT; ++j) {
+            const int n = nb + j;
+            float xi_j[S::C3], xin_j[K - 1], xir_j[K - 1], xic_j[K - 1], v_j[K - 1], vn[K - 1], vbar[K - 1];
+#pragma unroll
+            for (int comp = 0; comp < S::C3; ++comp) xi_j[comp] = x[comp][j];
+#pragma unroll
+            for (int i = 0; i < K - 1; ++i) {
+                xin_j[i] = (j == 0) ? xn[i][VPT - 1] : x[3 * i][j - 1];
+                xir_j[i] = xr[i][j];
+                xic_j[i] = xc[i][j];
+                v_j[i] = v[i][j];
+            }
+            float d = 0.0f;
+            if (n < tp.ns) {
+                d = primal_voxel<K>(vn, vbar, v_j, xi_j, xin_j, xir_j, xic_j, n > 0, n + 1 < tp.ns, pr, hr, pc, hc,
+                                    u[j], pp.c, pp.lam, pp.tau1);
+            } else {
+#pragma unroll
+                for (int i = 0; i < K - 1; ++i) vn[i] = vbar[i] = 0.0f;
+            }
+            if (store_v) dqmax = fmaxf(dqmax, d);
+#pragma unroll
+            for (int i = 0; i < K - 1; ++i) {
+                onew[i][j] = vn[i];
+                obar[i][j] = vbar[i];
+            }
         }
     }
 #pragma unroll
-    for (int i = 0; i < K - 1; ++i)
-        sts4(vb + T::v_at(i, rr, 4 * q), make_float4(obar[i][0], obar[i][1], obar[i][2], obar[i][3]));
+    for (int i = 0; i < K - 1; ++i) stv<VPT>(vb + T::v_at(i, rr, off), obar[i]);
     if (store_v) {
         const int64_t o = (int64_t)(ci.x + row - ci.y) * tp.nstride_w + nb;
-        if (nb + 4 <= tp.ns) {
+        if (nb + VPT <= tp.ns) {
 #pragma unroll
-            for (int i = 0; i < K - 1; ++i)
-                *reinterpret_cast<float4 *>(Vout + i * tp.plane_w + o) =
-                    make_float4(onew[i][0], onew[i][1], onew[i][2], onew[i][3]);
+            for (int i = 0; i < K - 1; ++i) stv<VPT>(Vout + i * tp.plane_w + o, onew[i]);
         } else {
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
+            for (int j = 0; j < VPT; ++j)
                 if (nb + j < tp.ns)
 #pragma unroll
                     for (int i = 0; i < K - 1; ++i) Vout[i * tp.plane_w + o + j] = onew[i][j];
@@ -241,24 +289,24 @@ __device__ __forceinline__ void stage_a_quad(const TiledSmem<K, R, NT> &sm, cons
 }
 
 // Stage A for the single slice n0+NT of tile row rr (the high halo along n).
-template <int K, int R, int NT>
-__device__ __forceinline__ void stage_a_nhalo(const TiledSmem<K, R, NT> &sm, const TiledParams &tp,
-                                              const PhaseParams<K> &pp, int p, int c, int r0, int rr, int n0)
+template <int K, int R, int NT, int VPT>
+__device__ __forceinline__ void stage_a_nhalo(const TiledSmem<K, R, NT, VPT> &sm, const TiledParams &tp,
+                                              const PhaseParams<K> &pp, int p, int sc, int sp, int r0, int rr, int n0)
 {
-    using S = TileShape<K, R, NT>;
-    using T = TiledSmem<K, R, NT>;
+    using S = TileShape<K, R, NT, VPT>;
+    using T = TiledSmem<K, R, NT, VPT>;
     const int row = r0 + rr, n = n0 + NT;
-    float *vb = sm.vb_plane(p);
-    const int4 ci = tp.cols[c];
+    float *vb = sm.vb_plane(sc);
+    const int4 ci = sm.cols()[p];
     if (!row_in_col(ci, row) || n >= tp.ns) {
 #pragma unroll
         for (int i = 0; i < K - 1; ++i) vb[T::v_at(i, rr, NT)] = 0.0f;
         return;
     }
     const bool pr = row > ci.y, hr = row + 1 < ci.z;
-    const bool pc = c - 1 >= tp.col_begin && row_in_col(tp.cols[c - 1], row);
-    const bool hc = c + 1 < tp.col_end && row_in_col(tp.cols[c + 1], row);
-    const float *xs = sm.xi_slot(p), *xp = sm.xi_slot(p - 1);
+    const bool pc = row_in_col(sm.cols()[p - 1], row);
+    const bool hc = row_in_col(sm.cols()[p + 1], row);
+    const float *xs = sm.xi_slot(sc), *xp = sm.xi_slot(sp);
     float xi[S::C3], xin[K - 1], xir[K - 1], xic[K - 1], v[K - 1], vn[K - 1], vbar[K - 1];
 #pragma unroll
     for (int comp = 0; comp < S::C3; ++comp) xi[comp] = xs[T::xi_at(comp, rr + 1, NT + 4)];
@@ -267,130 +315,161 @@ __device__ __forceinline__ void stage_a_nhalo(const TiledSmem<K, R, NT> &sm, con
         xin[i] = xs[T::xi_at(3 * i, rr + 1, NT + 3)];
         xir[i] = xs[T::xi_at(3 * i + 1, rr, NT + 4)];
         xic[i] = xp[T::xi_at(3 * i + 2, rr + 1, NT + 4)];
-        v[i] = sm.v_slot(p)[T::v_at(i, rr, NT)];
+        v[i] = sm.v_slot(sc)[T::v_at(i, rr, NT)];
     }
-    const float uu = sm.u_slot(p)[T::v_at(0, rr, NT)];
+    const float uu = sm.u_slot(sc)[T::v_at(0, rr, NT)];
     primal_voxel<K>(vn, vbar, v, xi, xin, xir, xic, n > 0, n + 1 < tp.ns, pr, hr, pc, hc, uu, pp.c, pp.lam, pp.tau1);
 #pragma unroll
     for (int i = 0; i < K - 1; ++i) vb[T::v_at(i, rr, NT)] = vbar[i];
 }
 
-// Stage B: dual step at plane c (ring position p) for slices n0+4q .. +3 of
-// tile row rr.  Called by every lane of the main warps (warp-wide gathers).
-template <int K, int R, int NT>
-__device__ __forceinline__ void stage_b_quad(const TiledSmem<K, R, NT> &sm, const TiledParams &tp, int p, int c,
-                                             int r0, int rr, int n0, int q, float tau2, DykstraThresholds thr,
-                                             float *__restrict__ Xout)
+// The full Dykstra loop for 32 queued voxels (ring entries head .. head+31,
+// fewer when count < 32), results stored to Xout by the lane that ran it.
+template <int K, int R, int NT, int VPT>
+__device__ __forceinline__ void drain_queue(float *qq, int head, int count, const TiledParams &tp,
+                                            DykstraThresholds thr, float *__restrict__ Xout)
 {
-    using S = TileShape<K, R, NT>;
-    using T = TiledSmem<K, R, NT>;
+    using S = TileShape<K, R, NT, VPT>;
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    if (lane < count) {
+        const float *ent = qq + ((head + lane) & (S::QCAP - 1)) * S::QSTRIDE;
+        float qe[K][3];
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            qe[i][0] = ent[3 * i];
+            qe[i][1] = ent[3 * i + 1];
+            qe[i][2] = ent[3 * i + 2];
+        }
+        const int64_t o = (int64_t)(uint32_t)__float_as_int(ent[3 * K]);
+        dual_project<K>(qe, thr);
+#pragma unroll
+        for (int i = 0; i < K - 1; ++i)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) Xout[(3 * i + a) * tp.plane_w + o] = qe[i][a];
+    }
+    __syncwarp();
+}
+
+// Stage B: dual step at ring position p (slot sc; slot sn holds plane p+1)
+// for VPT slices n0+VPT*q .. of tile row rr.  Called by every lane of the row
+// warps (warp-wide gathers); qhead/qcount describe the warp's ring queue.
+template <int K, int R, int NT, int VPT>
+__device__ __forceinline__ void stage_b_chunk(const TiledSmem<K, R, NT, VPT> &sm, const TiledParams &tp, int p,
+                                              int sc, int sn, int r0, int rr, int n0, int q, float tau2,
+                                              DykstraThresholds thr, float *__restrict__ Xout, int &qhead,
+                                              int &qcount)
+{
+    using S = TileShape<K, R, NT, VPT>;
+    using T = TiledSmem<K, R, NT, VPT>;
     const int lane = threadIdx.x & 31;
     const int row = r0 + rr;
-    const int4 ci = tp.cols[c];
-    const int nb = n0 + 4 * q;
+    const int4 ci = sm.cols()[p];
+    const int off = VPT * q;
+    const int nb = n0 + off;
     const bool live = row_in_col(ci, row) && nb < tp.ns;
+    const int64_t o = (int64_t)(ci.x + row - ci.y) * tp.nstride_w + nb;
 
-    float qv[4][K][3];
-    unsigned need = 0;  // bit j: slot j needs the full projection loop
+    float qv[VPT][K][3];
+    unsigned need = 0;  // bit j: slice nb+j needs the full projection loop
     if (live) {
         const bool hr = row + 1 < ci.z;
-        const bool hc = c + 1 < tp.col_end && row_in_col(tp.cols[c + 1], row);
-        const float *xs = sm.xi_slot(p);
-        const float *vb0 = sm.vb_plane(p), *vb1 = sm.vb_plane(p + 1);
-        float x[S::C3][4], b[K - 1][4], bnext[K - 1], br[K - 1][4], bc[K - 1][4];
+        const bool hc = row_in_col(sm.cols()[p + 1], row);
+        const float *xs = sm.xi_slot(sc);
+        const float *vb0 = sm.vb_plane(sc), *vb1 = sm.vb_plane(sn);
+        if constexpr (VPT == 2) {
+            float2 x[S::C3], b[K - 1], bn[K - 1], br[K - 1], bc[K - 1], q2[K][3];
 #pragma unroll
-        for (int comp = 0; comp < S::C3; ++comp) f4_to(x[comp], lds4(xs + T::xi_at(comp, rr + 1, 4 * q + 4)));
-#pragma unroll
-        for (int i = 0; i < K - 1; ++i) {
-            f4_to(b[i], lds4(vb0 + T::v_at(i, rr, 4 * q)));
-            bnext[i] = vb0[T::v_at(i, rr, 4 * q + 4)];
-            f4_to(br[i], lds4(vb0 + T::v_at(i, rr + 1, 4 * q)));
-            f4_to(bc[i], lds4(vb1 + T::v_at(i, rr, 4 * q)));
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            float xi_j[S::C3], b_j[K - 1], bn_j[K - 1], br_j[K - 1], bc_j[K - 1];
-#pragma unroll
-            for (int comp = 0; comp < S::C3; ++comp) xi_j[comp] = x[comp][j];
+            for (int comp = 0; comp < S::C3; ++comp)
+                x[comp] = reinterpret_cast<const float2 *>(xs)[T::xi_at(comp, rr + 1, off + 4) / 2];
 #pragma unroll
             for (int i = 0; i < K - 1; ++i) {
-                b_j[i] = b[i][j];
-                bn_j[i] = (j < 3) ? b[i][j + 1] : bnext[i];
-                br_j[i] = br[i][j];
-                bc_j[i] = bc[i][j];
+                b[i] = reinterpret_cast<const float2 *>(vb0)[T::v_at(i, rr, off) / 2];
+                bn[i] = f2(b[i].y, vb0[T::v_at(i, rr, off + 2)]);
+                br[i] = reinterpret_cast<const float2 *>(vb0)[T::v_at(i, rr + 1, off) / 2];
+                bc[i] = reinterpret_cast<const float2 *>(vb1)[T::v_at(i, rr, off) / 2];
             }
-            dual_build_q<K>(qv[j], xi_j, b_j, bn_j, br_j, bc_j, nb + j + 1 < tp.ns, hr, hc, tau2);
-            if (nb + j < tp.ns && !dual_first_sweep_is_identity<K>(qv[j], thr)) need |= 1u << j;
+            dual_build_q_pair<K>(q2, x, b, bn, br, bc, f2(nb + 1 < tp.ns ? 1.0f : 0.0f, nb + 2 < tp.ns ? 1.0f : 0.0f),
+                                 f2(hr ? 1.0f : 0.0f), f2(hc ? 1.0f : 0.0f), tau2);
+            need = dual_needs_loop_pair<K>(q2, thr) & (nb + 1 < tp.ns ? 3u : 1u);
+#pragma unroll
+            for (int i = 0; i < K; ++i)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    qv[0][i][a] = q2[i][a].x;
+                    qv[1][i][a] = q2[i][a].y;
+                }
+        } else {
+            float x[S::C3][VPT], b[K - 1][VPT], bnext[K - 1], br[K - 1][VPT], bc[K - 1][VPT];
+#pragma unroll
+            for (int comp = 0; comp < S::C3; ++comp) ldv<VPT>(x[comp], xs + T::xi_at(comp, rr + 1, off + 4));
+#pragma unroll
+            for (int i = 0; i < K - 1; ++i) {
+                ldv<VPT>(b[i], vb0 + T::v_at(i, rr, off));
+                bnext[i] = vb0[T::v_at(i, rr, off + VPT)];
+                ldv<VPT>(br[i], vb0 + T::v_at(i, rr + 1, off));
+                ldv<VPT>(bc[i], vb1 + T::v_at(i, rr, off));
+            }
+#pragma unroll
+            for (int j = 0; j < VPT; ++j) {
+                float xi_j[S::C3], b_j[K - 1], bn_j[K - 1], br_j[K - 1], bc_j[K - 1];
+#pragma unroll
+                for (int comp = 0; comp < S::C3; ++comp) xi_j[comp] = x[comp][j];
+#pragma unroll
+                for (int i = 0; i < K - 1; ++i) {
+                    b_j[i] = b[i][j];
+                    bn_j[i] = (j < VPT - 1) ? b[i][j + 1] : bnext[i];
+                    br_j[i] = br[i][j];
+                    bc_j[i] = bc[i][j];
+                }
+                dual_build_q<K>(qv[j], xi_j, b_j, bn_j, br_j, bc_j, nb + j + 1 < tp.ns, hr, hc, tau2);
+                if (nb + j < tp.ns && !dual_first_sweep_is_identity<K>(qv[j], thr)) need |= 1u << j;
+            }
         }
     }
 
-    // gather the voxels that need the loop, run it 32 at a time, scatter back
+    // voxels that need the loop go to the ring queue; a full pass runs as soon
+    // as 32 are waiting
     float *qq = sm.queue(threadIdx.x >> 5);
-    int pos[4];
-    int count = 0;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < VPT; ++j) {
         const bool mine = (need >> j) & 1u;
         const unsigned bal = __ballot_sync(0xffffffffu, mine);
+        if (bal == 0u) continue;
         if (mine) {
-            pos[j] = count + __popc(bal & ((1u << lane) - 1u));
-            float *e = qq + pos[j] * S::QSTRIDE;
+            const int slot = (qhead + qcount + __popc(bal & ((1u << lane) - 1u))) & (S::QCAP - 1);
+            float *e = qq + slot * S::QSTRIDE;
 #pragma unroll
             for (int i = 0; i < K; ++i) {
                 e[3 * i] = qv[j][i][0];
                 e[3 * i + 1] = qv[j][i][1];
                 e[3 * i + 2] = qv[j][i][2];
             }
+            e[3 * K] = __int_as_float((int)(o + j));
         }
-        count += __popc(bal);
-    }
-    if (count > 0) {
-        __syncwarp();
-        for (int e = lane; e < count; e += 32) {
-            float *ent = qq + e * S::QSTRIDE;
-            float qe[K][3];
-#pragma unroll
-            for (int i = 0; i < K; ++i) {
-                qe[i][0] = ent[3 * i];
-                qe[i][1] = ent[3 * i + 1];
-                qe[i][2] = ent[3 * i + 2];
-            }
-            dual_project<K>(qe, thr);
-#pragma unroll
-            for (int i = 0; i < K; ++i) {
-                ent[3 * i] = qe[i][0];
-                ent[3 * i + 1] = qe[i][1];
-                ent[3 * i + 2] = qe[i][2];
-            }
+        qcount += __popc(bal);
+        if (qcount >= 32) {
+            drain_queue<K, R, NT, VPT>(qq, qhead, 32, tp, thr, Xout);
+            qhead = (qhead + 32) & (S::QCAP - 1);
+            qcount -= 32;
         }
-        __syncwarp();
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if ((need >> j) & 1u) {
-                const float *e = qq + pos[j] * S::QSTRIDE;
-#pragma unroll
-                for (int i = 0; i < K; ++i) {
-                    qv[j][i][0] = e[3 * i];
-                    qv[j][i][1] = e[3 * i + 1];
-                    qv[j][i][2] = e[3 * i + 2];
-                }
-            }
-        __syncwarp();
     }
     if (!live) return;
 
-    const int64_t o = (int64_t)(ci.x + row - ci.y) * tp.nstride_w + nb;
-    if (nb + 4 <= tp.ns) {
+    if (need == 0u && nb + VPT <= tp.ns) {
 #pragma unroll
         for (int i = 0; i < K - 1; ++i)
 #pragma unroll
-            for (int a = 0; a < 3; ++a)
-                *reinterpret_cast<float4 *>(Xout + (3 * i + a) * tp.plane_w + o) =
-                    make_float4(qv[0][i][a], qv[1][i][a], qv[2][i][a], qv[3][i][a]);
+            for (int a = 0; a < 3; ++a) {
+                float w[VPT];
+#pragma unroll
+                for (int j = 0; j < VPT; ++j) w[j] = qv[j][i][a];
+                stv<VPT>(Xout + (3 * i + a) * tp.plane_w + o, w);
+            }
     } else {
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if (nb + j < tp.ns)
+        for (int j = 0; j < VPT; ++j)
+            if (nb + j < tp.ns && !((need >> j) & 1u))
 #pragma unroll
                 for (int i = 0; i < K - 1; ++i)
 #pragma unroll
@@ -398,18 +477,20 @@ __device__ __forceinline__ void stage_b_quad(const TiledSmem<K, R, NT> &sm, cons
     }
 }
 
-template <int K, int R, int NT>
-__global__ void __launch_bounds__(TileShape<K, R, NT>::THREADS, 1)
+template <int K, int R, int NT, int VPT>
+__global__ void __launch_bounds__(TileShape<K, R, NT, VPT>::THREADS, 1)
     fused_tiled_kernel(const __grid_constant__ CUtensorMap tm_xi, const __grid_constant__ CUtensorMap tm_v,
                        const __grid_constant__ CUtensorMap tm_u, TiledParams tp, float *__restrict__ Xout,
                        float *__restrict__ Vout, PhaseParams<K> pp, float tau2, DykstraThresholds thr, float *dq,
                        int *err)
 {
-    using S = TileShape<K, R, NT>;
-    using T = TiledSmem<K, R, NT>;
-    extern __shared__ uint8_t smem_raw[];
+    using S = TileShape<K, R, NT, VPT>;
+    using T = TiledSmem<K, R, NT, VPT>;
+    extern __shared__ __align__(128) uint8_t smem_raw[];
     T sm;
-    sm.base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    // align to 128 bytes by pointer arithmetic on the shared array itself, so
+    // that the compiler keeps every access a shared-memory access
+    sm.base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
 
     const int4 wk = tp.work[blockIdx.x];
     const int r0 = wk.x, n0 = wk.y, ca = wk.z, cb = wk.w;
@@ -421,11 +502,23 @@ __global__ void __launch_bounds__(TileShape<K, R, NT>::THREADS, 1)
     if (tid == 0) {
         for (int i = 0; i < S::D; ++i) {
             mbar_init(sm.full(i), 1);
-            mbar_init(sm.ready(i), S::MAIN_WARPS + 1);
-            mbar_init(sm.empty(i), S::MAIN_WARPS + 1);
+            mbar_init(sm.ready(i), S::MAIN_WARPS + S::HALO_WARPS);
+            mbar_init(sm.empty(i), S::MAIN_WARPS + S::HALO_WARPS);
         }
         *abort = 0;
         mbar_fence_init();
+    }
+    for (int i = tid; i <= P + 1; i += blockDim.x) {
+        const int c = ca - 1 + i;
+        sm.cols()[i] = (c >= tp.col_begin && c < tp.col_end) ? tp.cols[c] : make_int4(0, 0, 0, 0);
+    }
+    {  // Vbar planes start as zeros: a missing neighbour's value is multiplied by 0, so it must be finite
+        float *vb = sm.vb_plane(0);
+        for (int i = tid; i < S::D * S::V_SLOT / 4; i += blockDim.x) vb[i] = 0.0f;
+    }
+    if (ca - 1 < tp.col_begin) {  // no plane before the first column: its Xi slot reads as zeros
+        float *x0 = sm.xi_slot(0);
+        for (int i = tid; i < S::XI_BYTES / 4; i += blockDim.x) x0[i] = 0.0f;
     }
     __syncthreads();
 
@@ -435,58 +528,78 @@ __global__ void __launch_bounds__(TileShape<K, R, NT>::THREADS, 1)
             tma_prefetch_desc(&tm_xi);
             tma_prefetch_desc(&tm_v);
             tma_prefetch_desc(&tm_u);
+            // slot and phase parity of ring position p; waits for the release
+            // of the plane D positions back in the same slot
+            int slot = 0;
+            uint32_t ph = 0;
             for (int p = 0; p <= P; ++p) {
-                if (p >= S::D && !mbar_wait_thread(sm.empty(p - S::D), T::parity(p - S::D), abort)) break;
+                if (p >= S::D && !mbar_wait_thread(sm.empty(slot), ph ^ 1u, abort)) break;
                 const int c = ca - 1 + p;
                 if (p == 0 && c < tp.col_begin) {  // no plane before the first column
                     mbar_arrive(sm.full(0));
-                    continue;
+                } else {
+                    const int4 ci = sm.cols()[p];
+                    const int line = ci.x + (r0 - 1 - ci.y);  // line of row r0-1 in column c
+                    const bool xi_only = p == 0;
+                    mbar_arrive_expect_tx(sm.full(slot),
+                                          S::XI_BYTES + (xi_only ? 0u : (uint32_t)(S::V_BYTES + S::U_BYTES)));
+                    tma_load_3d(sm.xi_slot(slot), &tm_xi, sm.full(slot), n0 - 4, line, 0);
+                    if (!xi_only) {
+                        tma_load_3d(sm.v_slot(slot), &tm_v, sm.full(slot), n0, line + 1, 0);
+                        tma_load_2d(sm.u_slot(slot), &tm_u, sm.full(slot), tp.u_x0 + n0, line + 1);
+                    }
                 }
-                const int4 ci = tp.cols[c];
-                const int line = ci.x + (r0 - 1 - ci.y);  // line of row r0-1 in column c
-                const bool xi_only = p == 0;
-                mbar_arrive_expect_tx(sm.full(p),
-                                      S::XI_BYTES + (xi_only ? 0u : (uint32_t)(S::V_BYTES + S::U_BYTES)));
-                tma_load_3d(sm.xi_slot(p), &tm_xi, sm.full(p), n0 - 4, line, 0);
-                if (!xi_only) {
-                    tma_load_3d(sm.v_slot(p), &tm_v, sm.full(p), n0, line + 1, 0);
-                    tma_load_2d(sm.u_slot(p), &tm_u, sm.full(p), tp.u_x0 + n0, line + 1);
-                }
+                if (++slot == S::D) slot = 0, ph ^= 1u;
             }
         }
     } else {
         const bool is_main = warp < S::MAIN_WARPS;
+        const int hq = tid - S::MAIN;  // chunk of the halo row (halo warps)
         const int rr = is_main ? tid / S::Q : R;
-        const int q = is_main ? tid % S::Q : lane;
-        const bool quad_a = is_main || lane < S::Q;
-        const bool nhalo = !is_main && lane <= R;
+        const int q = is_main ? tid % S::Q : hq;
+        const bool chunk_a = is_main || hq < S::Q;
+        const bool nhalo = !is_main && hq <= R;  // lanes of the first halo warp
         bool ok = true;
+        int qhead = 0, qcount = 0;  // the warp's queue of voxels waiting for the Dykstra loop
+        // ring slots of positions p-1, p, p+1 and the barrier parities of p-1, p
+        int s_prev = S::D - 1, s_cur = 0, s_next = 1;
+        uint32_t ph_prev = 1, ph_cur = 0;
         for (int p = 0; p <= P && ok; ++p) {
-            const int c = ca - 1 + p;
             if (p > 0) {
                 if (p == 1) ok = mbar_wait_warp(sm.full(0), 0, abort);
-                if (ok) ok = mbar_wait_warp(sm.full(p), T::parity(p), abort);
+                if (ok) ok = mbar_wait_warp(sm.full(s_cur), ph_cur, abort);
                 if (!ok) break;
-                if (quad_a) stage_a_quad<K, R, NT>(sm, tp, pp, p, c, r0, rr, n0, q, is_main && c < cb, Vout, dqmax);
-                if (nhalo) stage_a_nhalo<K, R, NT>(sm, tp, pp, p, c, r0, lane, n0);
+                if (chunk_a)
+                    stage_a_chunk<K, R, NT, VPT>(sm, tp, pp, p, s_cur, s_prev, r0, rr, n0, q,
+                                                 is_main && ca - 1 + p < cb, Vout, dqmax);
+                if (nhalo) stage_a_nhalo<K, R, NT, VPT>(sm, tp, pp, p, s_cur, s_prev, r0, hq, n0);
             }
             __syncwarp();
-            if (lane == 0) mbar_arrive(sm.ready(p));
-            if (p == 0) continue;
-            if (is_main && p >= 2) {
-                // dual step at plane c-1 once every warp's Vbar of that plane is in
-                ok = mbar_wait_warp(sm.ready(p - 1), T::parity(p - 1), abort);
-                if (!ok) break;
-                stage_b_quad<K, R, NT>(sm, tp, p - 1, c - 1, r0, rr, n0, q, tau2, thr, Xout);
+            if (lane == 0) mbar_arrive(sm.ready(s_cur));
+            if (p > 0) {
+                if (is_main && p >= 2) {
+                    // dual step at position p-1 once every warp's Vbar of that plane is in
+                    ok = mbar_wait_warp(sm.ready(s_prev), ph_prev, abort);
+                    if (!ok) break;
+                    stage_b_chunk<K, R, NT, VPT>(sm, tp, p - 1, s_prev, s_cur, r0, rr, n0, q, tau2, thr, Xout, qhead,
+                                                 qcount);
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(sm.empty(s_prev));
             }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(sm.empty(p - 1));
+            s_prev = s_cur;
+            ph_prev = ph_cur;
+            s_cur = s_next;
+            if (s_cur == 0) ph_cur ^= 1u;
+            s_next = (s_next + 1 == S::D) ? 0 : s_next + 1;
         }
-        // the last column of the volume has no plane after it
-        if (ok && is_main && c_last == cb - 1 && P >= 1) {
-            ok = mbar_wait_warp(sm.ready(P), T::parity(P), abort);
-            if (ok) stage_b_quad<K, R, NT>(sm, tp, P, c_last, r0, rr, n0, q, tau2, thr, Xout);
+        // the last column of the volume has no plane after it (s_prev now holds position P)
+        if (ok && is_main && c_last == cb - 1) {
+            ok = mbar_wait_warp(sm.ready(s_prev), ph_prev, abort);
+            if (ok)
+                stage_b_chunk<K, R, NT, VPT>(sm, tp, P, s_prev, s_cur, r0, rr, n0, q, tau2, thr, Xout, qhead, qcount);
         }
+        if (ok && is_main && qcount > 0) drain_queue<K, R, NT, VPT>(sm.queue(warp), qhead, qcount, tp, thr, Xout);
     }
     __syncthreads();
     if (tid == 0 && *abort) atomicExch(err, 1);

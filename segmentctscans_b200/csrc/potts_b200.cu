@@ -382,33 +382,38 @@ int encode_map(CUtensorMap *m, const float *base, int rank, const uint64_t *dims
 }
 
 struct TileChoice {
-    int rows, slices, segment;
+    int rows, slices, vpt, segment;
 };
 
-// Tile shapes compiled per K (rows x slices); the first entry is the default.
+// Tile shapes compiled per K (rows x slices x voxels per thread); the first
+// entry is the default.
 template <int K>
 struct TileShapes;
-template <> struct TileShapes<2> { static constexpr int n = 2; static constexpr int r[n] = {8, 8}, t[n] = {128, 64}; };
-template <> struct TileShapes<3> { static constexpr int n = 4; static constexpr int r[n] = {8, 8, 16, 4}, t[n] = {128, 64, 64, 128}; };
-template <> struct TileShapes<4> { static constexpr int n = 2; static constexpr int r[n] = {8, 4}, t[n] = {64, 128}; };
-template <> struct TileShapes<5> { static constexpr int n = 1; static constexpr int r[n] = {4}, t[n] = {64}; };
-template <> struct TileShapes<6> { static constexpr int n = 1; static constexpr int r[n] = {4}, t[n] = {64}; };
+template <> struct TileShapes<2> { static constexpr int n = 2; static constexpr int r[n] = {8, 8}, t[n] = {128, 64}, v[n] = {2, 4}; };
+template <> struct TileShapes<3> { static constexpr int n = 4; static constexpr int r[n] = {8, 8, 16, 8}, t[n] = {128, 128, 64, 64}, v[n] = {2, 4, 4, 2}; };
+template <> struct TileShapes<4> { static constexpr int n = 2; static constexpr int r[n] = {8, 4}, t[n] = {64, 128}, v[n] = {4, 4}; };
+template <> struct TileShapes<5> { static constexpr int n = 1; static constexpr int r[n] = {4}, t[n] = {64}, v[n] = {4}; };
+template <> struct TileShapes<6> { static constexpr int n = 1; static constexpr int r[n] = {4}, t[n] = {64}, v[n] = {4}; };
 
 template <int K>
 int choose_tile(const potts_options &o, TileChoice *tc)
 {
     tc->rows = TileShapes<K>::r[0];
     tc->slices = TileShapes<K>::t[0];
+    tc->vpt = TileShapes<K>::v[0];
     tc->segment = o.segment_cols > 0 ? o.segment_cols : 32;
-    if (o.tile_rows > 0 || o.tile_slices > 0) {
+    if (tc->segment > 64) return fail(POTTS_EINVAL, "segment_cols must be <= 64");
+    if (o.tile_rows > 0 || o.tile_slices > 0 || o.tile_vpt > 0) {
         for (int i = 0; i < TileShapes<K>::n; ++i)
             if ((o.tile_rows <= 0 || o.tile_rows == TileShapes<K>::r[i]) &&
-                (o.tile_slices <= 0 || o.tile_slices == TileShapes<K>::t[i])) {
+                (o.tile_slices <= 0 || o.tile_slices == TileShapes<K>::t[i]) &&
+                (o.tile_vpt <= 0 || o.tile_vpt == TileShapes<K>::v[i])) {
                 tc->rows = TileShapes<K>::r[i];
                 tc->slices = TileShapes<K>::t[i];
+                tc->vpt = TileShapes<K>::v[i];
                 return POTTS_OK;
             }
-        return fail(POTTS_EINVAL, "tile_rows x tile_slices is not a compiled tile shape for this K");
+        return fail(POTTS_EINVAL, "tile_rows x tile_slices x tile_vpt is not a compiled tile shape for this K");
     }
     return POTTS_OK;
 }
@@ -482,19 +487,19 @@ struct FusedPlan {
     TileChoice tile{};
 };
 
-template <int K, int R, int NT>
+template <int K, int R, int NT, int VPT>
 int launch_tiled_shape(potts_context *ctx, const FusedPlan &fp, int in, float *Xout, float *Vout,
                        const PhaseParams<K> &pp, float tau2, float *dq)
 {
-    using S = potts::TileShape<K, R, NT>;
+    using S = potts::TileShape<K, R, NT, VPT>;
     static bool attr_set = false;
     if (!attr_set) {
-        POTTS_CUDA(cudaFuncSetAttribute(potts::fused_tiled_kernel<K, R, NT>,
+        POTTS_CUDA(cudaFuncSetAttribute(potts::fused_tiled_kernel<K, R, NT, VPT>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM_ALLOC));
         attr_set = true;
     }
     if (fp.n_work == 0) return POTTS_OK;
-    potts::fused_tiled_kernel<K, R, NT><<<fp.n_work, S::THREADS, S::SMEM_ALLOC, ctx->stream>>>(
+    potts::fused_tiled_kernel<K, R, NT, VPT><<<fp.n_work, S::THREADS, S::SMEM_ALLOC, ctx->stream>>>(
         fp.xi[in], fp.v[in], fp.u, fp.tp, Xout, Vout, pp, tau2, ctx->thr, dq, (int *)ctx->err.p);
     POTTS_CUDA(cudaGetLastError());
     return POTTS_OK;
@@ -505,9 +510,9 @@ int launch_tiled(potts_context *ctx, const FusedPlan &fp, int in, float *Xout, f
                  float tau2, float *dq)
 {
     if constexpr (I < TileShapes<K>::n) {
-        constexpr int R = TileShapes<K>::r[I], NT = TileShapes<K>::t[I];
-        if (fp.tile.rows == R && fp.tile.slices == NT)
-            return launch_tiled_shape<K, R, NT>(ctx, fp, in, Xout, Vout, pp, tau2, dq);
+        constexpr int R = TileShapes<K>::r[I], NT = TileShapes<K>::t[I], VPT = TileShapes<K>::v[I];
+        if (fp.tile.rows == R && fp.tile.slices == NT && fp.tile.vpt == VPT)
+            return launch_tiled_shape<K, R, NT, VPT>(ctx, fp, in, Xout, Vout, pp, tau2, dq);
         return launch_tiled<K, I + 1>(ctx, fp, in, Xout, Vout, pp, tau2, dq);
     } else {
         return fail(POTTS_EINVAL, "no compiled tile shape matches");
@@ -519,6 +524,8 @@ int prepare_fused(potts_context *ctx, const Geometry &g, const float *const xi[2
                   const float *d_u, const potts_options &o, FusedPlan *fp)
 {
     POTTS_TRY(choose_tile<K>(o, &fp->tile));
+    if (g.plane_w >= (int64_t(1) << 31))
+        return fail(POTTS_EINVAL, "a state plane of 2^31 voxels or more needs slabs (set slab_w)");
     const int R = fp->tile.rows, NT = fp->tile.slices;
     POTTS_TRY(plan_tiles(ctx, g.ns, fp->tile));
     fp->n_work = ctx->n_work;
@@ -597,6 +604,9 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
         // Fused schedule: a dual step gives Xi^1 from V^0 (= Vbar^0); launch m
         // (m = 1 .. iters-1) turns (Xi^m, V^{m-1}) into (Xi^{m+1}, V^m); a final
         // primal step gives V^iters from Xi^iters.
+        // the tiled kernel reads (and multiplies by zero) padding and stale
+        // neighbours: keep all of the state finite
+        POTTS_CUDA(cudaMemsetAsync(st.xi[0], 0, sizeof(float) * 8 * (K - 1) * (size_t)g.plane_w, s));
         FusedPlan fp;
         const float *xs[2] = {st.xi[0], st.xi[1]}, *vs[2] = {st.v[0], st.v[1]};
         if (iters > 1) POTTS_TRY(prepare_fused<K>(ctx, g, xs, vs, d_u, o, &fp));
@@ -761,7 +771,7 @@ int check_params(int K, const float *ci, float lam, float tau1, float tau2, int 
         return fail(POTTS_EINVAL, "unknown variant");
     if (o.storage != POTTS_STORE_F32) return fail(POTTS_EINVAL, "unknown storage");
     if (o.gap_every < 0 || o.slab_w < 0) return fail(POTTS_EINVAL, "gap_every and slab_w must be >= 0");
-    if (o.tile_rows < 0 || o.tile_slices < 0 || o.segment_cols < 0)
+    if (o.tile_rows < 0 || o.tile_slices < 0 || o.segment_cols < 0 || o.tile_vpt < 0)
         return fail(POTTS_EINVAL, "tile options must be >= 0");
     return POTTS_OK;
 }
@@ -836,6 +846,7 @@ void potts_default_options(potts_options *o)
     o->tile_rows = 0;
     o->tile_slices = 0;
     o->segment_cols = 0;
+    o->tile_vpt = 0;
 }
 
 const char *potts_status_string(int s)

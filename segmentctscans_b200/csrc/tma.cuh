@@ -42,22 +42,40 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
+// try_wait that may suspend the thread for up to `ns` nanoseconds before
+// reporting that the phase is still incomplete (fewer polling instructions).
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t *bar, uint32_t parity, uint32_t ns)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
+
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
-// Waits for phase `parity` of the barrier with an iteration limit (each
-// try_wait suspends for a bounded hardware interval).  Gives up early when
-// *abort is set by another warp, and sets it when it runs out of tries.
-// Warp-uniform: every lane of the calling warp must call it; all get the same
-// answer.
+// Waits for phase `parity` of the barrier: at most kWaitTries try_waits that
+// each suspend the thread for up to kWaitSleepNs (about 2 s in all).  Gives up
+// early when *abort is set by another warp, and sets it when it runs out of
+// tries.  Warp-uniform: every lane of the calling warp must call it; all get
+// the same answer.
+constexpr int kWaitTries = 2000;
+constexpr uint32_t kWaitSleepNs = 1000000;
+
 __device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity, volatile int *abort)
 {
-    bool done = false;
-    for (int i = 0; i < (1 << 22) && !done; ++i) {
-        done = mbar_try_wait(bar, parity);
-        if (!done && *abort) break;
+    bool done = mbar_try_wait(bar, parity);
+    for (int i = 0; i < kWaitTries && !done; ++i) {
+        if (*abort) break;
+        done = mbar_try_wait_sleep(bar, parity, kWaitSleepNs);
     }
     if (!done) *abort = 1;
     return __all_sync(0xffffffffu, done) != 0;
@@ -66,9 +84,10 @@ __device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity, v
 // Single-thread form (for the producer lane).
 __device__ __forceinline__ bool mbar_wait_thread(uint64_t *bar, uint32_t parity, volatile int *abort)
 {
-    for (int i = 0; i < (1 << 22); ++i) {
-        if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_try_wait(bar, parity)) return true;
+    for (int i = 0; i < kWaitTries; ++i) {
         if (*abort) return false;
+        if (mbar_try_wait_sleep(bar, parity, kWaitSleepNs)) return true;
     }
     *abort = 1;
     return false;

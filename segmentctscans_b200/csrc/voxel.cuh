@@ -49,6 +49,7 @@ __device__ __forceinline__ void dual_build_q(float (&q)[K][3], const float (&xi)
 {
     float vk = 1.0f, vkn = 1.0f, vkr = 1.0f, vkc = 1.0f;
     float xk0 = 0.0f, xk1 = 0.0f, xk2 = 0.0f;
+    const float fhn = hn ? 1.0f : 0.0f, fhr = hr ? 1.0f : 0.0f, fhc = hc ? 1.0f : 0.0f;
 #pragma unroll
     for (int i = 0; i < K; ++i) {
         float vi, wn, wr, wc, x0, x1, x2;
@@ -76,9 +77,11 @@ __device__ __forceinline__ void dual_build_q(float (&q)[K][3], const float (&xi)
             x1 = xk1;
             x2 = xk2;
         }
-        const float g0 = hn ? (wn - vi) : 0.0f;
-        const float g1 = hr ? (wr - vi) : 0.0f;
-        const float g2 = hc ? (wc - vi) : 0.0f;
+        // the difference to a missing neighbour is multiplied by 0 (its value
+        // must be finite), which equals the reference's skipped term
+        const float g0 = fhn * (wn - vi);
+        const float g1 = fhr * (wr - vi);
+        const float g2 = fhc * (wc - vi);
         q[i][0] = fmaf(g0, tau2, x0);
         q[i][1] = fmaf(g1, tau2, x1);
         q[i][2] = fmaf(g2, tau2, x2);
@@ -230,6 +233,20 @@ __device__ __forceinline__ float div_small(float x, int j)
     }
 }
 
+// u > RN(x / j) for j in 1..6, without a division in the common case.
+// t = fma(j, u, -x) carries the exact sign of j*u - x.  When |t| exceeds
+// max(|u| 2^-19, 2^-120), |u - x/j| is larger than the spacing of floats
+// around u, so RN(x/j) lies strictly on the same side of u as x/j and the sign
+// of t decides; otherwise the quotient is computed and compared.
+__device__ __forceinline__ bool gt_div_small(float u, float x, int j)
+{
+    if (j == 1 || j == 2 || j == 4) return u > div_small(x, j);
+    const float t = fmaf((float)j, u, -x);
+    const float margin = fmaxf(fabsf(u) * 0x1p-19f, 0x1p-120f);
+    if (fabsf(t) > margin) return t > 0.0f;
+    return u > __fdiv_rn(x, (float)j);
+}
+
 // Projection onto the simplex (potts-model/potts-min-partition.cpp:292-347).
 template <int K>
 __device__ __forceinline__ void project_simplex(float (&q)[K])
@@ -243,18 +260,14 @@ __device__ __forceinline__ void project_simplex(float (&q)[K])
 #pragma unroll
     for (int i = 0; i < K; ++i) {
         sum = sum + u[i];
-        const float theta = div_small(sum - 1.0f, i + 1);
-        if (u[i] > theta) {
+        if (gt_div_small(u[i], sum - 1.0f, i + 1)) {  // u[i] > (sum - 1) / (i + 1)
             rho = i + 1;
             rho_sum = sum;
         }
     }
     const float theta = div_small(rho_sum - 1.0f, rho);
 #pragma unroll
-    for (int i = 0; i < K; ++i) {
-        const float t = q[i] - theta;
-        q[i] = (t < 0.0f) ? 0.0f : t;
-    }
+    for (int i = 0; i < K; ++i) q[i] = fmaxf(q[i] - theta, 0.0f);  // max(q - theta, 0); -0 vs +0 aside
 }
 
 // ---------------------------------------------------------------------------
@@ -274,6 +287,8 @@ __device__ __forceinline__ float primal_voxel(float (&vnew)[K - 1], float (&vbar
     float q[K], vv[K];
     float vk = 1.0f;
     float xk0 = 0.0f, xk1 = 0.0f, xk2 = 0.0f, xkn = 0.0f, xkr = 0.0f, xkc = 0.0f;
+    const float fpn = pn ? 1.0f : 0.0f, fhn = hn ? 1.0f : 0.0f, fpr = pr ? 1.0f : 0.0f;
+    const float fhr = hr ? 1.0f : 0.0f, fpc = pc ? 1.0f : 0.0f, fhc = hc ? 1.0f : 0.0f;
 #pragma unroll
     for (int i = 0; i < K; ++i) {
         float x0, x1, x2, wn, wr, wc, vi;
@@ -301,13 +316,16 @@ __device__ __forceinline__ float primal_voxel(float (&vnew)[K - 1], float (&vbar
             wc = xkc;
             vi = vk;
         }
-        float div = 0.0f;
-        if (pn) div = div - wn;
-        if (hn) div = div + x0;
-        if (pr) div = div - wr;
-        if (hr) div = div + x1;
-        if (pc) div = div - wc;
-        if (hc) div = div + x2;
+        // div = 0; div -= wn if pn; div += x0 if hn; ... in this order.  A term
+        // whose neighbour is missing is multiplied by 0 instead of skipped,
+        // which gives the same value as long as the skipped operand is finite
+        // (callers pass 0 or finite stale state for missing neighbours).
+        float div = fmaf(-fpn, wn, 0.0f);
+        div = fmaf(fhn, x0, div);
+        div = fmaf(-fpr, wr, div);
+        div = fmaf(fhr, x1, div);
+        div = fmaf(-fpc, wc, div);
+        div = fmaf(fhc, x2, div);
         vv[i] = vi;
         const float dl = u - c[i];
         const float d2 = dl * dl;
@@ -325,6 +343,162 @@ __device__ __forceinline__ float primal_voxel(float (&vnew)[K - 1], float (&vbar
     for (int i = 0; i < K - 1; ++i) {
         vnew[i] = q[i];
         vbar[i] = 2.0f * q[i] - vv[i];
+    }
+    return dq;
+}
+
+// ---------------------------------------------------------------------------
+// Two voxels at once (consecutive slices of one line) with Blackwell's paired
+// FP32 instructions.  Each lane of a pair goes through exactly the operations
+// of primal_voxel / dual_build_q / dual_first_sweep_is_identity above, in the
+// same order and with the same rounding, so the results are the same bits.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+template <int K>
+__device__ __forceinline__ void dual_build_q_pair(float2 (&q)[K][3], const float2 (&xi)[3 * (K - 1)],
+                                                  const float2 (&vb)[K - 1], const float2 (&vbn)[K - 1],
+                                                  const float2 (&vbr)[K - 1], const float2 (&vbc)[K - 1], float2 fhn,
+                                                  float2 fhr, float2 fhc, float tau2)
+{
+    float2 vk = f2(1.0f), vkn = f2(1.0f), vkr = f2(1.0f), vkc = f2(1.0f);
+    float2 xk0 = f2(0.0f), xk1 = f2(0.0f), xk2 = f2(0.0f);
+    const float2 t2 = f2(tau2);
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        float2 vi, wn, wr, wc, x0, x1, x2;
+        if (i < K - 1) {
+            vi = vb[i];
+            vk = sub2(vk, vi);
+            wn = vbn[i];
+            vkn = sub2(vkn, wn);
+            wr = vbr[i];
+            vkr = sub2(vkr, wr);
+            wc = vbc[i];
+            vkc = sub2(vkc, wc);
+            x0 = xi[3 * i];
+            x1 = xi[3 * i + 1];
+            x2 = xi[3 * i + 2];
+            xk0 = sub2(xk0, x0);
+            xk1 = sub2(xk1, x1);
+            xk2 = sub2(xk2, x2);
+        } else {
+            vi = vk;
+            wn = vkn;
+            wr = vkr;
+            wc = vkc;
+            x0 = xk0;
+            x1 = xk1;
+            x2 = xk2;
+        }
+        q[i][0] = fma2(mul2(fhn, sub2(wn, vi)), t2, x0);
+        q[i][1] = fma2(mul2(fhr, sub2(wr, vi)), t2, x1);
+        q[i][2] = fma2(mul2(fhc, sub2(wc, vi)), t2, x2);
+    }
+}
+
+// bit j set: the first sweep of voxel j is not the identity (see
+// dual_first_sweep_is_identity)
+template <int K>
+__device__ __forceinline__ unsigned dual_needs_loop_pair(const float2 (&q)[K][3], DykstraThresholds thr)
+{
+    bool l0 = false, l1 = false;
+#pragma unroll
+    for (int i1 = 0; i1 < K - 1; ++i1) {
+#pragma unroll
+        for (int i2 = i1 + 1; i2 < K; ++i2) {
+            const float2 a0 = sub2(q[i2][0], q[i1][0]);
+            const float2 a1 = sub2(q[i2][1], q[i1][1]);
+            const float2 a2 = sub2(q[i2][2], q[i1][2]);
+            float2 s = mul2(a0, a0);
+            s = fma2(a1, a1, s);
+            s = fma2(a2, a2, s);
+            l0 |= (s.x > thr.len_gt_one);
+            l1 |= (s.y > thr.len_gt_one);
+        }
+    }
+    return (l0 ? 1u : 0u) | (l1 ? 2u : 0u);
+}
+
+template <int K>
+__device__ __forceinline__ float2 primal_pair(float2 (&vnew)[K - 1], float2 (&vbar)[K - 1],
+                                              const float2 (&v)[K - 1], const float2 (&xi)[3 * (K - 1)],
+                                              const float2 (&xin)[K - 1], const float2 (&xir)[K - 1],
+                                              const float2 (&xic)[K - 1], float2 fpn, float2 fhn, float2 fpr,
+                                              float2 fhr, float2 fpc, float2 fhc, float2 u, const float (&c)[K],
+                                              float lam, float tau1)
+{
+    float2 q[K], vv[K];
+    float2 vk = f2(1.0f);
+    float2 xk0 = f2(0.0f), xk1 = f2(0.0f), xk2 = f2(0.0f), xkn = f2(0.0f), xkr = f2(0.0f), xkc = f2(0.0f);
+    const float2 mfpn = f2(-fpn.x, -fpn.y), mfpr = f2(-fpr.x, -fpr.y), mfpc = f2(-fpc.x, -fpc.y);
+    const float2 mlam = f2(-lam), t1 = f2(tau1);
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        float2 x0, x1, x2, wn, wr, wc, vi;
+        if (i < K - 1) {
+            x0 = xi[3 * i];
+            x1 = xi[3 * i + 1];
+            x2 = xi[3 * i + 2];
+            xk0 = sub2(xk0, x0);
+            xk1 = sub2(xk1, x1);
+            xk2 = sub2(xk2, x2);
+            wn = xin[i];
+            xkn = sub2(xkn, wn);
+            wr = xir[i];
+            xkr = sub2(xkr, wr);
+            wc = xic[i];
+            xkc = sub2(xkc, wc);
+            vi = v[i];
+            vk = sub2(vk, vi);
+        } else {
+            x0 = xk0;
+            x1 = xk1;
+            x2 = xk2;
+            wn = xkn;
+            wr = xkr;
+            wc = xkc;
+            vi = vk;
+        }
+        float2 div = fma2(mfpn, wn, f2(0.0f));
+        div = fma2(fhn, x0, div);
+        div = fma2(mfpr, wr, div);
+        div = fma2(fhr, x1, div);
+        div = fma2(mfpc, wc, div);
+        div = fma2(fhc, x2, div);
+        vv[i] = vi;
+        const float2 dl = sub2(u, f2(c[i]));
+        const float2 d2 = mul2(dl, dl);
+        const float2 w = fma2(mlam, d2, div);
+        q[i] = fma2(t1, w, vi);
+    }
+    // simplex projection of each voxel (the sort and the threshold search are
+    // per voxel; the final shift is paired)
+    float qa[K], qb[K];
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        qa[i] = q[i].x;
+        qb[i] = q[i].y;
+    }
+    project_simplex<K>(qa);
+    project_simplex<K>(qb);
+#pragma unroll
+    for (int i = 0; i < K; ++i) q[i] = f2(qa[i], qb[i]);
+    float2 dq = f2(0.0f);
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        const float2 e = sub2(q[i], vv[i]);
+        dq = (i == 0) ? mul2(e, e) : fma2(e, e, dq);
+    }
+#pragma unroll
+    for (int i = 0; i < K - 1; ++i) {
+        vnew[i] = q[i];
+        vbar[i] = sub2(mul2(f2(2.0f), q[i]), vv[i]);
     }
     return dq;
 }

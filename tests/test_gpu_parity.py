@@ -183,8 +183,8 @@ def test_errors_are_reported(cuda_device):
         assert res.span == m.span
 
 
-TILE_SHAPES = {2: [(8, 128), (8, 64)], 3: [(8, 128), (8, 64), (16, 64), (4, 128)], 4: [(8, 64), (4, 128)],
-               5: [(4, 64)], 6: [(4, 64)]}
+TILE_SHAPES = {2: [(8, 128, 2), (8, 64, 4)], 3: [(8, 128, 2), (8, 128, 4), (16, 64, 4), (8, 64, 2)],
+               4: [(8, 64, 4), (4, 128, 4)], 5: [(4, 64, 4)], 6: [(4, 64, 4)]}
 
 
 @pytest.mark.parametrize("K", [2, 3, 4, 5, 6])
@@ -192,10 +192,10 @@ def test_every_tile_shape_and_segment_length(cuda_device, oracle_mod, K):
     """Partial n-tiles (n = 150), the n/row halos, segment starts and ends (1, 3 and 32 columns)."""
     m, u, ci = random_volume(150, 37, 35, 16.3, K, seed=20 + K)
     o = oracle_mod.solve(m, u, ci, 30.0, TAU, TAU, 9, precision="f32")
-    for rows, slices in TILE_SHAPES[K]:
-        for seg in (1, 3, 32):
+    for rows, slices, vpt in TILE_SHAPES[K]:
+        for seg in (1, 3, 32, 64):
             g = gpu_solve(m, u, ci, 30.0, TAU, TAU, 9, variant=0, tile_rows=rows, tile_slices=slices,
-                          segment_cols=seg)
+                          tile_vpt=vpt, segment_cols=seg)
             assert_same(m, g, o)
 
 
@@ -213,3 +213,5 @@ def test_unknown_tile_shape_is_rejected(cuda_device):
     with pytest.raises(PottsError) as e:
         gpu_solve(m, u, ci, 30.0, TAU, TAU, 5, variant=0, tile_rows=5, tile_slices=40)
     assert e.value.status == 1
+    with pytest.raises(PottsError):
+        gpu_solve(m, u, ci, 30.0, TAU, TAU, 5, variant=0, segment_cols=65)
