@@ -77,7 +77,7 @@ typedef struct potts_options {
     int sync_monitor; /* 1: reference behaviour, read the monitor back and sync after every iteration */
     int tile_rows;    /* fused form: rows per tile (0 = default for K) */
     int tile_slices;  /* fused form: slices (n) per tile (0 = default for K) */
-    int segment_cols; /* fused form: columns one tile marches over (0 = 32, at most 64) */
+    int segment_cols; /* fused form: columns one tile marches over (0 = 64, at most 64) */
     int tile_vpt;     /* fused form: consecutive slices per thread, 2 or 4 (0 = default for K) */
 } potts_options;
 

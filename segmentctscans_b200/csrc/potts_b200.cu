@@ -390,7 +390,7 @@ struct TileChoice {
 template <int K>
 struct TileShapes;
 template <> struct TileShapes<2> { static constexpr int n = 2; static constexpr int r[n] = {8, 8}, t[n] = {128, 64}, v[n] = {2, 4}; };
-template <> struct TileShapes<3> { static constexpr int n = 4; static constexpr int r[n] = {8, 8, 16, 8}, t[n] = {128, 128, 64, 64}, v[n] = {2, 4, 4, 2}; };
+template <> struct TileShapes<3> { static constexpr int n = 4; static constexpr int r[n] = {16, 8, 8, 8}, t[n] = {64, 128, 64, 128}, v[n] = {2, 2, 2, 4}; };
 template <> struct TileShapes<4> { static constexpr int n = 2; static constexpr int r[n] = {8, 4}, t[n] = {64, 128}, v[n] = {4, 4}; };
 template <> struct TileShapes<5> { static constexpr int n = 1; static constexpr int r[n] = {4}, t[n] = {64}, v[n] = {4}; };
 template <> struct TileShapes<6> { static constexpr int n = 1; static constexpr int r[n] = {4}, t[n] = {64}, v[n] = {4}; };
@@ -401,7 +401,7 @@ int choose_tile(const potts_options &o, TileChoice *tc)
     tc->rows = TileShapes<K>::r[0];
     tc->slices = TileShapes<K>::t[0];
     tc->vpt = TileShapes<K>::v[0];
-    tc->segment = o.segment_cols > 0 ? o.segment_cols : 32;
+    tc->segment = o.segment_cols > 0 ? o.segment_cols : 64;
     if (tc->segment > 64) return fail(POTTS_EINVAL, "segment_cols must be <= 64");
     if (o.tile_rows > 0 || o.tile_slices > 0 || o.tile_vpt > 0) {
         for (int i = 0; i < TileShapes<K>::n; ++i)
@@ -465,11 +465,12 @@ int plan_tiles(potts_context *ctx, int ns, const TileChoice &tc)
             }
         }
     }
-    // items sharing columns run together, so halo rows of neighbouring tiles meet in L2
+    // items sharing columns run together (halo rows of neighbouring tiles meet
+    // in L2), the slice tiles of the same rows side by side
     std::sort(items.begin(), items.end(), [](const Item &a, const Item &b) {
         if (a.ca != b.ca) return a.ca < b.ca;
-        if (a.n0 != b.n0) return a.n0 < b.n0;
-        return a.r0 < b.r0;
+        if (a.r0 != b.r0) return a.r0 < b.r0;
+        return a.n0 < b.n0;
     });
     std::vector<int4> work(std::max<size_t>(items.size(), 1));
     for (size_t i = 0; i < items.size(); ++i) work[i] = make_int4(items[i].r0, items[i].n0, items[i].ca, items[i].cb);
@@ -539,11 +540,12 @@ int prepare_fused(potts_context *ctx, const Geometry &g, const float *const xi[2
         const uint32_t bv[3] = {(uint32_t)(NT + 4), (uint32_t)(R + 1), (uint32_t)(K - 1)};
         POTTS_TRY(encode_map(&fp->v[b], v[b], 3, dv, sx, bv));
     }
-    // u: read in place when the slab starts on a 16-byte boundary, else staged
+    // u: read in place when the slab's slices start on a 16-byte boundary,
+    // else staged into a buffer with the state's stride
     const float *ubase = d_u;
     uint64_t ustride = (uint64_t)g.nstride_in;
     int ux0 = g.slab_start;
-    if (g.slab_start % 4 != 0) {
+    if (g.slab_start % 4 != 0 || reinterpret_cast<uintptr_t>(d_u) % 16 != 0) {
         POTTS_TRY(ensure(ctx, ctx->ustage, sizeof(float) * (size_t)g.plane_w));
         const int chunks = (g.ns + potts::kPlainThreads - 1) / potts::kPlainThreads;
         potts::stage_u_kernel<<<(unsigned)(g.n_lines * chunks), potts::kPlainThreads, 0, ctx->stream>>>(

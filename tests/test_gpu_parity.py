@@ -183,7 +183,7 @@ def test_errors_are_reported(cuda_device):
         assert res.span == m.span
 
 
-TILE_SHAPES = {2: [(8, 128, 2), (8, 64, 4)], 3: [(8, 128, 2), (8, 128, 4), (16, 64, 4), (8, 64, 2)],
+TILE_SHAPES = {2: [(8, 128, 2), (8, 64, 4)], 3: [(8, 128, 2), (16, 64, 2), (8, 64, 2), (8, 128, 4)],
                4: [(8, 64, 4), (4, 128, 4)], 5: [(4, 64, 4)], 6: [(4, 64, 4)]}
 
 
