@@ -160,6 +160,29 @@ int potts_solve_host(potts_context *ctx, const potts_mapping *map, const float *
                      float lambda, float tau1, float tau2, int iters, const potts_options *opts, float *h_res,
                      uint8_t *h_labels, potts_stats *stats);
 
+/*
+ * FP64 energies (lagrangian, dual, gap) of a state (V, Xi), with the same
+ * per-voxel terms as potts_stats.energy_trace, computed without allocating
+ * device memory.  No counterpart in the reference.  For callers that cannot
+ * call cudaMalloc (a host framework that owns the device memory pool, a
+ * process whose device memory is reserved up front, a loop that cannot afford
+ * an allocation's synchronisation).  Working memory is fixed, file-scope
+ * device memory of the library (POTTS_STATIC_MAX_COLS column entries and one
+ * partial sum per block, about 275 KB per GPU, held until the process exits).
+ * d_u, d_V (K-1 planes) and d_Xi (3(K-1) planes) are device arrays laid out
+ * with `map` (span = base[cols] per plane); h_out receives 3 doubles; the
+ * work runs on `stream` (a cudaStream_t, NULL = default stream) on the
+ * current device, and the call returns after the result is on the host.
+ * The first call on a device looks up the working memory's device address:
+ * make it before any stream capture.  Every call uses the same working
+ * memory, so calls that overlap on the GPU race; a call's working memory is
+ * fully rewritten before it is read.  Returns POTTS_EINVAL for more than
+ * POTTS_STATIC_MAX_COLS columns.
+ */
+#define POTTS_STATIC_MAX_COLS 16384
+int potts_energies_static(const potts_mapping *map, const float *d_u, int K, const float *ci, float lambda,
+                          const float *d_V, const float *d_Xi, void *stream, double *h_out);
+
 /* Mask constructor of layout_cylinder::mapping_storage (include/layout_cylinder.h:152-195):
  * fills start_row[cols] and base[cols+1], returns the span (base[cols]). */
 uint64_t potts_cylinder_mapping(uint32_t rows, uint32_t cols, double xc, double yc, double r, uint32_t nstride,

@@ -75,7 +75,9 @@ SIGNATURES = {
                                       ctypes.POINTER(_U32), ctypes.POINTER(_U32), ctypes.POINTER(_U32),
                                       ctypes.POINTER(_U32)]),
     "potts_get_stride": (_U32, [_U32]),
+    "potts_energies_static": (_I, [_MP, _P, _I, _FP, _F, _P, _P, _P, ctypes.POINTER(ctypes.c_double)]),
 }
+STATIC_MAX_COLS = 16384
 
 _lib = None
 

@@ -16,6 +16,10 @@
 #include "kernels_tiled.cuh"
 #include "voxel.cuh"
 
+// Sets the message potts_last_error() returns on this thread; used by the
+// library's other translation units.
+__attribute__((visibility("hidden"))) void potts_set_last_error(const std::string &msg);
+
 using potts::DykstraThresholds;
 using potts::Geometry;
 using potts::PhaseParams;
@@ -833,6 +837,8 @@ int context_init(int device, void *stream, bool use_stream, potts_context **out)
 }
 
 }  // namespace
+
+__attribute__((visibility("hidden"))) void potts_set_last_error(const std::string &msg) { g_last_error = msg; }
 
 extern "C" {
 
