@@ -13,8 +13,14 @@ Metric: in-mask voxel-iterations per second (Gvox-iter/s), whole job.
   e2e    the same solves through the host-buffer C-ABI call (pinned u in,
          ci[argmax] + label bytes out), copies inside the timed region
 Also: the roofline of the dominant kernel (the fused iteration) from the
-solver's own per-iteration device timing, and a CPU baseline (the FP64 oracle
-on this machine's cores, bounded sample).
+solver's own per-iteration device timing, a CPU baseline (the FP64 oracle on
+this machine's cores, bounded sample), and "storage": one solve each of the
+FP32 split (plain) form and of the bfloat16 / binary16 storage forms on the
+same input, with their speed and their label flips and V error against the
+FP32 solve (bit-identical to the FP32 plain form).
+
+--workload config2 runs the same volume with K = 4 (a fourth phase at
+4.6e-2 on 15% of the pores).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Under torchrun each rank solves its own phantom (weak scaling, no data-path
@@ -41,7 +47,8 @@ METRIC = "Potts PD Gvox-iter/s at k=3, %HBM peak; BF16-store vs FP32 at ≤1e-4 
 UNIT = "Gvox-iter/s"
 K_LABELS = 3
 LAMBDA = 30.0
-RADIUS = {"config1": 370.0, "config0": 60.0, "mid": 180.0}
+RADIUS = {"config1": 370.0, "config2": 370.0, "config0": 60.0, "mid": 180.0}
+STORE_BYTES = {"f32": 4, "bf16": 2, "f16": 2}
 
 
 def parse_args():
@@ -53,7 +60,11 @@ def parse_args():
     p.add_argument("--iters", type=int, default=1000)
     p.add_argument("--gap-every", type=int, default=50)
     p.add_argument("--variant", choices=["fused", "plain"], default="fused")
-    p.add_argument("--workload", choices=["config1", "config0", "mid"], default="config1",
+    p.add_argument("--storage", choices=["f32", "bf16", "f16"], default="f32",
+                   help="state storage of the timed solves")
+    p.add_argument("--no-storage-compare", action="store_true",
+                   help="skip the FP32-plain / BF16 / FP16 comparison solves")
+    p.add_argument("--workload", choices=["config1", "config2", "config0", "mid"], default="config1",
                    help="config1: 768x768x1024 r=370 (the benchmark); config0: 128^3 r=60; "
                         "mid: 384x384x256 r=180 (profiling size, state > L2)")
     p.add_argument("--no-e2e", action="store_true")
@@ -63,6 +74,8 @@ def parse_args():
     p.add_argument("--tile-slices", type=int, default=0, help="fused tile slices (0 = library default)")
     p.add_argument("--segment", type=int, default=0, help="columns per fused work item (0 = library default)")
     p.add_argument("--tile-vpt", type=int, default=0, help="fused slices per thread (0 = library default)")
+    p.add_argument("--prefetch", type=int, default=0,
+                   help="fused: planes of L2 prefetch ahead of the load ring (0 = library default, -1 = none)")
     return p.parse_args()
 
 
@@ -191,14 +204,16 @@ def profiled_traffic(variant: str) -> dict | None:
         return None
 
 
-def bytes_per_voxel_iter(variant: str, k: int = K_LABELS) -> int:
-    """Algorithmic DRAM bytes per in-mask voxel and iteration (FP32 state).
+def bytes_per_voxel_iter(variant: str, k: int = K_LABELS, storage: str = "f32") -> int:
+    """Algorithmic DRAM bytes per in-mask voxel and iteration (state values of
+    STORE_BYTES[storage] bytes, u always FP32).
     fused: Xi (3(K-1)) and V (K-1) read and written once, u read once;
     split: dual launch reads Vbar, Xi and writes Xi; primal launch reads Xi, V, u
            and writes V, Vbar."""
+    e = STORE_BYTES[storage]
     if variant == "fused":
-        return 4 * (8 * (k - 1) + 1)
-    return 4 * (13 * (k - 1) + 1)
+        return e * 8 * (k - 1) + 4
+    return e * 13 * (k - 1) + 4
 
 
 # ----------------------------------------------------------------------------- CPU baseline (oracle)
@@ -267,7 +282,7 @@ def run_ours(args, dist_: Dist) -> None:
     import torch
 
     from segmentctscans_b200 import potts
-    from segmentctscans_b200.phantom import config0_phantom, config1_phantom, make_phantom
+    from segmentctscans_b200.phantom import config0_phantom, config1_phantom, config2_phantom, make_phantom
 
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device")
@@ -277,11 +292,14 @@ def run_ours(args, dist_: Dist) -> None:
 
     if args.workload == "config1":
         ph = config1_phantom(seed=dist_.rank, device=dev)
+    elif args.workload == "config2":
+        ph = config2_phantom(seed=dist_.rank, device=dev)
     elif args.workload == "config0":
         ph = config0_phantom(seed=dist_.rank, device=dev)
     else:
         ph = make_phantom(256, 384, 384, 180.0, seed=dist_.rank, radius_range=(6.0, 30.0), noise=7e-3, device=dev)
     m, u, ci = ph.mapping, ph.u, ph.ci
+    k = len(ci)
     truth = ph.truth
     del ph
     torch.cuda.empty_cache()
@@ -294,12 +312,12 @@ def run_ours(args, dist_: Dist) -> None:
     lab = torch.empty(span, dtype=torch.uint8, device=dev)
 
     tile_opts = {"tile_rows": args.tile_rows, "tile_slices": args.tile_slices, "segment_cols": args.segment,
-                 "tile_vpt": args.tile_vpt}
+                 "tile_vpt": args.tile_vpt, "prefetch": args.prefetch}
 
     def step():
         return potts.solve_device(ctx, m, u.data_ptr(), ci, LAMBDA, tau, tau, args.iters, res_ptr=res.data_ptr(),
                                   labels_ptr=lab.data_ptr(), stats=True, variant=variant,
-                                  gap_every=args.gap_every, **tile_opts)
+                                  gap_every=args.gap_every, storage=args.storage, **tile_opts)
 
     for _ in range(args.warmup):
         step()
@@ -326,12 +344,12 @@ def run_ours(args, dist_: Dist) -> None:
     loop_ms = sum(s.loop_ms for s in stats)
     loop_launches = sum(s.loop_launches for s in stats)
     launch_s = loop_ms / 1000.0 / max(loop_launches, 1)
-    bpv = bytes_per_voxel_iter(args.variant)
+    bpv = bytes_per_voxel_iter(args.variant, k, args.storage)
     # the split form runs two launches per iteration
     per_launch_bytes = bpv * vox if args.variant == "fused" else bpv * vox / 2
     achieved = per_launch_bytes / launch_s / 1e9
     peaks = measured_peaks()
-    tr = profiled_traffic(args.variant)
+    tr = profiled_traffic(args.variant if args.storage == "f32" and k == 3 else None)
     traffic = tr["dram_bytes_per_voxel_iter"] * vox if tr else None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
@@ -357,7 +375,7 @@ def run_ours(args, dist_: Dist) -> None:
 
         def e2e_step():
             potts.solve_host(ctx, m, hu_np, ci, LAMBDA, tau, tau, args.iters, res=hres_np, labels=hlab_np,
-                             variant=variant, gap_every=args.gap_every, **tile_opts)
+                             variant=variant, gap_every=args.gap_every, storage=args.storage, **tile_opts)
 
         e2e_step()  # allocates the context's staging buffers
         torch.cuda.synchronize(dev)
@@ -376,6 +394,10 @@ def run_ours(args, dist_: Dist) -> None:
         e2e = {"value": vox_iters_all / te / 1e9, "unit": UNIT, "h2d_bytes_per_step": 4 * span,
                "d2h_bytes_per_step": 5 * span, "matches_device_run": same}
 
+    storage = None
+    if not args.no_storage_compare and args.variant == "fused" and args.storage == "f32":
+        storage = storage_compare(args, dist_, ctx, m, u, ci, tau, stream, dev, value)
+
     cpu = None
     if dist_.rank == 0 and dist_.world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_seconds)
@@ -385,20 +407,86 @@ def run_ours(args, dist_: Dist) -> None:
         out = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist_.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1000 * t_max / args.steps, 2), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"potts_k3_{m.rows}x{m.cols}x{m.n_images}_r{RADIUS[args.workload]:g}",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.storage == "f32" else f"f32 math, {args.storage} state",
+            "data": "synthetic",
+            "config": {"workload": f"potts_k{k}_{m.rows}x{m.cols}x{m.n_images}_r{RADIUS[args.workload]:g}",
                        "rows": m.rows, "cols": m.cols, "n": m.n_images, "radius": RADIUS[args.workload],
-                       "in_mask_voxels": vox, "k": K_LABELS, "lambda": LAMBDA, "tau": tau, "iters": args.iters,
-                       "gap_every": args.gap_every, "variant": args.variant, "storage": "f32",
+                       "in_mask_voxels": vox, "k": k, "lambda": LAMBDA, "tau": tau, "iters": args.iters,
+                       "gap_every": args.gap_every, "variant": args.variant, "storage": args.storage,
                        "tile": [args.tile_rows, args.tile_slices, args.tile_vpt, args.segment],
+                       "prefetch": args.prefetch,
                        "parallelism": f"replica x{dist_.world}" if dist_.world > 1 else "single",
                        "l2": "inputs larger than L2 (state ~30 GB per GPU)"},
             "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clk, "cpu_baseline": cpu,
+            "storage": storage,
             "quality": {"final_sqrt_max_dV2": last.dq_last, "energy_last": gap, "truth_agreement": round(agree, 5)},
         }
         print(json.dumps(out), flush=True)
     ctx.close()
     dist_.close()
+
+
+def storage_compare(args, dist_: Dist, ctx, m, u, ci, tau, stream, dev, fused_value: float) -> dict:
+    """One solve each of the FP32 split form and the 16-bit storage forms on the volume of the timed
+    solves; labels and V of each against the FP32 fused solve (bit-identical to the FP32 split form)."""
+    import torch
+
+    from segmentctscans_b200 import potts
+
+    k = len(ci)
+    span, vox = m.span, m.data_size
+    lab_ref = torch.empty(span, dtype=torch.uint8, device=dev)
+    lab = torch.empty(span, dtype=torch.uint8, device=dev)
+    v_ref = torch.empty((k - 1) * span, dtype=torch.float32, device=dev)
+    v = torch.empty((k - 1) * span, dtype=torch.float32, device=dev)
+
+    def solve(storage, variant, labels, V, iters):
+        return potts.solve_device(ctx, m, u.data_ptr(), ci, LAMBDA, tau, tau, iters, labels_ptr=labels.data_ptr(),
+                                  V_ptr=V.data_ptr(), stats=True, variant=variant, gap_every=args.gap_every,
+                                  storage=storage)
+
+    def timed(storage, variant, labels, V):
+        solve(storage, variant, labels, V, 2)  # allocations, module load
+        torch.cuda.synchronize(dev)
+        dist_.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = solve(storage, variant, labels, V, args.iters)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        t = dist_.reduce(e0.elapsed_time(e1) / 1000.0, "max")
+        value = dist_.reduce(float(vox) * args.iters, "sum") / t / 1e9
+        launch_s = st.loop_ms / 1000.0 / max(st.loop_launches, 1)
+        bpv = bytes_per_voxel_iter("fused" if variant == 0 else "plain", k, storage)
+        per_launch = bpv * vox if variant == 0 else bpv * vox / 2
+        return value, per_launch / launch_s / 1e9, bpv, st
+
+    def in_mask(x, planes=1):
+        return x.view(planes, m.n_lines, m.nstride)[:, :, : m.n_images]
+
+    out = {"reference": "FP32 fused solve of this line (bit-identical to the FP32 plain form)",
+           "f32_fused": {"value": round(fused_value, 3)}}
+    value, gbs, bpv, st = timed("f32", 1, lab_ref, v_ref)
+    out["f32_plain"] = {"value": round(value, 3), "achieved_gbs": round(gbs, 1), "bytes_per_voxel_iter": bpv}
+    # the FP32 reference state: the fused form gives the same bits as the plain one just run
+    plain_value = value
+    vr = in_mask(v_ref, k - 1).double()
+    lr = in_mask(lab_ref)
+    vr_norm = float(torch.linalg.vector_norm(vr).item())
+    for storage in ("bf16", "f16"):
+        value, gbs, bpv, st = timed(storage, 0, lab, v)
+        flips = int((in_mask(lab) != lr).sum().item())
+        dv = float(torch.linalg.vector_norm(in_mask(v, k - 1).double() - vr).item())
+        flips = int(dist_.reduce(float(flips), "sum"))
+        out[storage] = {"value": round(value, 3), "achieved_gbs": round(gbs, 1), "bytes_per_voxel_iter": bpv,
+                        "speedup_vs_f32_plain": round(value / plain_value, 3),
+                        "speedup_vs_f32_fused": round(value / fused_value, 3),
+                        "label_flips": flips, "flip_rate": flips / dist_.reduce(float(vox), "sum"),
+                        "v_rel_l2": dv / max(vr_norm, 1e-300),
+                        "gap_last": st.energy_trace[-1].tolist() if st.energy_trace is not None else None}
+    del lab_ref, lab, v_ref, v
+    torch.cuda.empty_cache()
+    return out
 
 
 def main():

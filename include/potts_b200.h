@@ -64,8 +64,16 @@ enum potts_variant {
     POTTS_VARIANT_PLAIN = 1  /* the reference's split: a dual launch and a primal launch per iteration */
 };
 
+/* Storage of the solver state (Xi, V, Vbar).  Arithmetic is FP32 in every
+ * format; the 16-bit formats round each stored value to nearest (ties to
+ * even), also the Vbar the fused form keeps on chip, so that the fused and the
+ * split forms give the same bits.  The reference stores FP32 only
+ * (potts-min-partition.cpp:586-600); the 16-bit formats halve the bytes per
+ * iteration.  Only the default tile shape of each K is compiled for them. */
 enum potts_storage {
-    POTTS_STORE_F32 = 0 /* state (Xi, V) stored in FP32 */
+    POTTS_STORE_F32 = 0,  /* FP32, as the reference */
+    POTTS_STORE_BF16 = 1, /* bfloat16 (8-bit mantissa) */
+    POTTS_STORE_F16 = 2   /* IEEE binary16 (11-bit mantissa); Xi and V lie in [-1, 1] */
 };
 
 typedef struct potts_options {
@@ -79,6 +87,8 @@ typedef struct potts_options {
     int tile_slices;  /* fused form: slices (n) per tile (0 = default for K) */
     int segment_cols; /* fused form: columns one tile marches over (0 = 64, at most 64) */
     int tile_vpt;     /* fused form: consecutive slices per thread, 2 or 4 (0 = default for K) */
+    int prefetch;     /* fused form: planes the load ring prefetches into L2 ahead of its loads
+                         (0 = default, < 0 = none, at most 16) */
 } potts_options;
 
 typedef struct potts_stats {

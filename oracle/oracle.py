@@ -113,9 +113,16 @@ class OracleResult:
     sweep_hist: np.ndarray
 
 
+STORE = {"f32": 0, "native": 0, "bf16": 1, "f16": 2}
+
+
 def solve(m, u: np.ndarray, ci, lam: float, tau1: float, tau2: float, iters: int, *, precision: str = "f64",
-          slab_w: int = 0, want_state: bool = True, gap_every: int = 0) -> OracleResult:
-    """The whole solve (potts-model/potts-min-partition.cpp:540-679) on the CPU."""
+          slab_w: int = 0, want_state: bool = True, gap_every: int = 0, store: str = "native") -> OracleResult:
+    """The whole solve (potts-model/potts-min-partition.cpp:540-679) on the CPU.
+
+    `store` models reduced-precision storage of the state: "bf16" or "f16" round every stored value
+    of Xi, V and Vbar to that format (to nearest, ties to even), except the stored V of "bf16", which
+    is rounded stochastically with bits from a counter hash of (line, n, iteration, component pair)."""
     dt, ct = _real(precision)
     K = len(ci)
     span = int(m.base[m.cols])
@@ -131,18 +138,18 @@ def solve(m, u: np.ndarray, ci, lam: float, tau1: float, tau2: float, iters: int
     ne = iters // gap_every if gap_every > 0 else 0
     en = np.zeros((max(ne, 1), 3), np.float64) if ne > 0 else None
     hist = np.zeros(21, np.int32)
-    f = getattr(lib(), f"oracle_solve_{precision}")
+    f = getattr(lib(), f"oracle_solve_store_{precision}")
     f.restype = ctypes.c_int
     f.argtypes = [ctypes.POINTER(OCyl), ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.POINTER(ctypes.c_float),
                   ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int,
                   ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ct),
                   ctypes.POINTER(ct), ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.POINTER(ctypes.c_double),
-                  ctypes.POINTER(ctypes.c_int)]
+                  ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     oc = ocyl(m)
     rc = f(ctypes.byref(oc), _ptr(u, ctypes.c_float), K, _ptr(c, ctypes.c_float), float(lam), float(tau1),
            float(tau2), int(iters), int(slab_w), _ptr(res, ctypes.c_float), _ptr(labels, ctypes.c_uint8),
            _ptr(V, ct), _ptr(Xi, ct), _ptr(dq, ctypes.c_float), int(gap_every), _ptr(en, ctypes.c_double),
-           _ptr(hist, ctypes.c_int))
+           _ptr(hist, ctypes.c_int), STORE[store])
     if rc != 0:
         raise RuntimeError("oracle_solve failed (bad arguments or slab planner)")
     return OracleResult(res, labels, V, Xi, dq[:iters], en, hist)

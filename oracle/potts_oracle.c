@@ -162,7 +162,67 @@ typedef struct {
     REAL *xi;  /* 3(K-1) planes of span */
     REAL *V;   /* K-1 planes */
     REAL *Vb;  /* K-1 planes */
+    int store; /* 0: state kept in REAL; 1: stored as bfloat16; 2: stored as IEEE binary16 */
+    int it;    /* 0-based iteration of the current primal step (keys the stochastic rounding of V) */
 } ostate;
+
+/* Rounding of a stored state value to the storage format (round to nearest,
+ * ties to even) and back.  bfloat16 keeps the top 16 bits of the binary32
+ * pattern; binary16 uses the compiler's _Float16 conversion (IEEE). */
+static inline REAL store_round(int store, REAL x)
+{
+    if (store == 1) {
+        float f = (float)x;
+        uint32_t b;
+        memcpy(&b, &f, 4);
+        if ((b & 0x7fffffffu) <= 0x7f800000u) { /* not NaN */
+            b += 0x7fffu + ((b >> 16) & 1u);
+            b &= 0xffff0000u;
+        }
+        memcpy(&f, &b, 4);
+        return (REAL)f;
+    }
+    if (store == 2) return (REAL)(float)(_Float16)(float)x;
+    return x;
+}
+
+/* The stored V of the bfloat16 format is rounded stochastically, with the
+ * random bits drawn from a counter-based hash of (line, n, iteration, pair of
+ * components): the result is reproducible and the same in every kernel form,
+ * and rounding no longer swallows the small updates of a converging solve.
+ * The mixer is "lowbias32" of Chris Wellons' hash-prospector (public domain);
+ * the key multipliers are the golden-ratio and xxHash32 primes.  The random
+ * 16 bits are added to the binary32 pattern before the low half is cut off,
+ * which rounds away from zero with probability equal to the cut fraction. */
+static inline uint32_t sr_mix(uint32_t x)
+{
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+static inline uint32_t sr_hash(uint32_t line, uint32_t n, uint32_t it, uint32_t pair)
+{
+    return sr_mix((line * 0x9e3779b1u) ^ (n * 0x85ebca77u) ^ ((it * 4u + pair) * 0xc2b2ae3du));
+}
+
+static inline REAL store_round_v(const ostate *st, REAL x, uint32_t line, uint32_t n, int i)
+{
+    if (st->store != 1) return store_round(st->store, x);
+    float f = (float)x;
+    uint32_t b;
+    memcpy(&b, &f, 4);
+    if ((b & 0x7fffffffu) < 0x7f800000u) { /* finite */
+        const uint32_t h = sr_hash(line, n, (uint32_t)st->it, (uint32_t)(i >> 1));
+        b += (i & 1) ? (h >> 16) : (h & 0xffffu);
+        b &= 0xffff0000u;
+    }
+    memcpy(&f, &b, 4);
+    return (REAL)f;
+}
 
 /* init_v_kernel, potts-min-partition.cpp:56-94: V = V_bar = one-hot of the
  * nearest label (strict <, first wins). */
@@ -247,7 +307,7 @@ static void grad_step(ostate *st, REAL tau2, int n_lo, int n_hi, int *sweep_hist
                     int sw = NAME(oracle_project_K)(q, K);
                     lh[sw] += 1;
                     for (int i = 0; i < K - 1; ++i)
-                        for (int a = 0; a < 3; ++a) st->xi[(3 * i + a) * S + o] = q[3 * i + a];
+                        for (int a = 0; a < 3; ++a) st->xi[(3 * i + a) * S + o] = store_round(st->store, q[3 * i + a]);
                 }
             }
         }
@@ -321,9 +381,10 @@ static REAL div_step(ostate *st, const float *u, const REAL *c, REAL lam, REAL t
                     REAL e = q[i] - v[i];
                     dq = (i == 0) ? e * e : FMA(e, e, dq);
                 }
+                const uint32_t line = m->base[col] / m->nstride + (uint32_t)(row - row_begin(m, col));
                 for (int i = 0; i < K - 1; ++i) {
-                    st->Vb[i * S + o] = (REAL)2 * q[i] - v[i];
-                    st->V[i * S + o] = q[i];
+                    st->Vb[i * S + o] = store_round(st->store, (REAL)2 * q[i] - v[i]);
+                    st->V[i * S + o] = store_round_v(st, q[i], line, (uint32_t)n, i);
                 }
                 if (dq > dq_max) dq_max = dq;
             }
@@ -431,7 +492,9 @@ static void energies(const ostate *st, const float *u, const REAL *c, REAL lam, 
 }
 
 /* ---------------------------------------------------------------------------
- * Whole solve, potts-min-partition.cpp:540-679.
+ * Whole solve, potts-min-partition.cpp:540-679.  oracle_solve_store also
+ * models reduced-precision storage of the state: every stored value of Xi, V
+ * and Vbar is rounded to bfloat16 (store = 1) or binary16 (store = 2).
  *
  * slab_w <= 0 or >= n_images: one slab over the whole volume.  Otherwise the
  * reference's planner: halo = iters, res_w = slab_w - 2*halo, slabs start at
@@ -446,9 +509,10 @@ static void energies(const ostate *st, const float *u, const REAL *c, REAL lam, 
  *
  * Returns 0, or -1 on bad arguments / allocation failure / planner failure.
  * ------------------------------------------------------------------------- */
-int NAME(oracle_solve)(const ocyl *m, const float *u, int K, const float *c_f, float lam_f, float tau1_f,
-                       float tau2_f, int iters, int slab_w, float *res, uint8_t *labels, REAL *V_out, REAL *Xi_out,
-                       float *dq_trace, int gap_every, double *energy_trace, int *sweep_hist)
+int NAME(oracle_solve_store)(const ocyl *m, const float *u, int K, const float *c_f, float lam_f, float tau1_f,
+                             float tau2_f, int iters, int slab_w, float *res, uint8_t *labels, REAL *V_out,
+                             REAL *Xi_out, float *dq_trace, int gap_every, double *energy_trace, int *sweep_hist,
+                             int store)
 {
     if (!m || !u || K < 2 || K > KMAX || iters < 0) return -1;
     const int n = (int)m->n_images;
@@ -461,6 +525,7 @@ int NAME(oracle_solve)(const ocyl *m, const float *u, int K, const float *c_f, f
     st.m = m;
     st.K = K;
     st.span = span;
+    st.store = store;
     const size_t ns = (size_t)(span > 0 ? span : 1);
     st.xi = (REAL *)calloc(ns * 3 * (size_t)(K - 1), sizeof(REAL));
     st.V = (REAL *)calloc(ns * (size_t)(K - 1), sizeof(REAL));
@@ -482,6 +547,7 @@ int NAME(oracle_solve)(const ocyl *m, const float *u, int K, const float *c_f, f
         memset(st.xi, 0, ns * 3 * (size_t)(K - 1) * sizeof(REAL));
         for (int it = 0; it < iters; ++it) {
             grad_step(&st, tau2, s0, s1, sweep_hist);
+            st.it = it;
             REAL dq = div_step(&st, u, c, lam, tau1, s0, s1);
             if (dq_trace) dq_trace[it] = (float)dq;
             if (energy_trace && gap_every > 0 && (it + 1) % gap_every == 0)
@@ -501,11 +567,19 @@ int NAME(oracle_solve)(const ocyl *m, const float *u, int K, const float *c_f, f
     return 0;
 }
 
+int NAME(oracle_solve)(const ocyl *m, const float *u, int K, const float *c_f, float lam_f, float tau1_f,
+                       float tau2_f, int iters, int slab_w, float *res, uint8_t *labels, REAL *V_out, REAL *Xi_out,
+                       float *dq_trace, int gap_every, double *energy_trace, int *sweep_hist)
+{
+    return NAME(oracle_solve_store)(m, u, K, c_f, lam_f, tau1_f, tau2_f, iters, slab_w, res, labels, V_out, Xi_out,
+                                    dq_trace, gap_every, energy_trace, sweep_hist, 0);
+}
+
 /* Single steps on caller-owned state (whole volume as one slab), for tests of
  * the adjoint identity and of individual kernels. */
 void NAME(oracle_grad_step)(const ocyl *m, int K, REAL *xi, const REAL *Vb, float tau2)
 {
-    ostate st = {m, K, (int64_t)m->base[m->cols], xi, NULL, (REAL *)Vb};
+    ostate st = {m, K, (int64_t)m->base[m->cols], xi, NULL, (REAL *)Vb, 0, 0};
     grad_step(&st, (REAL)tau2, 0, (int)m->n_images, NULL);
 }
 
@@ -514,7 +588,7 @@ REAL NAME(oracle_div_step)(const ocyl *m, int K, const REAL *xi, REAL *V, REAL *
 {
     REAL c[KMAX];
     for (int i = 0; i < K; ++i) c[i] = (REAL)c_f[i];
-    ostate st = {m, K, (int64_t)m->base[m->cols], (REAL *)xi, V, Vb};
+    ostate st = {m, K, (int64_t)m->base[m->cols], (REAL *)xi, V, Vb, 0, 0};
     return div_step(&st, u, c, (REAL)lam, (REAL)tau1, 0, (int)m->n_images);
 }
 
@@ -523,6 +597,6 @@ void NAME(oracle_energies)(const ocyl *m, int K, const REAL *xi, const REAL *V, 
 {
     REAL c[KMAX];
     for (int i = 0; i < K; ++i) c[i] = (REAL)c_f[i];
-    ostate st = {m, K, (int64_t)m->base[m->cols], (REAL *)xi, (REAL *)V, NULL};
+    ostate st = {m, K, (int64_t)m->base[m->cols], (REAL *)xi, (REAL *)V, NULL, 0, 0};
     energies(&st, u, c, (REAL)lam, 0, (int)m->n_images, out);
 }

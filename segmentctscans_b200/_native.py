@@ -12,7 +12,8 @@ from .build import LIB_PATH
 
 POTTS_OK, POTTS_EINVAL, POTTS_ENOMEM, POTTS_ECUDA, POTTS_ETIMEOUT, POTTS_ENODEV = range(6)
 VARIANT_FUSED, VARIANT_PLAIN = 0, 1
-STORE_F32 = 0
+STORE_F32, STORE_BF16, STORE_F16 = 0, 1, 2
+STORAGE = {"f32": STORE_F32, "bf16": STORE_BF16, "f16": STORE_F16}
 MAX_PHASES = 6
 
 
@@ -29,7 +30,7 @@ class PottsOptions(ctypes.Structure):
         ("variant", ctypes.c_int), ("storage", ctypes.c_int), ("gap_every", ctypes.c_int),
         ("slab_w", ctypes.c_int), ("track_dq", ctypes.c_int), ("sync_monitor", ctypes.c_int),
         ("tile_rows", ctypes.c_int), ("tile_slices", ctypes.c_int), ("segment_cols", ctypes.c_int),
-        ("tile_vpt", ctypes.c_int),
+        ("tile_vpt", ctypes.c_int), ("prefetch", ctypes.c_int),
     ]
 
 
@@ -121,5 +122,9 @@ def default_options(**kw) -> PottsOptions:
     for k, v in kw.items():
         if not hasattr(o, k):
             raise TypeError(f"unknown option {k}")
+        if k == "storage" and isinstance(v, str):
+            if v not in STORAGE:
+                raise ValueError(f"unknown storage {v!r}; one of {sorted(STORAGE)}")
+            v = STORAGE[v]
         setattr(o, k, int(v))
     return o

@@ -7,6 +7,7 @@
 #include <cstdint>
 
 #include "geometry.cuh"
+#include "storage.cuh"
 #include "voxel.cuh"
 
 namespace potts {
@@ -32,9 +33,9 @@ __device__ __forceinline__ PlainIndex plain_index(const Geometry &g, int n_begin
 }
 
 // init_v_kernel: V = Vbar = one-hot of the nearest label (Vbar optional).
-template <int K>
-__global__ void __launch_bounds__(kPlainThreads) init_kernel(Geometry g, const float *__restrict__ u, float *V,
-                                                              float *Vb, PhaseParams<K> pp)
+template <int K, typename ST>
+__global__ void __launch_bounds__(kPlainThreads) init_kernel(Geometry g, const float *__restrict__ u, ST *V, ST *Vb,
+                                                              PhaseParams<K> pp)
 {
     const PlainIndex p = plain_index(g, 0, g.ns);
     if (!p.valid) return;
@@ -44,15 +45,15 @@ __global__ void __launch_bounds__(kPlainThreads) init_kernel(Geometry g, const f
 #pragma unroll
     for (int i = 0; i < K - 1; ++i) {
         const float one = (i == cl) ? 1.0f : 0.0f;
-        V[i * g.plane_w + o] = one;
-        if (Vb) Vb[i * g.plane_w + o] = one;
+        V[i * g.plane_w + o] = Store<ST>::st(one);
+        if (Vb) Vb[i * g.plane_w + o] = Store<ST>::st(one);
     }
 }
 
 // grad_kernel: Xi <- Pi_K(Xi + tau2 * grad+ Vbar), in place.
-template <int K>
-__global__ void __launch_bounds__(kPlainThreads) dual_kernel(Geometry g, float *__restrict__ xi,
-                                                              const float *__restrict__ vb, float tau2,
+template <int K, typename ST>
+__global__ void __launch_bounds__(kPlainThreads) dual_kernel(Geometry g, ST *__restrict__ xi,
+                                                              const ST *__restrict__ vb, float tau2,
                                                               DykstraThresholds thr)
 {
     const PlainIndex p = plain_index(g, 0, g.ns);
@@ -66,17 +67,17 @@ __global__ void __launch_bounds__(kPlainThreads) dual_kernel(Geometry g, float *
     float vx[K - 1], vn[K - 1], vr[K - 1], vc[K - 1], x[3 * (K - 1)], xo[3 * (K - 1)];
 #pragma unroll
     for (int i = 0; i < K - 1; ++i) {
-        const float *b = vb + i * g.plane_w;
-        vx[i] = b[o];
-        vn[i] = hn ? b[o + 1] : 0.0f;
-        vr[i] = hr ? b[o + g.nstride_w] : 0.0f;
-        vc[i] = hc ? b[oc] : 0.0f;
+        const ST *b = vb + i * g.plane_w;
+        vx[i] = Store<ST>::ld(b[o]);
+        vn[i] = hn ? Store<ST>::ld(b[o + 1]) : 0.0f;
+        vr[i] = hr ? Store<ST>::ld(b[o + g.nstride_w]) : 0.0f;
+        vc[i] = hc ? Store<ST>::ld(b[oc]) : 0.0f;
     }
 #pragma unroll
-    for (int j = 0; j < 3 * (K - 1); ++j) x[j] = xi[j * g.plane_w + o];
+    for (int j = 0; j < 3 * (K - 1); ++j) x[j] = Store<ST>::ld(xi[j * g.plane_w + o]);
     dual_voxel<K>(xo, x, vx, vn, vr, vc, hn, hr, hc, tau2, thr);
 #pragma unroll
-    for (int j = 0; j < 3 * (K - 1); ++j) xi[j * g.plane_w + o] = xo[j];
+    for (int j = 0; j < 3 * (K - 1); ++j) xi[j * g.plane_w + o] = Store<ST>::st(xo[j]);
 }
 
 // Block-wide max of a non-negative float, then one atomic per block into *dst.
@@ -99,12 +100,13 @@ __device__ __forceinline__ void block_max_to(float v, float *dst)
 }
 
 // div_kernel: V <- Pi_S(V + tau1 (div- Xi - G)), Vbar <- 2 V_new - V (optional),
-// max |dV|^2 into *dq (optional).
-template <int K>
-__global__ void __launch_bounds__(kPlainThreads) primal_kernel(Geometry g, const float *__restrict__ xi,
-                                                                float *__restrict__ V, float *__restrict__ Vb,
+// max |dV|^2 into *dq (optional).  it: 0-based iteration (keys the stochastic
+// rounding of a bfloat16 V).
+template <int K, typename ST>
+__global__ void __launch_bounds__(kPlainThreads) primal_kernel(Geometry g, const ST *__restrict__ xi,
+                                                                ST *__restrict__ V, ST *__restrict__ Vb,
                                                                 const float *__restrict__ u, PhaseParams<K> pp,
-                                                                float *dq)
+                                                                float *dq, int it)
 {
     const PlainIndex p = plain_index(g, 0, g.ns);
     float d = 0.0f;
@@ -118,23 +120,32 @@ __global__ void __launch_bounds__(kPlainThreads) primal_kernel(Geometry g, const
         float x[3 * (K - 1)], xn[K - 1], xr[K - 1], xc[K - 1], v[K - 1], vnew[K - 1], vbar[K - 1];
 #pragma unroll
         for (int i = 0; i < K - 1; ++i) {
-            const float *b0 = xi + (3 * i) * g.plane_w;
-            const float *b1 = xi + (3 * i + 1) * g.plane_w;
-            const float *b2 = xi + (3 * i + 2) * g.plane_w;
-            x[3 * i] = b0[o];
-            x[3 * i + 1] = b1[o];
-            x[3 * i + 2] = b2[o];
-            xn[i] = pn ? b0[o - 1] : 0.0f;
-            xr[i] = pr ? b1[o - g.nstride_w] : 0.0f;
-            xc[i] = pc ? b2[opc] : 0.0f;
-            v[i] = V[i * g.plane_w + o];
+            const ST *b0 = xi + (3 * i) * g.plane_w;
+            const ST *b1 = xi + (3 * i + 1) * g.plane_w;
+            const ST *b2 = xi + (3 * i + 2) * g.plane_w;
+            x[3 * i] = Store<ST>::ld(b0[o]);
+            x[3 * i + 1] = Store<ST>::ld(b1[o]);
+            x[3 * i + 2] = Store<ST>::ld(b2[o]);
+            xn[i] = pn ? Store<ST>::ld(b0[o - 1]) : 0.0f;
+            xr[i] = pr ? Store<ST>::ld(b1[o - g.nstride_w]) : 0.0f;
+            xc[i] = pc ? Store<ST>::ld(b2[opc]) : 0.0f;
+            v[i] = Store<ST>::ld(V[i * g.plane_w + o]);
         }
         const float uu = u[p.line * g.nstride_in + g.slab_start + p.n];
         d = primal_voxel<K>(vnew, vbar, v, x, xn, xr, xc, pn, hn, pr, hr, pc, hc, uu, pp.c, pp.lam, pp.tau1);
+        uint32_t h[(K - 1 + 1) / 2];
+        if constexpr (Store<ST>::kStochasticV) {
+#pragma unroll
+            for (int k = 0; k < (K - 1 + 1) / 2; ++k)
+                h[k] = sr_hash((uint32_t)p.line, (uint32_t)(g.slab_start + p.n), (uint32_t)it, (uint32_t)k);
+        }
 #pragma unroll
         for (int i = 0; i < K - 1; ++i) {
-            V[i * g.plane_w + o] = vnew[i];
-            if (Vb) Vb[i * g.plane_w + o] = vbar[i];
+            if constexpr (Store<ST>::kStochasticV)
+                V[i * g.plane_w + o] = Store<ST>::st_v(vnew[i], sr_bits(h[i >> 1], i));
+            else
+                V[i * g.plane_w + o] = Store<ST>::st(vnew[i]);
+            if (Vb) Vb[i * g.plane_w + o] = Store<ST>::st(vbar[i]);
         }
     }
     if (dq) block_max_to(d, dq);
@@ -142,9 +153,9 @@ __global__ void __launch_bounds__(kPlainThreads) primal_kernel(Geometry g, const
 
 // update_kernel: argmax over n in [res_begin, res_end) of the slab, written
 // with the input mapping; optionally copies V and Xi out.
-template <int K>
-__global__ void __launch_bounds__(kPlainThreads) update_kernel(Geometry g, const float *__restrict__ V,
-                                                                const float *__restrict__ xi, PhaseParams<K> pp,
+template <int K, typename ST>
+__global__ void __launch_bounds__(kPlainThreads) update_kernel(Geometry g, const ST *__restrict__ V,
+                                                                const ST *__restrict__ xi, PhaseParams<K> pp,
                                                                 int res_begin, int res_end, float *res,
                                                                 uint8_t *labels, float *V_out, float *Xi_out,
                                                                 int64_t plane_out)
@@ -155,7 +166,7 @@ __global__ void __launch_bounds__(kPlainThreads) update_kernel(Geometry g, const
     const int64_t oo = p.line * g.nstride_in + g.slab_start + p.n;
     float v[K - 1];
 #pragma unroll
-    for (int i = 0; i < K - 1; ++i) v[i] = V[i * g.plane_w + o];
+    for (int i = 0; i < K - 1; ++i) v[i] = Store<ST>::ld(V[i * g.plane_w + o]);
     const int lab = argmax_label<K>(v);
     if (res) res[oo] = pp.c[lab];
     if (labels) labels[oo] = (uint8_t)lab;
@@ -165,7 +176,7 @@ __global__ void __launch_bounds__(kPlainThreads) update_kernel(Geometry g, const
     }
     if (Xi_out) {
 #pragma unroll
-        for (int j = 0; j < 3 * (K - 1); ++j) Xi_out[j * plane_out + oo] = xi[j * g.plane_w + o];
+        for (int j = 0; j < 3 * (K - 1); ++j) Xi_out[j * plane_out + oo] = Store<ST>::ld(xi[j * g.plane_w + o]);
     }
 }
 
@@ -174,9 +185,9 @@ __global__ void __launch_bounds__(kPlainThreads) update_kernel(Geometry g, const
 //   e_i = lam (u - c_i)^2 - div Xi_i,  L += sum_i V_i e_i,  D += min_i e_i.
 // One pair of partial sums per block; energy_finish adds them in block order.
 // ---------------------------------------------------------------------------
-template <int K>
-__global__ void __launch_bounds__(kPlainThreads) energy_kernel(Geometry g, const float *__restrict__ xi,
-                                                                const float *__restrict__ V,
+template <int K, typename ST>
+__global__ void __launch_bounds__(kPlainThreads) energy_kernel(Geometry g, const ST *__restrict__ xi,
+                                                                const ST *__restrict__ V,
                                                                 const float *__restrict__ u, PhaseParams<K> pp,
                                                                 double2 *partial)
 {
@@ -195,19 +206,19 @@ __global__ void __launch_bounds__(kPlainThreads) energy_kernel(Geometry g, const
         for (int i = 0; i < K; ++i) {
             double x0, x1, x2, wn, wr, wc, vi;
             if (i < K - 1) {
-                x0 = xi[(3 * i) * g.plane_w + o];
-                x1 = xi[(3 * i + 1) * g.plane_w + o];
-                x2 = xi[(3 * i + 2) * g.plane_w + o];
+                x0 = Store<ST>::ld(xi[(3 * i) * g.plane_w + o]);
+                x1 = Store<ST>::ld(xi[(3 * i + 1) * g.plane_w + o]);
+                x2 = Store<ST>::ld(xi[(3 * i + 2) * g.plane_w + o]);
                 xk0 -= x0;
                 xk1 -= x1;
                 xk2 -= x2;
-                wn = pn ? (double)xi[(3 * i) * g.plane_w + o - 1] : 0.0;
-                wr = pr ? (double)xi[(3 * i + 1) * g.plane_w + o - g.nstride_w] : 0.0;
-                wc = pc ? (double)xi[(3 * i + 2) * g.plane_w + opc] : 0.0;
+                wn = pn ? (double)Store<ST>::ld(xi[(3 * i) * g.plane_w + o - 1]) : 0.0;
+                wr = pr ? (double)Store<ST>::ld(xi[(3 * i + 1) * g.plane_w + o - g.nstride_w]) : 0.0;
+                wc = pc ? (double)Store<ST>::ld(xi[(3 * i + 2) * g.plane_w + opc]) : 0.0;
                 xkn -= wn;
                 xkr -= wr;
                 xkc -= wc;
-                vi = V[i * g.plane_w + o];
+                vi = Store<ST>::ld(V[i * g.plane_w + o]);
                 vk -= vi;
             } else {
                 x0 = xk0;

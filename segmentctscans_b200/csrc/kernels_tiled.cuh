@@ -49,6 +49,7 @@
 
 #include "geometry.cuh"
 #include "kernels_plain.cuh"
+#include "storage.cuh"
 #include "tma.cuh"
 #include "voxel.cuh"
 
@@ -65,14 +66,20 @@ struct TiledParams {
     int nstride_w;  // stride of the state arrays
     int64_t plane_w;
     int u_x0;       // n offset of the slab in the u tensor map
+    int n_base;     // global slice of the slab's slice 0
+    int it;         // 0-based iteration of the launch's primal step (keys stochastic rounding)
+    int prefetch;   // planes ahead of the load ring prefetched into L2 (0: none)
 };
 
-template <int K, int R, int NT, int VPT>
+template <int K, int R, int NT, int VPT, typename ST>
 struct TileShape {
     static constexpr int D = 3;  // ring depth (planes)
     static constexpr int C3 = 3 * (K - 1), C1 = K - 1, Q = NT / VPT;  // Q threads per tile row
-    static constexpr int NX = NT + 8;  // Xi box: slices n0-4 .. n0+NT+3
-    static constexpr int NV = NT + 4;  // V/u/Vbar box: slices n0 .. n0+NT+3
+    static constexpr int ES = (int)sizeof(ST);          // bytes per stored state value
+    static constexpr int XH = ES == 4 ? 4 : 8;          // Xi box starts XH slices early (16-byte TMA start)
+    static constexpr int NX = NT + 2 * XH;              // Xi box: slices n0-XH .. n0+NT+XH-1
+    static constexpr int NVT = NT + (ES == 4 ? 4 : 8);  // V box: slices n0 .. (whole 16-byte rows)
+    static constexpr int NV = NT + 4;                   // u and Vbar (FP32): slices n0 .. n0+NT+3
     static constexpr int MAIN = R * Q;
     static constexpr int MAIN_WARPS = MAIN / 32;
     static constexpr int HALO_WARPS = (Q + 31) / 32;  // the high halo row (and the slice n0+NT)
@@ -80,16 +87,17 @@ struct TileShape {
     static constexpr int THREADS = MAIN + 32 * HALO_WARPS + 32;
     static constexpr int QSTRIDE = (3 * K + 1) | 1;  // queue entry: q (3K floats) + state offset; odd stride
     static constexpr int QCAP = 64;                    // ring of one pass (32) + one gather round (32)
-    static constexpr int XI_BYTES = C3 * (R + 2) * NX * 4;
-    static constexpr int V_BYTES = C1 * (R + 1) * NV * 4;
+    static constexpr int XI_BYTES = C3 * (R + 2) * NX * ES;
+    static constexpr int V_BYTES = C1 * (R + 1) * NVT * ES;
     static constexpr int U_BYTES = (R + 1) * NV * 4;
+    static constexpr int VB_BYTES = C1 * (R + 1) * NV * 4;
     static constexpr int al(int b) { return (b + 127) / 128 * 128; }
-    static constexpr int XI_SLOT = al(XI_BYTES), V_SLOT = al(V_BYTES), U_SLOT = al(U_BYTES);
+    static constexpr int XI_SLOT = al(XI_BYTES), V_SLOT = al(V_BYTES), U_SLOT = al(U_BYTES), VB_SLOT = al(VB_BYTES);
     static constexpr int OFF_XI = 0;
     static constexpr int OFF_V = OFF_XI + D * XI_SLOT;
     static constexpr int OFF_U = OFF_V + D * V_SLOT;
     static constexpr int OFF_VB = OFF_U + D * U_SLOT;
-    static constexpr int OFF_Q = OFF_VB + D * V_SLOT;
+    static constexpr int OFF_Q = OFF_VB + D * VB_SLOT;
     static constexpr int MAX_SEGMENT = 64;  // columns per work item
     static constexpr int OFF_COLS = OFF_Q + al(MAIN_WARPS * QCAP * QSTRIDE * 4);
     static constexpr int OFF_BAR = OFF_COLS + al((MAX_SEGMENT + 3) * 16);
@@ -100,41 +108,47 @@ struct TileShape {
     static_assert(SMEM_ALLOC <= 227 * 1024, "shared memory of one block");
 };
 
-// VPT consecutive floats of shared or global memory as one vector access.
-template <int VPT>
-__device__ __forceinline__ void ldv(float (&a)[VPT], const float *p)
+// VPT consecutive stored values of shared or global memory, widened to FP32
+// (and the reverse, rounding), as vector accesses.
+template <int VPT, typename ST>
+__device__ __forceinline__ void ldv(float (&a)[VPT], const ST *p)
 {
-    if constexpr (VPT == 4) {
+    if constexpr (VPT == 4 && sizeof(ST) == 4) {
         const float4 v = *reinterpret_cast<const float4 *>(p);
         a[0] = v.x, a[1] = v.y, a[2] = v.z, a[3] = v.w;
     } else {
-        const float2 v = *reinterpret_cast<const float2 *>(p);
-        a[0] = v.x, a[1] = v.y;
+#pragma unroll
+        for (int j = 0; j < VPT; j += 2) {
+            const float2 v = Store<ST>::ld2(p + j);
+            a[j] = v.x, a[j + 1] = v.y;
+        }
     }
 }
-template <int VPT>
-__device__ __forceinline__ void stv(float *p, const float (&a)[VPT])
+template <int VPT, typename ST>
+__device__ __forceinline__ void stv(ST *p, const float (&a)[VPT])
 {
-    if constexpr (VPT == 4)
+    if constexpr (VPT == 4 && sizeof(ST) == 4) {
         *reinterpret_cast<float4 *>(p) = make_float4(a[0], a[1], a[2], a[3]);
-    else
-        *reinterpret_cast<float2 *>(p) = make_float2(a[0], a[1]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < VPT; j += 2) Store<ST>::st2(p + j, make_float2(a[j], a[j + 1]));
+    }
 }
 
 __device__ __forceinline__ bool row_in_col(int4 ci, int row) { return row >= ci.y && row < ci.z; }
 
-template <int K, int R, int NT, int VPT>
+template <int K, int R, int NT, int VPT, typename ST>
 struct TiledSmem {
-    using S = TileShape<K, R, NT, VPT>;
+    using S = TileShape<K, R, NT, VPT, ST>;
     uint8_t *base;
 
-    __device__ __forceinline__ float *xi_slot(int slot) const
+    __device__ __forceinline__ ST *xi_slot(int slot) const
     {
-        return reinterpret_cast<float *>(base + S::OFF_XI + slot * S::XI_SLOT);
+        return reinterpret_cast<ST *>(base + S::OFF_XI + slot * S::XI_SLOT);
     }
-    __device__ __forceinline__ float *v_slot(int slot) const
+    __device__ __forceinline__ ST *v_slot(int slot) const
     {
-        return reinterpret_cast<float *>(base + S::OFF_V + slot * S::V_SLOT);
+        return reinterpret_cast<ST *>(base + S::OFF_V + slot * S::V_SLOT);
     }
     __device__ __forceinline__ float *u_slot(int slot) const
     {
@@ -142,7 +156,7 @@ struct TiledSmem {
     }
     __device__ __forceinline__ float *vb_plane(int slot) const
     {
-        return reinterpret_cast<float *>(base + S::OFF_VB + slot * S::V_SLOT);
+        return reinterpret_cast<float *>(base + S::OFF_VB + slot * S::VB_SLOT);
     }
     __device__ __forceinline__ float *queue(int warp) const
     {
@@ -167,21 +181,23 @@ struct TiledSmem {
     {
         return reinterpret_cast<volatile int *>(base + S::OFF_BAR + 3 * S::D * 8);
     }
-    // element (comp, box row, box slice) of an Xi plane / a V-shaped plane
+    // element (comp, box row, box slice) of an Xi plane (slice 0 = n0 - XH), of
+    // a stored V plane, and of a u / Vbar plane (slice 0 = n0 in both)
     __device__ __forceinline__ static int xi_at(int comp, int rr, int nn) { return (comp * (R + 2) + rr) * S::NX + nn; }
+    __device__ __forceinline__ static int vt_at(int comp, int rr, int nn) { return (comp * (R + 1) + rr) * S::NVT + nn; }
     __device__ __forceinline__ static int v_at(int comp, int rr, int nn) { return (comp * (R + 1) + rr) * S::NV + nn; }
 };
 
 // Stage A for VPT consecutive slices n0+VPT*q .. of tile row rr (row r0+rr).
 // Planes are indexed by "ring position" p = c - ca + 1 (plane ca-1 is p = 0);
 // sc and sp are the ring slots of planes p and p-1.
-template <int K, int R, int NT, int VPT>
-__device__ __forceinline__ void stage_a_chunk(const TiledSmem<K, R, NT, VPT> &sm, const TiledParams &tp,
+template <int K, int R, int NT, int VPT, typename ST>
+__device__ __forceinline__ void stage_a_chunk(const TiledSmem<K, R, NT, VPT, ST> &sm, const TiledParams &tp,
                                               const PhaseParams<K> &pp, int p, int sc, int sp, int r0, int rr,
-                                              int n0, int q, bool store_v, float *__restrict__ Vout, float &dqmax)
+                                              int n0, int q, bool store_v, ST *__restrict__ Vout, float &dqmax)
 {
-    using S = TileShape<K, R, NT, VPT>;
-    using T = TiledSmem<K, R, NT, VPT>;
+    using S = TileShape<K, R, NT, VPT, ST>;
+    using T = TiledSmem<K, R, NT, VPT, ST>;
     const int row = r0 + rr;
     float *vb = sm.vb_plane(sc);
     const int4 ci = sm.cols()[p];
@@ -198,23 +214,24 @@ __device__ __forceinline__ void stage_a_chunk(const TiledSmem<K, R, NT, VPT> &sm
     const bool pr = row > ci.y, hr = row + 1 < ci.z;
     const bool pc = row_in_col(sm.cols()[p - 1], row);
     const bool hc = row_in_col(sm.cols()[p + 1], row);
-    const float *xs = sm.xi_slot(sc), *xp = sm.xi_slot(sp);
-    const float *vs = sm.v_slot(sc), *us = sm.u_slot(sc);
+    const ST *xs = sm.xi_slot(sc), *xp = sm.xi_slot(sp);
+    const ST *vs = sm.v_slot(sc);
+    const float *us = sm.u_slot(sc);
+    constexpr int XH = S::XH;
 
     float onew[K - 1][VPT], obar[K - 1][VPT];
     if constexpr (VPT == 2) {
         // both slices with paired FP32 instructions
-        const float2 *xs2 = reinterpret_cast<const float2 *>(xs);
         float2 x[S::C3], xin[K - 1], xr[K - 1], xc[K - 1], v[K - 1], vn[K - 1], vbar[K - 1];
 #pragma unroll
-        for (int comp = 0; comp < S::C3; ++comp) x[comp] = xs2[T::xi_at(comp, rr + 1, off + 4) / 2];
+        for (int comp = 0; comp < S::C3; ++comp) x[comp] = Store<ST>::ld2(xs + T::xi_at(comp, rr + 1, off + XH));
 #pragma unroll
         for (int i = 0; i < K - 1; ++i) {
-            const float2 before = xs2[T::xi_at(3 * i, rr + 1, off + 2) / 2];  // slices nb-2, nb-1
+            const float2 before = Store<ST>::ld2(xs + T::xi_at(3 * i, rr + 1, off + XH - 2));  // slices nb-2, nb-1
             xin[i] = f2(before.y, x[3 * i].x);
-            xr[i] = xs2[T::xi_at(3 * i + 1, rr, off + 4) / 2];
-            xc[i] = reinterpret_cast<const float2 *>(xp)[T::xi_at(3 * i + 2, rr + 1, off + 4) / 2];
-            v[i] = reinterpret_cast<const float2 *>(vs)[T::v_at(i, rr, off) / 2];
+            xr[i] = Store<ST>::ld2(xs + T::xi_at(3 * i + 1, rr, off + XH));
+            xc[i] = Store<ST>::ld2(xp + T::xi_at(3 * i + 2, rr + 1, off + XH));
+            v[i] = Store<ST>::ld2(vs + T::vt_at(i, rr, off));
         }
         const float2 u2 = reinterpret_cast<const float2 *>(us)[T::v_at(0, rr, off) / 2];
         const bool second = nb + 1 < tp.ns;
@@ -226,20 +243,20 @@ __device__ __forceinline__ void stage_a_chunk(const TiledSmem<K, R, NT, VPT> &sm
 #pragma unroll
         for (int i = 0; i < K - 1; ++i) {
             onew[i][0] = vn[i].x;
-            obar[i][0] = vbar[i].x;
+            obar[i][0] = Store<ST>::round(vbar[i].x);  // Vbar as if stored
             onew[i][1] = second ? vn[i].y : 0.0f;
-            obar[i][1] = second ? vbar[i].y : 0.0f;
+            obar[i][1] = second ? Store<ST>::round(vbar[i].y) : 0.0f;
         }
     } else {
         float x[S::C3][VPT], xn[K - 1][VPT], xr[K - 1][VPT], xc[K - 1][VPT], v[K - 1][VPT], u[VPT];
 #pragma unroll
-        for (int comp = 0; comp < S::C3; ++comp) ldv<VPT>(x[comp], xs + T::xi_at(comp, rr + 1, off + 4));
+        for (int comp = 0; comp < S::C3; ++comp) ldv<VPT>(x[comp], xs + T::xi_at(comp, rr + 1, off + XH));
 #pragma unroll
         for (int i = 0; i < K - 1; ++i) {
-            ldv<VPT>(xn[i], xs + T::xi_at(3 * i, rr + 1, off + 4 - VPT));  // the chunk before: slices nb-VPT .. nb-1
-            ldv<VPT>(xr[i], xs + T::xi_at(3 * i + 1, rr, off + 4));
-            ldv<VPT>(xc[i], xp + T::xi_at(3 * i + 2, rr + 1, off + 4));
-            ldv<VPT>(v[i], vs + T::v_at(i, rr, off));
+            ldv<VPT>(xn[i], xs + T::xi_at(3 * i, rr + 1, off + XH - VPT));  // the chunk before: slices nb-VPT .. nb-1
+            ldv<VPT>(xr[i], xs + T::xi_at(3 * i + 1, rr, off + XH));
+            ldv<VPT>(xc[i], xp + T::xi_at(3 * i + 2, rr + 1, off + XH));
+            ldv<VPT>(v[i], vs + T::vt_at(i, rr, off));
         }
         ldv<VPT>(u, us + T::v_at(0, rr, off));
 #pragma unroll
@@ -267,7 +284,7 @@ __device__ __forceinline__ void stage_a_chunk(const TiledSmem<K, R, NT, VPT> &sm
 #pragma unroll
             for (int i = 0; i < K - 1; ++i) {
                 onew[i][j] = vn[i];
-                obar[i][j] = vbar[i];
+                obar[i][j] = Store<ST>::round(vbar[i]);  // Vbar as if stored
             }
         }
     }
@@ -275,7 +292,33 @@ __device__ __forceinline__ void stage_a_chunk(const TiledSmem<K, R, NT, VPT> &sm
     for (int i = 0; i < K - 1; ++i) stv<VPT>(vb + T::v_at(i, rr, off), obar[i]);
     if (store_v) {
         const int64_t o = (int64_t)(ci.x + row - ci.y) * tp.nstride_w + nb;
-        if (nb + VPT <= tp.ns) {
+        if constexpr (Store<ST>::kStochasticV) {
+            const uint32_t line = (uint32_t)(ci.x + row - ci.y);
+            ST sv[K - 1][VPT];
+#pragma unroll
+            for (int j = 0; j < VPT; ++j) {
+                uint32_t h[(K - 1 + 1) / 2];
+#pragma unroll
+                for (int k = 0; k < (K - 1 + 1) / 2; ++k)
+                    h[k] = sr_hash(line, (uint32_t)(tp.n_base + nb + j), (uint32_t)tp.it, (uint32_t)k);
+#pragma unroll
+                for (int i = 0; i < K - 1; ++i) sv[i][j] = Store<ST>::st_v(onew[i][j], sr_bits(h[i >> 1], i));
+            }
+            if (nb + VPT <= tp.ns) {
+#pragma unroll
+                for (int i = 0; i < K - 1; ++i)
+#pragma unroll
+                    for (int j = 0; j < VPT; j += 2)
+                        *reinterpret_cast<__nv_bfloat162 *>(Vout + i * tp.plane_w + o + j) =
+                            __halves2bfloat162(sv[i][j], sv[i][j + 1]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < VPT; ++j)
+                    if (nb + j < tp.ns)
+#pragma unroll
+                        for (int i = 0; i < K - 1; ++i) Vout[i * tp.plane_w + o + j] = sv[i][j];
+            }
+        } else if (nb + VPT <= tp.ns) {
 #pragma unroll
             for (int i = 0; i < K - 1; ++i) stv<VPT>(Vout + i * tp.plane_w + o, onew[i]);
         } else {
@@ -283,18 +326,18 @@ __device__ __forceinline__ void stage_a_chunk(const TiledSmem<K, R, NT, VPT> &sm
             for (int j = 0; j < VPT; ++j)
                 if (nb + j < tp.ns)
 #pragma unroll
-                    for (int i = 0; i < K - 1; ++i) Vout[i * tp.plane_w + o + j] = onew[i][j];
+                    for (int i = 0; i < K - 1; ++i) Vout[i * tp.plane_w + o + j] = Store<ST>::st(onew[i][j]);
         }
     }
 }
 
 // Stage A for the single slice n0+NT of tile row rr (the high halo along n).
-template <int K, int R, int NT, int VPT>
-__device__ __forceinline__ void stage_a_nhalo(const TiledSmem<K, R, NT, VPT> &sm, const TiledParams &tp,
+template <int K, int R, int NT, int VPT, typename ST>
+__device__ __forceinline__ void stage_a_nhalo(const TiledSmem<K, R, NT, VPT, ST> &sm, const TiledParams &tp,
                                               const PhaseParams<K> &pp, int p, int sc, int sp, int r0, int rr, int n0)
 {
-    using S = TileShape<K, R, NT, VPT>;
-    using T = TiledSmem<K, R, NT, VPT>;
+    using S = TileShape<K, R, NT, VPT, ST>;
+    using T = TiledSmem<K, R, NT, VPT, ST>;
     const int row = r0 + rr, n = n0 + NT;
     float *vb = sm.vb_plane(sc);
     const int4 ci = sm.cols()[p];
@@ -306,30 +349,31 @@ __device__ __forceinline__ void stage_a_nhalo(const TiledSmem<K, R, NT, VPT> &sm
     const bool pr = row > ci.y, hr = row + 1 < ci.z;
     const bool pc = row_in_col(sm.cols()[p - 1], row);
     const bool hc = row_in_col(sm.cols()[p + 1], row);
-    const float *xs = sm.xi_slot(sc), *xp = sm.xi_slot(sp);
+    const ST *xs = sm.xi_slot(sc), *xp = sm.xi_slot(sp);
+    constexpr int XN = NT + S::XH;  // slice n0+NT in the Xi box
     float xi[S::C3], xin[K - 1], xir[K - 1], xic[K - 1], v[K - 1], vn[K - 1], vbar[K - 1];
 #pragma unroll
-    for (int comp = 0; comp < S::C3; ++comp) xi[comp] = xs[T::xi_at(comp, rr + 1, NT + 4)];
+    for (int comp = 0; comp < S::C3; ++comp) xi[comp] = Store<ST>::ld(xs[T::xi_at(comp, rr + 1, XN)]);
 #pragma unroll
     for (int i = 0; i < K - 1; ++i) {
-        xin[i] = xs[T::xi_at(3 * i, rr + 1, NT + 3)];
-        xir[i] = xs[T::xi_at(3 * i + 1, rr, NT + 4)];
-        xic[i] = xp[T::xi_at(3 * i + 2, rr + 1, NT + 4)];
-        v[i] = sm.v_slot(sc)[T::v_at(i, rr, NT)];
+        xin[i] = Store<ST>::ld(xs[T::xi_at(3 * i, rr + 1, XN - 1)]);
+        xir[i] = Store<ST>::ld(xs[T::xi_at(3 * i + 1, rr, XN)]);
+        xic[i] = Store<ST>::ld(xp[T::xi_at(3 * i + 2, rr + 1, XN)]);
+        v[i] = Store<ST>::ld(sm.v_slot(sc)[T::vt_at(i, rr, NT)]);
     }
     const float uu = sm.u_slot(sc)[T::v_at(0, rr, NT)];
     primal_voxel<K>(vn, vbar, v, xi, xin, xir, xic, n > 0, n + 1 < tp.ns, pr, hr, pc, hc, uu, pp.c, pp.lam, pp.tau1);
 #pragma unroll
-    for (int i = 0; i < K - 1; ++i) vb[T::v_at(i, rr, NT)] = vbar[i];
+    for (int i = 0; i < K - 1; ++i) vb[T::v_at(i, rr, NT)] = Store<ST>::round(vbar[i]);
 }
 
 // The full Dykstra loop for 32 queued voxels (ring entries head .. head+31,
 // fewer when count < 32), results stored to Xout by the lane that ran it.
-template <int K, int R, int NT, int VPT>
+template <int K, int R, int NT, int VPT, typename ST>
 __device__ __forceinline__ void drain_queue(float *qq, int head, int count, const TiledParams &tp,
-                                            DykstraThresholds thr, float *__restrict__ Xout)
+                                            DykstraThresholds thr, ST *__restrict__ Xout)
 {
-    using S = TileShape<K, R, NT, VPT>;
+    using S = TileShape<K, R, NT, VPT, ST>;
     const int lane = threadIdx.x & 31;
     __syncwarp();
     if (lane < count) {
@@ -346,7 +390,7 @@ __device__ __forceinline__ void drain_queue(float *qq, int head, int count, cons
 #pragma unroll
         for (int i = 0; i < K - 1; ++i)
 #pragma unroll
-            for (int a = 0; a < 3; ++a) Xout[(3 * i + a) * tp.plane_w + o] = qe[i][a];
+            for (int a = 0; a < 3; ++a) Xout[(3 * i + a) * tp.plane_w + o] = Store<ST>::st(qe[i][a]);
     }
     __syncwarp();
 }
@@ -354,14 +398,14 @@ __device__ __forceinline__ void drain_queue(float *qq, int head, int count, cons
 // Stage B: dual step at ring position p (slot sc; slot sn holds plane p+1)
 // for VPT slices n0+VPT*q .. of tile row rr.  Called by every lane of the row
 // warps (warp-wide gathers); qhead/qcount describe the warp's ring queue.
-template <int K, int R, int NT, int VPT>
-__device__ __forceinline__ void stage_b_chunk(const TiledSmem<K, R, NT, VPT> &sm, const TiledParams &tp, int p,
+template <int K, int R, int NT, int VPT, typename ST>
+__device__ __forceinline__ void stage_b_chunk(const TiledSmem<K, R, NT, VPT, ST> &sm, const TiledParams &tp, int p,
                                               int sc, int sn, int r0, int rr, int n0, int q, float tau2,
-                                              DykstraThresholds thr, float *__restrict__ Xout, int &qhead,
+                                              DykstraThresholds thr, ST *__restrict__ Xout, int &qhead,
                                               int &qcount)
 {
-    using S = TileShape<K, R, NT, VPT>;
-    using T = TiledSmem<K, R, NT, VPT>;
+    using S = TileShape<K, R, NT, VPT, ST>;
+    using T = TiledSmem<K, R, NT, VPT, ST>;
     const int lane = threadIdx.x & 31;
     const int row = r0 + rr;
     const int4 ci = sm.cols()[p];
@@ -375,13 +419,14 @@ __device__ __forceinline__ void stage_b_chunk(const TiledSmem<K, R, NT, VPT> &sm
     if (live) {
         const bool hr = row + 1 < ci.z;
         const bool hc = row_in_col(sm.cols()[p + 1], row);
-        const float *xs = sm.xi_slot(sc);
+        const ST *xs = sm.xi_slot(sc);
         const float *vb0 = sm.vb_plane(sc), *vb1 = sm.vb_plane(sn);
+        constexpr int XH = S::XH;
         if constexpr (VPT == 2) {
             float2 x[S::C3], b[K - 1], bn[K - 1], br[K - 1], bc[K - 1], q2[K][3];
 #pragma unroll
             for (int comp = 0; comp < S::C3; ++comp)
-                x[comp] = reinterpret_cast<const float2 *>(xs)[T::xi_at(comp, rr + 1, off + 4) / 2];
+                x[comp] = Store<ST>::ld2(xs + T::xi_at(comp, rr + 1, off + XH));
 #pragma unroll
             for (int i = 0; i < K - 1; ++i) {
                 b[i] = reinterpret_cast<const float2 *>(vb0)[T::v_at(i, rr, off) / 2];
@@ -402,7 +447,7 @@ __device__ __forceinline__ void stage_b_chunk(const TiledSmem<K, R, NT, VPT> &sm
         } else {
             float x[S::C3][VPT], b[K - 1][VPT], bnext[K - 1], br[K - 1][VPT], bc[K - 1][VPT];
 #pragma unroll
-            for (int comp = 0; comp < S::C3; ++comp) ldv<VPT>(x[comp], xs + T::xi_at(comp, rr + 1, off + 4));
+            for (int comp = 0; comp < S::C3; ++comp) ldv<VPT>(x[comp], xs + T::xi_at(comp, rr + 1, off + XH));
 #pragma unroll
             for (int i = 0; i < K - 1; ++i) {
                 ldv<VPT>(b[i], vb0 + T::v_at(i, rr, off));
@@ -449,7 +494,7 @@ __device__ __forceinline__ void stage_b_chunk(const TiledSmem<K, R, NT, VPT> &sm
         }
         qcount += __popc(bal);
         if (qcount >= 32) {
-            drain_queue<K, R, NT, VPT>(qq, qhead, 32, tp, thr, Xout);
+            drain_queue<K, R, NT, VPT, ST>(qq, qhead, 32, tp, thr, Xout);
             qhead = (qhead + 32) & (S::QCAP - 1);
             qcount -= 32;
         }
@@ -473,19 +518,19 @@ __device__ __forceinline__ void stage_b_chunk(const TiledSmem<K, R, NT, VPT> &sm
 #pragma unroll
                 for (int i = 0; i < K - 1; ++i)
 #pragma unroll
-                    for (int a = 0; a < 3; ++a) Xout[(3 * i + a) * tp.plane_w + o + j] = qv[j][i][a];
+                    for (int a = 0; a < 3; ++a) Xout[(3 * i + a) * tp.plane_w + o + j] = Store<ST>::st(qv[j][i][a]);
     }
 }
 
-template <int K, int R, int NT, int VPT>
-__global__ void __launch_bounds__(TileShape<K, R, NT, VPT>::THREADS, 1)
+template <int K, int R, int NT, int VPT, typename ST>
+__global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
     fused_tiled_kernel(const __grid_constant__ CUtensorMap tm_xi, const __grid_constant__ CUtensorMap tm_v,
-                       const __grid_constant__ CUtensorMap tm_u, TiledParams tp, float *__restrict__ Xout,
-                       float *__restrict__ Vout, PhaseParams<K> pp, float tau2, DykstraThresholds thr, float *dq,
+                       const __grid_constant__ CUtensorMap tm_u, TiledParams tp, ST *__restrict__ Xout,
+                       ST *__restrict__ Vout, PhaseParams<K> pp, float tau2, DykstraThresholds thr, float *dq,
                        int *err)
 {
-    using S = TileShape<K, R, NT, VPT>;
-    using T = TiledSmem<K, R, NT, VPT>;
+    using S = TileShape<K, R, NT, VPT, ST>;
+    using T = TiledSmem<K, R, NT, VPT, ST>;
     extern __shared__ __align__(128) uint8_t smem_raw[];
     T sm;
     // align to 128 bytes by pointer arithmetic on the shared array itself, so
@@ -514,11 +559,11 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT>::THREADS, 1)
     }
     {  // Vbar planes start as zeros: a missing neighbour's value is multiplied by 0, so it must be finite
         float *vb = sm.vb_plane(0);
-        for (int i = tid; i < S::D * S::V_SLOT / 4; i += blockDim.x) vb[i] = 0.0f;
+        for (int i = tid; i < S::D * S::VB_SLOT / 4; i += blockDim.x) vb[i] = 0.0f;
     }
     if (ca - 1 < tp.col_begin) {  // no plane before the first column: its Xi slot reads as zeros
-        float *x0 = sm.xi_slot(0);
-        for (int i = tid; i < S::XI_BYTES / 4; i += blockDim.x) x0[i] = 0.0f;
+        uint32_t *x0 = reinterpret_cast<uint32_t *>(sm.xi_slot(0));
+        for (int i = tid; i < S::XI_SLOT / 4; i += blockDim.x) x0[i] = 0u;
     }
     __syncthreads();
 
@@ -543,11 +588,21 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT>::THREADS, 1)
                     const bool xi_only = p == 0;
                     mbar_arrive_expect_tx(sm.full(slot),
                                           S::XI_BYTES + (xi_only ? 0u : (uint32_t)(S::V_BYTES + S::U_BYTES)));
-                    tma_load_3d(sm.xi_slot(slot), &tm_xi, sm.full(slot), n0 - 4, line, 0);
+                    tma_load_3d(sm.xi_slot(slot), &tm_xi, sm.full(slot), n0 - S::XH, line, 0);
                     if (!xi_only) {
                         tma_load_3d(sm.v_slot(slot), &tm_v, sm.full(slot), n0, line + 1, 0);
                         tma_load_2d(sm.u_slot(slot), &tm_u, sm.full(slot), tp.u_x0 + n0, line + 1);
                     }
+                }
+                // L2 prefetch of the plane tp.prefetch positions ahead (the
+                // ring's depth bounds what is in flight into shared memory)
+                const int pf = p + tp.prefetch;
+                if (tp.prefetch > 0 && pf <= P && ca - 1 + pf >= tp.col_begin) {
+                    const int4 cf = sm.cols()[pf];
+                    const int lf = cf.x + (r0 - 1 - cf.y);
+                    tma_prefetch_l2_3d(&tm_xi, n0 - S::XH, lf, 0);
+                    tma_prefetch_l2_3d(&tm_v, n0, lf + 1, 0);
+                    tma_prefetch_l2_2d(&tm_u, tp.u_x0 + n0, lf + 1);
                 }
                 if (++slot == S::D) slot = 0, ph ^= 1u;
             }
@@ -570,9 +625,9 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT>::THREADS, 1)
                 if (ok) ok = mbar_wait_warp(sm.full(s_cur), ph_cur, abort);
                 if (!ok) break;
                 if (chunk_a)
-                    stage_a_chunk<K, R, NT, VPT>(sm, tp, pp, p, s_cur, s_prev, r0, rr, n0, q,
+                    stage_a_chunk<K, R, NT, VPT, ST>(sm, tp, pp, p, s_cur, s_prev, r0, rr, n0, q,
                                                  is_main && ca - 1 + p < cb, Vout, dqmax);
-                if (nhalo) stage_a_nhalo<K, R, NT, VPT>(sm, tp, pp, p, s_cur, s_prev, r0, hq, n0);
+                if (nhalo) stage_a_nhalo<K, R, NT, VPT, ST>(sm, tp, pp, p, s_cur, s_prev, r0, hq, n0);
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(sm.ready(s_cur));
@@ -581,7 +636,7 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT>::THREADS, 1)
                     // dual step at position p-1 once every warp's Vbar of that plane is in
                     ok = mbar_wait_warp(sm.ready(s_prev), ph_prev, abort);
                     if (!ok) break;
-                    stage_b_chunk<K, R, NT, VPT>(sm, tp, p - 1, s_prev, s_cur, r0, rr, n0, q, tau2, thr, Xout, qhead,
+                    stage_b_chunk<K, R, NT, VPT, ST>(sm, tp, p - 1, s_prev, s_cur, r0, rr, n0, q, tau2, thr, Xout, qhead,
                                                  qcount);
                 }
                 __syncwarp();
@@ -597,9 +652,9 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT>::THREADS, 1)
         if (ok && is_main && c_last == cb - 1) {
             ok = mbar_wait_warp(sm.ready(s_prev), ph_prev, abort);
             if (ok)
-                stage_b_chunk<K, R, NT, VPT>(sm, tp, P, s_prev, s_cur, r0, rr, n0, q, tau2, thr, Xout, qhead, qcount);
+                stage_b_chunk<K, R, NT, VPT, ST>(sm, tp, P, s_prev, s_cur, r0, rr, n0, q, tau2, thr, Xout, qhead, qcount);
         }
-        if (ok && is_main && qcount > 0) drain_queue<K, R, NT, VPT>(sm.queue(warp), qhead, qcount, tp, thr, Xout);
+        if (ok && is_main && qcount > 0) drain_queue<K, R, NT, VPT, ST>(sm.queue(warp), qhead, qcount, tp, thr, Xout);
     }
     __syncthreads();
     if (tid == 0 && *abort) atomicExch(err, 1);

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -288,11 +289,19 @@ int upload_lines(potts_context *ctx, const potts_mapping *map)
     return POTTS_OK;
 }
 
-// Where the state of one slab lives.
+// Where the state of one slab lives (stored as ST: float, bfloat16 or binary16).
+template <typename ST>
 struct SlabState {
-    float *xi[2];  // 3(K-1) planes each (ping-pong for the fused form)
-    float *v[2];   // K-1 planes each (v[1] is Vbar in the split form)
+    ST *xi[2];  // 3(K-1) planes each (ping-pong for the fused form)
+    ST *v[2];   // K-1 planes each (v[1] is Vbar in the split form)
 };
+
+// Storage format selected by potts_options::storage.
+template <typename ST>
+struct StoreInfo;
+template <> struct StoreInfo<float> { static constexpr CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT32; };
+template <> struct StoreInfo<__nv_bfloat16> { static constexpr CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16; };
+template <> struct StoreInfo<__half> { static constexpr CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT16; };
 
 int state_planes(int K, int variant)
 {
@@ -312,14 +321,14 @@ inline unsigned plain_blocks(const Geometry &g, int n_begin, int n_end)
     return (unsigned)(g.n_lines * chunks);
 }
 
-template <int K>
-int run_energy(potts_context *ctx, const Geometry &g, const float *xi, const float *V, const float *d_u,
+template <int K, typename ST>
+int run_energy(potts_context *ctx, const Geometry &g, const ST *xi, const ST *V, const float *d_u,
                const PhaseParams<K> &pp, double *out)
 {
     POTTS_TRY(seg_end(ctx));
     const unsigned nb = plain_blocks(g, 0, g.ns);
     ctx->total_launches += 2;
-    potts::energy_kernel<K><<<nb, potts::kPlainThreads, 0, ctx->stream>>>(g, xi, V, d_u, pp,
+    potts::energy_kernel<K, ST><<<nb, potts::kPlainThreads, 0, ctx->stream>>>(g, xi, V, d_u, pp,
                                                                           (double2 *)ctx->partial.p);
     potts::energy_finish<<<1, 1024, 0, ctx->stream>>>((const double2 *)ctx->partial.p, (int64_t)nb, out);
     POTTS_CUDA(cudaGetLastError());
@@ -365,9 +374,9 @@ EncodeTiledFn encode_fn()
     return fn;
 }
 
-// A float tensor of `rank` dims (dims[0] contiguous), strides in bytes of dims 1.., box per dim.
-int encode_map(CUtensorMap *m, const float *base, int rank, const uint64_t *dims, const uint64_t *strides,
-               const uint32_t *box)
+// A tensor of `rank` dims (dims[0] contiguous), strides in bytes of dims 1.., box per dim.
+int encode_map(CUtensorMap *m, CUtensorMapDataType dt, const void *base, int rank, const uint64_t *dims,
+               const uint64_t *strides, const uint32_t *box)
 {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return fail(POTTS_ECUDA, "cuTensorMapEncodeTiled is not available from the driver");
@@ -378,12 +387,15 @@ int encode_map(CUtensorMap *m, const float *base, int rank, const uint64_t *dims
         bd[i] = box[i];
     }
     for (int i = 0; i + 1 < rank; ++i) gs[i] = strides[i];
-    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank, const_cast<float *>(base), gd, gs, bd, es,
+    CUresult r = fn(m, dt, (cuuint32_t)rank, const_cast<void *>(base), gd, gs, bd, es,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(POTTS_ECUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
     return POTTS_OK;
 }
+
+// Planes of L2 prefetch ahead of the fused kernel's load ring.
+constexpr int kDefaultPrefetch = 2;
 
 struct TileChoice {
     int rows, slices, vpt, segment;
@@ -399,8 +411,10 @@ template <> struct TileShapes<4> { static constexpr int n = 2; static constexpr 
 template <> struct TileShapes<5> { static constexpr int n = 1; static constexpr int r[n] = {4}, t[n] = {64}, v[n] = {4}; };
 template <> struct TileShapes<6> { static constexpr int n = 1; static constexpr int r[n] = {4}, t[n] = {64}, v[n] = {4}; };
 
+// n_compiled: how many of the shapes (from the first) are compiled for the
+// storage format.
 template <int K>
-int choose_tile(const potts_options &o, TileChoice *tc)
+int choose_tile(const potts_options &o, int n_compiled, TileChoice *tc)
 {
     tc->rows = TileShapes<K>::r[0];
     tc->slices = TileShapes<K>::t[0];
@@ -408,7 +422,7 @@ int choose_tile(const potts_options &o, TileChoice *tc)
     tc->segment = o.segment_cols > 0 ? o.segment_cols : 64;
     if (tc->segment > 64) return fail(POTTS_EINVAL, "segment_cols must be <= 64");
     if (o.tile_rows > 0 || o.tile_slices > 0 || o.tile_vpt > 0) {
-        for (int i = 0; i < TileShapes<K>::n; ++i)
+        for (int i = 0; i < n_compiled; ++i)
             if ((o.tile_rows <= 0 || o.tile_rows == TileShapes<K>::r[i]) &&
                 (o.tile_slices <= 0 || o.tile_slices == TileShapes<K>::t[i]) &&
                 (o.tile_vpt <= 0 || o.tile_vpt == TileShapes<K>::v[i])) {
@@ -417,7 +431,8 @@ int choose_tile(const potts_options &o, TileChoice *tc)
                 tc->vpt = TileShapes<K>::v[i];
                 return POTTS_OK;
             }
-        return fail(POTTS_EINVAL, "tile_rows x tile_slices x tile_vpt is not a compiled tile shape for this K");
+        return fail(POTTS_EINVAL,
+                    "tile_rows x tile_slices x tile_vpt is not a compiled tile shape for this K and storage");
     }
     return POTTS_OK;
 }
@@ -492,57 +507,68 @@ struct FusedPlan {
     TileChoice tile{};
 };
 
-template <int K, int R, int NT, int VPT>
-int launch_tiled_shape(potts_context *ctx, const FusedPlan &fp, int in, float *Xout, float *Vout,
+template <int K, int R, int NT, int VPT, typename ST>
+int launch_tiled_shape(potts_context *ctx, const FusedPlan &fp, int in, ST *Xout, ST *Vout,
                        const PhaseParams<K> &pp, float tau2, float *dq)
 {
-    using S = potts::TileShape<K, R, NT, VPT>;
+    using S = potts::TileShape<K, R, NT, VPT, ST>;
     static bool attr_set = false;
     if (!attr_set) {
-        POTTS_CUDA(cudaFuncSetAttribute(potts::fused_tiled_kernel<K, R, NT, VPT>,
+        POTTS_CUDA(cudaFuncSetAttribute(potts::fused_tiled_kernel<K, R, NT, VPT, ST>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM_ALLOC));
         attr_set = true;
     }
     if (fp.n_work == 0) return POTTS_OK;
-    potts::fused_tiled_kernel<K, R, NT, VPT><<<fp.n_work, S::THREADS, S::SMEM_ALLOC, ctx->stream>>>(
+    potts::fused_tiled_kernel<K, R, NT, VPT, ST><<<fp.n_work, S::THREADS, S::SMEM_ALLOC, ctx->stream>>>(
         fp.xi[in], fp.v[in], fp.u, fp.tp, Xout, Vout, pp, tau2, ctx->thr, dq, (int *)ctx->err.p);
     POTTS_CUDA(cudaGetLastError());
     return POTTS_OK;
 }
 
-template <int K, int I = 0>
-int launch_tiled(potts_context *ctx, const FusedPlan &fp, int in, float *Xout, float *Vout, const PhaseParams<K> &pp,
+// FP32 storage compiles every tile shape of K; the 16-bit formats the default one.
+template <int K, typename ST>
+constexpr int compiled_shapes()
+{
+    return std::is_same<ST, float>::value ? TileShapes<K>::n : 1;
+}
+
+template <int K, typename ST, int I = 0>
+int launch_tiled(potts_context *ctx, const FusedPlan &fp, int in, ST *Xout, ST *Vout, const PhaseParams<K> &pp,
                  float tau2, float *dq)
 {
-    if constexpr (I < TileShapes<K>::n) {
+    if constexpr (I < compiled_shapes<K, ST>()) {
         constexpr int R = TileShapes<K>::r[I], NT = TileShapes<K>::t[I], VPT = TileShapes<K>::v[I];
         if (fp.tile.rows == R && fp.tile.slices == NT && fp.tile.vpt == VPT)
-            return launch_tiled_shape<K, R, NT, VPT>(ctx, fp, in, Xout, Vout, pp, tau2, dq);
-        return launch_tiled<K, I + 1>(ctx, fp, in, Xout, Vout, pp, tau2, dq);
+            return launch_tiled_shape<K, R, NT, VPT, ST>(ctx, fp, in, Xout, Vout, pp, tau2, dq);
+        return launch_tiled<K, ST, I + 1>(ctx, fp, in, Xout, Vout, pp, tau2, dq);
     } else {
         return fail(POTTS_EINVAL, "no compiled tile shape matches");
     }
 }
 
-template <int K>
-int prepare_fused(potts_context *ctx, const Geometry &g, const float *const xi[2], const float *const v[2],
+template <int K, typename ST>
+int prepare_fused(potts_context *ctx, const Geometry &g, const ST *const xi[2], const ST *const v[2],
                   const float *d_u, const potts_options &o, FusedPlan *fp)
 {
-    POTTS_TRY(choose_tile<K>(o, &fp->tile));
+    POTTS_TRY(choose_tile<K>(o, compiled_shapes<K, ST>(), &fp->tile));
     if (g.plane_w >= (int64_t(1) << 31))
         return fail(POTTS_EINVAL, "a state plane of 2^31 voxels or more needs slabs (set slab_w)");
     const int R = fp->tile.rows, NT = fp->tile.slices;
     POTTS_TRY(plan_tiles(ctx, g.ns, fp->tile));
     fp->n_work = ctx->n_work;
     const uint64_t L = (uint64_t)g.n_lines;
+    // boxes as in potts::TileShape: Xi slices n0-XH .. n0+NT+XH-1, V slices
+    // n0 .. n0+NT+3 (FP32) or n0+NT+7 (16-bit), whole 16-byte rows
+    constexpr uint64_t es = sizeof(ST);
+    constexpr int XH = es == 4 ? 4 : 8;
     for (int b = 0; b < 2; ++b) {
         const uint64_t dx[3] = {(uint64_t)g.nstride_w, L, (uint64_t)(3 * (K - 1))};
-        const uint64_t sx[2] = {(uint64_t)g.nstride_w * 4, (uint64_t)g.plane_w * 4};
-        const uint32_t bx[3] = {(uint32_t)(NT + 8), (uint32_t)(R + 2), (uint32_t)(3 * (K - 1))};
-        POTTS_TRY(encode_map(&fp->xi[b], xi[b], 3, dx, sx, bx));
+        const uint64_t sx[2] = {(uint64_t)g.nstride_w * es, (uint64_t)g.plane_w * es};
+        const uint32_t bx[3] = {(uint32_t)(NT + 2 * XH), (uint32_t)(R + 2), (uint32_t)(3 * (K - 1))};
+        POTTS_TRY(encode_map(&fp->xi[b], StoreInfo<ST>::dt, xi[b], 3, dx, sx, bx));
         const uint64_t dv[3] = {(uint64_t)g.nstride_w, L, (uint64_t)(K - 1)};
-        const uint32_t bv[3] = {(uint32_t)(NT + 4), (uint32_t)(R + 1), (uint32_t)(K - 1)};
-        POTTS_TRY(encode_map(&fp->v[b], v[b], 3, dv, sx, bv));
+        const uint32_t bv[3] = {(uint32_t)(NT + (es == 4 ? 4 : 8)), (uint32_t)(R + 1), (uint32_t)(K - 1)};
+        POTTS_TRY(encode_map(&fp->v[b], StoreInfo<ST>::dt, v[b], 3, dv, sx, bv));
     }
     // u: read in place when the slab's slices start on a 16-byte boundary,
     // else staged into a buffer with the state's stride
@@ -563,7 +589,7 @@ int prepare_fused(potts_context *ctx, const Geometry &g, const float *const xi[2
     const uint64_t du[2] = {ustride, L};
     const uint64_t su[1] = {ustride * 4};
     const uint32_t bu[2] = {(uint32_t)(NT + 4), (uint32_t)(R + 1)};
-    POTTS_TRY(encode_map(&fp->u, ubase, 2, du, su, bu));
+    POTTS_TRY(encode_map(&fp->u, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, ubase, 2, du, su, bu));
     fp->tp.cols = (const int4 *)ctx->cols.p;
     fp->tp.work = (const int4 *)ctx->work.p;
     fp->tp.col_begin = (int)ctx->mapping.m.col_begin;
@@ -572,17 +598,20 @@ int prepare_fused(potts_context *ctx, const Geometry &g, const float *const xi[2
     fp->tp.nstride_w = g.nstride_w;
     fp->tp.plane_w = g.plane_w;
     fp->tp.u_x0 = ux0;
+    fp->tp.n_base = g.slab_start;
+    fp->tp.it = 0;
+    fp->tp.prefetch = o.prefetch < 0 ? 0 : (o.prefetch == 0 ? kDefaultPrefetch : o.prefetch);
     return POTTS_OK;
 }
 
 // One slab: init, iters iterations, argmax of [res_begin, res_end).
-template <int K>
+template <int K, typename ST>
 int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const PhaseParams<K> &pp, float tau2,
-             int iters, const potts_options &o, const SlabState &st, int res_begin, int res_end, const Outputs &out,
-             int64_t plane_out)
+             int iters, const potts_options &o, const SlabState<ST> &st, int res_begin, int res_end,
+             const Outputs &out, int64_t plane_out)
 {
     const unsigned nb = plain_blocks(g, 0, g.ns);
-    const size_t xi_bytes = sizeof(float) * 3 * (K - 1) * (size_t)g.plane_w;
+    const size_t xi_bytes = sizeof(ST) * 3 * (K - 1) * (size_t)g.plane_w;
     float *dq = o.track_dq ? (float *)ctx->dq.p : nullptr;
     double *energy = (double *)ctx->energy.p;
     const int ge = o.gap_every;
@@ -591,14 +620,14 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
 
     int cur = 0;
     if (o.variant == POTTS_VARIANT_PLAIN) {
-        float *xi = st.xi[0], *V = st.v[0], *Vb = st.v[1];
-        potts::init_kernel<K><<<nb, potts::kPlainThreads, 0, s>>>(g, d_u, V, Vb, pp);
+        ST *xi = st.xi[0], *V = st.v[0], *Vb = st.v[1];
+        potts::init_kernel<K, ST><<<nb, potts::kPlainThreads, 0, s>>>(g, d_u, V, Vb, pp);
         ctx->total_launches += 1;
         POTTS_CUDA(cudaMemsetAsync(xi, 0, xi_bytes, s));
         for (int it = 0; it < iters; ++it) {
             POTTS_TRY(seg_begin(ctx));
-            potts::dual_kernel<K><<<nb, potts::kPlainThreads, 0, s>>>(g, xi, Vb, tau2, ctx->thr);
-            potts::primal_kernel<K><<<nb, potts::kPlainThreads, 0, s>>>(g, xi, V, Vb, d_u, pp, dq ? dq + it : nullptr);
+            potts::dual_kernel<K, ST><<<nb, potts::kPlainThreads, 0, s>>>(g, xi, Vb, tau2, ctx->thr);
+            potts::primal_kernel<K, ST><<<nb, potts::kPlainThreads, 0, s>>>(g, xi, V, Vb, d_u, pp, dq ? dq + it : nullptr, it);
             ctx->loop_launches += 2;
             ctx->total_launches += 2;
             if (ge > 0 && (it + 1) % ge == 0) POTTS_TRY(run_energy<K>(ctx, g, xi, V, d_u, pp, energy + 3 * ((it + 1) / ge - 1)));
@@ -612,15 +641,15 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
         // primal step gives V^iters from Xi^iters.
         // the tiled kernel reads (and multiplies by zero) padding and stale
         // neighbours: keep all of the state finite
-        POTTS_CUDA(cudaMemsetAsync(st.xi[0], 0, sizeof(float) * 8 * (K - 1) * (size_t)g.plane_w, s));
+        POTTS_CUDA(cudaMemsetAsync(st.xi[0], 0, sizeof(ST) * 8 * (K - 1) * (size_t)g.plane_w, s));
         FusedPlan fp;
-        const float *xs[2] = {st.xi[0], st.xi[1]}, *vs[2] = {st.v[0], st.v[1]};
-        if (iters > 1) POTTS_TRY(prepare_fused<K>(ctx, g, xs, vs, d_u, o, &fp));
-        potts::init_kernel<K><<<nb, potts::kPlainThreads, 0, s>>>(g, d_u, st.v[0], nullptr, pp);
+        const ST *xs[2] = {st.xi[0], st.xi[1]}, *vs[2] = {st.v[0], st.v[1]};
+        if (iters > 1) POTTS_TRY((prepare_fused<K, ST>(ctx, g, xs, vs, d_u, o, &fp)));
+        potts::init_kernel<K, ST><<<nb, potts::kPlainThreads, 0, s>>>(g, d_u, st.v[0], (ST *)nullptr, pp);
         ctx->total_launches += 1;
         POTTS_CUDA(cudaMemsetAsync(st.xi[0], 0, xi_bytes, s));
         if (iters > 0) {
-            potts::dual_kernel<K><<<nb, potts::kPlainThreads, 0, s>>>(g, st.xi[0], st.v[0], tau2, ctx->thr);
+            potts::dual_kernel<K, ST><<<nb, potts::kPlainThreads, 0, s>>>(g, st.xi[0], st.v[0], tau2, ctx->thr);
             ctx->total_launches += 1;
         }
         for (int m = 1; m < iters; ++m) {
@@ -628,7 +657,8 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
             POTTS_TRY(seg_begin(ctx));
             ctx->loop_launches += 1;
             ctx->total_launches += 1;
-            POTTS_TRY(launch_tiled<K>(ctx, fp, cur, st.xi[nxt], st.v[nxt], pp, tau2, dq ? dq + (m - 1) : nullptr));
+            fp.tp.it = m - 1;
+            POTTS_TRY((launch_tiled<K, ST>)(ctx, fp, cur, st.xi[nxt], st.v[nxt], pp, tau2, dq ? dq + (m - 1) : nullptr));
             if (ge > 0 && m % ge == 0) POTTS_TRY(run_energy<K>(ctx, g, st.xi[cur], st.v[nxt], d_u, pp, energy + 3 * (m / ge - 1)));
             if (o.sync_monitor && dq) POTTS_TRY(monitor_sync<K>(ctx, m - 1));
             cur = nxt;
@@ -636,8 +666,8 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
         POTTS_TRY(seg_end(ctx));
         if (iters > 0) {
             ctx->total_launches += 1;
-            potts::primal_kernel<K><<<nb, potts::kPlainThreads, 0, s>>>(g, st.xi[cur], st.v[cur], nullptr, d_u, pp,
-                                                                        dq ? dq + (iters - 1) : nullptr);
+            potts::primal_kernel<K, ST><<<nb, potts::kPlainThreads, 0, s>>>(
+                g, st.xi[cur], st.v[cur], (ST *)nullptr, d_u, pp, dq ? dq + (iters - 1) : nullptr, iters - 1);
             if (ge > 0 && iters % ge == 0) POTTS_TRY(run_energy<K>(ctx, g, st.xi[cur], st.v[cur], d_u, pp, energy + 3 * (iters / ge - 1)));
             if (o.sync_monitor && dq) POTTS_TRY(monitor_sync<K>(ctx, iters - 1));
         }
@@ -646,16 +676,16 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
     if (res_end > res_begin) {
         const unsigned nbu = plain_blocks(g, res_begin, res_end);
         ctx->total_launches += 1;
-        const float *Vf = o.variant == POTTS_VARIANT_PLAIN ? st.v[0] : st.v[cur];
-        const float *Xf = o.variant == POTTS_VARIANT_PLAIN ? st.xi[0] : st.xi[cur];
-        potts::update_kernel<K><<<nbu, potts::kPlainThreads, 0, s>>>(g, Vf, Xf, pp, res_begin, res_end, out.res,
+        const ST *Vf = o.variant == POTTS_VARIANT_PLAIN ? st.v[0] : st.v[cur];
+        const ST *Xf = o.variant == POTTS_VARIANT_PLAIN ? st.xi[0] : st.xi[cur];
+        potts::update_kernel<K, ST><<<nbu, potts::kPlainThreads, 0, s>>>(g, Vf, Xf, pp, res_begin, res_end, out.res,
                                                                       out.labels, out.V, out.Xi, plane_out);
         POTTS_CUDA(cudaGetLastError());
     }
     return POTTS_OK;
 }
 
-template <int K>
+template <int K, typename ST>
 int solve_k(potts_context *ctx, const float *d_u, const float *ci, float lam, float tau1, float tau2, int iters,
             const potts_options &o, const Outputs &out, potts_stats *stats)
 {
@@ -669,7 +699,7 @@ int solve_k(potts_context *ctx, const float *d_u, const float *ci, float lam, fl
     POTTS_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t margin = size_t(512) << 20;
     const size_t avail = free_b + ctx->state.bytes > margin ? free_b + ctx->state.bytes - margin : 0;
-    const uint64_t bytes_per_slice = sizeof(float) * (uint64_t)planes * (uint64_t)std::max<int64_t>(mc.n_lines, 1);
+    const uint64_t bytes_per_slice = sizeof(ST) * (uint64_t)planes * (uint64_t)std::max<int64_t>(mc.n_lines, 1);
     int slab_w = o.slab_w > 0 ? o.slab_w : (int)std::min<uint64_t>(prev_stride(avail / bytes_per_slice), 0x7fffffe0u);
     const int halo = iters;
     int res_w = n, n_slabs = 1;
@@ -684,7 +714,7 @@ int solve_k(potts_context *ctx, const float *d_u, const float *ci, float lam, fl
 
     const int nstride_w = (int)get_stride((uint32_t)slab_w);
     const int64_t plane_w = mc.n_lines * (int64_t)nstride_w;
-    const size_t state_bytes = sizeof(float) * (size_t)planes * (size_t)std::max<int64_t>(plane_w, 1);
+    const size_t state_bytes = sizeof(ST) * (size_t)planes * (size_t)std::max<int64_t>(plane_w, 1);
     POTTS_TRY(ensure(ctx, ctx->state, state_bytes));
     POTTS_TRY(ensure(ctx, ctx->dq, sizeof(float) * (size_t)std::max(iters, 1)));
     const int n_energy = o.gap_every > 0 ? iters / o.gap_every : 0;
@@ -694,8 +724,8 @@ int solve_k(potts_context *ctx, const float *d_u, const float *ci, float lam, fl
         POTTS_TRY(ensure(ctx, ctx->partial, sizeof(double2) * (size_t)std::max<int64_t>(mc.n_lines * chunks, 1)));
     }
 
-    float *base = (float *)ctx->state.p;
-    SlabState st;
+    ST *base = (ST *)ctx->state.p;
+    SlabState<ST> st;
     const size_t xi_planes = 3 * (K - 1), v_planes = K - 1;
     st.xi[0] = base;
     if (o.variant == POTTS_VARIANT_PLAIN) {
@@ -734,7 +764,7 @@ int solve_k(potts_context *ctx, const float *d_u, const float *ci, float lam, fl
         const int r0 = (s0 == 0) ? s0 : s0 + halo;
         const int r1 = (s1 == n) ? s1 : s1 - halo;
         if (mc.n_lines > 0)
-            POTTS_TRY(run_slab<K>(ctx, g, d_u, pp, tau2, iters, o, st, r0 - s0, r1 - s0, out, (int64_t)mc.span));
+            POTTS_TRY((run_slab<K, ST>)(ctx, g, d_u, pp, tau2, iters, o, st, r0 - s0, r1 - s0, out, (int64_t)mc.span));
     }
     POTTS_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
 
@@ -775,11 +805,27 @@ int check_params(int K, const float *ci, float lam, float tau1, float tau2, int 
     if (iters < 0) return fail(POTTS_EINVAL, "iters must be >= 0");
     if (o.variant != POTTS_VARIANT_FUSED && o.variant != POTTS_VARIANT_PLAIN)
         return fail(POTTS_EINVAL, "unknown variant");
-    if (o.storage != POTTS_STORE_F32) return fail(POTTS_EINVAL, "unknown storage");
+    if (o.storage != POTTS_STORE_F32 && o.storage != POTTS_STORE_BF16 && o.storage != POTTS_STORE_F16)
+        return fail(POTTS_EINVAL, "unknown storage");
     if (o.gap_every < 0 || o.slab_w < 0) return fail(POTTS_EINVAL, "gap_every and slab_w must be >= 0");
     if (o.tile_rows < 0 || o.tile_slices < 0 || o.segment_cols < 0 || o.tile_vpt < 0)
         return fail(POTTS_EINVAL, "tile options must be >= 0");
+    if (o.prefetch > 16) return fail(POTTS_EINVAL, "prefetch must be <= 16");
     return POTTS_OK;
+}
+
+template <typename ST>
+int solve_store(potts_context *ctx, const float *d_u, int K, const float *ci, float lam, float tau1, float tau2,
+                int iters, const potts_options &o, const Outputs &out, potts_stats *stats)
+{
+    switch (K) {
+    case 2: return solve_k<2, ST>(ctx, d_u, ci, lam, tau1, tau2, iters, o, out, stats);
+    case 3: return solve_k<3, ST>(ctx, d_u, ci, lam, tau1, tau2, iters, o, out, stats);
+    case 4: return solve_k<4, ST>(ctx, d_u, ci, lam, tau1, tau2, iters, o, out, stats);
+    case 5: return solve_k<5, ST>(ctx, d_u, ci, lam, tau1, tau2, iters, o, out, stats);
+    case 6: return solve_k<6, ST>(ctx, d_u, ci, lam, tau1, tau2, iters, o, out, stats);
+    }
+    return fail(POTTS_EINVAL, "K must be in [2, 6]");
 }
 
 int solve_dispatch(potts_context *ctx, const potts_mapping *map, const float *d_u, int K, const float *ci,
@@ -794,14 +840,9 @@ int solve_dispatch(potts_context *ctx, const potts_mapping *map, const float *d_
     if (!d_u) return fail(POTTS_EINVAL, "u is NULL");
     POTTS_CUDA(cudaSetDevice(ctx->device));
     POTTS_TRY(upload_lines(ctx, map));
-    switch (K) {
-    case 2: return solve_k<2>(ctx, d_u, ci, lam, tau1, tau2, iters, o, out, stats);
-    case 3: return solve_k<3>(ctx, d_u, ci, lam, tau1, tau2, iters, o, out, stats);
-    case 4: return solve_k<4>(ctx, d_u, ci, lam, tau1, tau2, iters, o, out, stats);
-    case 5: return solve_k<5>(ctx, d_u, ci, lam, tau1, tau2, iters, o, out, stats);
-    case 6: return solve_k<6>(ctx, d_u, ci, lam, tau1, tau2, iters, o, out, stats);
-    }
-    return fail(POTTS_EINVAL, "K must be in [2, 6]");
+    if (o.storage == POTTS_STORE_BF16) return solve_store<__nv_bfloat16>(ctx, d_u, K, ci, lam, tau1, tau2, iters, o, out, stats);
+    if (o.storage == POTTS_STORE_F16) return solve_store<__half>(ctx, d_u, K, ci, lam, tau1, tau2, iters, o, out, stats);
+    return solve_store<float>(ctx, d_u, K, ci, lam, tau1, tau2, iters, o, out, stats);
 }
 
 int context_init(int device, void *stream, bool use_stream, potts_context **out)
@@ -855,6 +896,7 @@ void potts_default_options(potts_options *o)
     o->tile_slices = 0;
     o->segment_cols = 0;
     o->tile_vpt = 0;
+    o->prefetch = 0;
 }
 
 const char *potts_status_string(int s)

@@ -109,6 +109,22 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const void *tmap, uint64_
         : "memory");
 }
 
+// Bulk prefetch of a tensor box into L2 (no shared memory, no barrier): the
+// later TMA load of the same box then reads from L2.
+__device__ __forceinline__ void tma_prefetch_l2_2d(const void *tmap, int x, int y)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];"
+                 ::"l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tma_prefetch_l2_3d(const void *tmap, int x, int y, int z)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];"
+                 ::"l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
+
 __device__ __forceinline__ void tma_prefetch_desc(const void *tmap)
 {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tmap)) : "memory");

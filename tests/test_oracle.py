@@ -191,3 +191,39 @@ def test_golden_small_solve(oracle_mod):
     assert np.array_equal(r.labels, z["labels"])
     np.testing.assert_array_equal(r.V, z["V"])
     np.testing.assert_array_equal(r.dq_trace, z["dq_trace"])
+
+
+# --------------------------------------------------------------------------- storage formats
+def _bf16_representable(x):
+    b = np.ascontiguousarray(x, np.float32).view(np.uint32)
+    return np.all((b & 0xFFFF) == 0)
+
+
+def test_store_formats_round_every_stored_value(oracle_mod):
+    m, u, ci = random_volume(20, 14, 14, 6.3, 4, seed=40)
+    mv = m.mask_values
+    a = oracle_mod.solve(m, u, ci, 30.0, TAU, TAU, 12, precision="f32")
+    f = oracle_mod.solve(m, u, ci, 30.0, TAU, TAU, 12, precision="f32", store="f32")
+    assert np.array_equal(a.V, f.V) and np.array_equal(a.Xi, f.Xi)
+    b = oracle_mod.solve(m, u, ci, 30.0, TAU, TAU, 12, precision="f32", store="bf16")
+    assert _bf16_representable(mv(b.V)) and _bf16_representable(mv(b.Xi))
+    h = oracle_mod.solve(m, u, ci, 30.0, TAU, TAU, 12, precision="f32", store="f16")
+    for x in (mv(h.V), mv(h.Xi)):
+        assert np.array_equal(x.astype(np.float16).astype(np.float32), x)
+    # a solve close to the FP32 one, not identical to it
+    for r, tol in ((b, 2e-2), (h, 3e-3)):
+        rel = np.linalg.norm(mv(r.V) - mv(a.V)) / np.linalg.norm(mv(a.V))
+        assert 0 < rel < tol
+
+
+def test_bf16_store_is_reproducible_and_keyed_by_global_slice(oracle_mod):
+    """The stochastic rounding of V depends on (line, global n, iteration, pair) only: slab cuts do
+    not change the kept interior."""
+    m, u, ci = random_volume(70, 14, 14, 6.1, 3, seed=6)
+    mv = m.mask_values
+    x = oracle_mod.solve(m, u, ci, 30.0, TAU, TAU, 6, precision="f32", store="bf16", want_state=False)
+    y = oracle_mod.solve(m, u, ci, 30.0, TAU, TAU, 6, precision="f32", store="bf16", want_state=False)
+    s = oracle_mod.solve(m, u, ci, 30.0, TAU, TAU, 6, precision="f32", store="bf16", slab_w=32,
+                         want_state=False)
+    assert np.array_equal(mv(x.res), mv(y.res)) and np.array_equal(mv(x.labels), mv(y.labels))
+    assert np.array_equal(mv(s.labels), mv(x.labels))
