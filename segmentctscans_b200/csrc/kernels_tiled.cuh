@@ -84,9 +84,13 @@ struct TileShape {
     static constexpr int MAIN_WARPS = MAIN / 32;
     static constexpr int HALO_WARPS = (Q + 31) / 32;  // the high halo row (and the slice n0+NT)
     static constexpr int PRODUCER_WARP = MAIN_WARPS + HALO_WARPS;
-    static constexpr int THREADS = MAIN + 32 * HALO_WARPS + 32;
+    // Dykstra warps run the projection loop of queued voxels; row warp r
+    // queues for Dykstra warp r % NW
+    static constexpr int NW = MAIN_WARPS >= 12 ? 6 : (MAIN_WARPS >= 2 ? MAIN_WARPS / 2 : 1);
+    static constexpr int DYKSTRA_WARP = PRODUCER_WARP + 1;  // the first one
+    static constexpr int THREADS = MAIN + 32 * HALO_WARPS + 32 + 32 * NW;
     static constexpr int QSTRIDE = (3 * K + 1) | 1;  // queue entry: q (3K floats) + state offset; odd stride
-    static constexpr int QCAP = 64;                    // ring of one pass (32) + one gather round (32)
+    static constexpr int QN = 128;                     // entries of each Dykstra warp's queue (a power of 2)
     static constexpr int XI_BYTES = C3 * (R + 2) * NX * ES;
     static constexpr int V_BYTES = C1 * (R + 1) * NVT * ES;
     static constexpr int U_BYTES = (R + 1) * NV * 4;
@@ -98,10 +102,12 @@ struct TileShape {
     static constexpr int OFF_U = OFF_V + D * V_SLOT;
     static constexpr int OFF_VB = OFF_U + D * U_SLOT;
     static constexpr int OFF_Q = OFF_VB + D * VB_SLOT;
+    static constexpr int OFF_QSEQ = OFF_Q + al(NW * QN * QSTRIDE * 4);
+    static constexpr int OFF_QCTL = OFF_QSEQ + al(NW * QN * 4);  // per queue: tail, head, finished writers
     static constexpr int MAX_SEGMENT = 64;  // columns per work item
-    static constexpr int OFF_COLS = OFF_Q + al(MAIN_WARPS * QCAP * QSTRIDE * 4);
+    static constexpr int OFF_COLS = OFF_QCTL + al(NW * 16);
     static constexpr int OFF_BAR = OFF_COLS + al((MAX_SEGMENT + 3) * 16);
-    static constexpr int SMEM = OFF_BAR + 3 * D * 8 + 16;
+    static constexpr int SMEM = OFF_BAR + 3 * D * 8 + 16;  // + abort flag
     static constexpr int SMEM_ALLOC = SMEM + 128;  // room to align the base to 128 bytes
     static_assert((VPT == 2 || VPT == 4) && NT % VPT == 0 && R + 1 <= 32, "tile shape");
     static_assert(MAIN % 32 == 0, "row threads fill whole warps");
@@ -158,9 +164,34 @@ struct TiledSmem {
     {
         return reinterpret_cast<float *>(base + S::OFF_VB + slot * S::VB_SLOT);
     }
-    __device__ __forceinline__ float *queue(int warp) const
+    // queue w of voxels waiting for the projection loop: entry data, and per
+    // entry the ticket + 1 of the last entry written there
+    __device__ __forceinline__ float *queue_entry(int w, uint32_t ticket) const
     {
-        return reinterpret_cast<float *>(base + S::OFF_Q) + warp * S::QCAP * S::QSTRIDE;
+        return reinterpret_cast<float *>(base + S::OFF_Q) + (w * S::QN + (ticket & (S::QN - 1))) * S::QSTRIDE;
+    }
+    __device__ __forceinline__ volatile uint32_t *queue_seq(int w, uint32_t ticket) const
+    {
+        return reinterpret_cast<volatile uint32_t *>(base + S::OFF_QSEQ) + w * S::QN + (ticket & (S::QN - 1));
+    }
+    // counters of queue w: tickets handed out to writers, tickets taken by
+    // its Dykstra warp, and row warps writing to it that have finished
+    __device__ __forceinline__ uint32_t *q_tail(int w) const
+    {
+        return reinterpret_cast<uint32_t *>(base + S::OFF_QCTL) + 4 * w;
+    }
+    __device__ __forceinline__ volatile uint32_t *q_head(int w) const
+    {
+        return reinterpret_cast<volatile uint32_t *>(base + S::OFF_QCTL) + 4 * w + 1;
+    }
+    __device__ __forceinline__ uint32_t *q_done(int w) const
+    {
+        return reinterpret_cast<uint32_t *>(base + S::OFF_QCTL) + 4 * w + 2;
+    }
+    // row warps that write to queue w
+    __device__ __forceinline__ static uint32_t q_writers(int w)
+    {
+        return (uint32_t)((S::MAIN_WARPS - 1 - w) / S::NW + 1);
     }
     __device__ __forceinline__ uint64_t *full(int slot) const
     {
@@ -367,42 +398,106 @@ __device__ __forceinline__ void stage_a_nhalo(const TiledSmem<K, R, NT, VPT, ST>
     for (int i = 0; i < K - 1; ++i) vb[T::v_at(i, rr, NT)] = Store<ST>::round(vbar[i]);
 }
 
-// The full Dykstra loop for 32 queued voxels (ring entries head .. head+31,
-// fewer when count < 32), results stored to Xout by the lane that ran it.
+// The Dykstra warp: runs the projection loop of the voxels that the row warps
+// queue.  Each lane takes one voxel, runs it a sweep at a time and, once it is
+// done, stores the result and takes the next waiting ticket, so that the loop
+// work of the block proceeds beside the stencil instead of stalling a row
+// warp.  It returns when every row warp has finished and the queue is empty,
+// or when the block aborts.  Every wait is bounded.
+constexpr int kQueueSpin = 1 << 20;   // polls of an entry's publication flag
+constexpr int kIdleRounds = 1 << 24;  // idle polls (~200 ns each) while the row warps work
+
 template <int K, int R, int NT, int VPT, typename ST>
-__device__ __forceinline__ void drain_queue(float *qq, int head, int count, const TiledParams &tp,
-                                            DykstraThresholds thr, ST *__restrict__ Xout)
+__device__ __forceinline__ void dykstra_worker(const TiledSmem<K, R, NT, VPT, ST> &sm, int w, const TiledParams &tp,
+                                               DykstraThresholds thr, ST *__restrict__ Xout, volatile int *abort)
 {
     using S = TileShape<K, R, NT, VPT, ST>;
+    constexpr int kPairs = K * (K - 1) / 2;
     const int lane = threadIdx.x & 31;
-    __syncwarp();
-    if (lane < count) {
-        const float *ent = qq + ((head + lane) & (S::QCAP - 1)) * S::QSTRIDE;
-        float qe[K][3];
+    const unsigned below = (1u << lane) - 1u;
+    using T = TiledSmem<K, R, NT, VPT, ST>;
+    volatile uint32_t *tail_v = sm.q_tail(w);
+    volatile uint32_t *done_v = sm.q_done(w);
+    float qe[K][3], P[kPairs][3];
+    int64_t o = 0;
+    int sweeps = 0;
+    bool active = false;
+    uint32_t next = 0;  // next ticket to hand out (the same in every lane)
+    int idle_rounds = 0;
+    while (true) {
+        const uint32_t tail = __shfl_sync(0xffffffffu, *tail_v, 0);
+        const unsigned idle = __ballot_sync(0xffffffffu, !active);
+        const uint32_t avail = tail - next;
+        if (avail > 0u && idle != 0u) {
+            const uint32_t take = min((uint32_t)__popc(idle), avail);
+            const uint32_t rank = (uint32_t)__popc(idle & below);
+            if (!active && rank < take) {
+                const uint32_t ticket = next + rank;
+                volatile uint32_t *seq = sm.queue_seq(w, ticket);
+                int spins = 0;
+                bool published = *seq == ticket + 1u;
+                while (!published && spins < kQueueSpin && !*abort) {
+                    ++spins;
+                    published = *seq == ticket + 1u;
+                }
+                if (published) {
+                    __threadfence_block();
+                    const float *ent = sm.queue_entry(w, ticket);
 #pragma unroll
-        for (int i = 0; i < K; ++i) {
-            qe[i][0] = ent[3 * i];
-            qe[i][1] = ent[3 * i + 1];
-            qe[i][2] = ent[3 * i + 2];
+                    for (int i = 0; i < K; ++i) {
+                        qe[i][0] = ent[3 * i];
+                        qe[i][1] = ent[3 * i + 1];
+                        qe[i][2] = ent[3 * i + 2];
+                    }
+                    o = (int64_t)(uint32_t)__float_as_int(ent[3 * K]);
+#pragma unroll
+                    for (int p = 0; p < kPairs; ++p) P[p][0] = P[p][1] = P[p][2] = 0.0f;
+                    sweeps = 0;
+                    active = true;
+                } else {
+                    *abort = 1;
+                }
+            }
+            next += take;
+            __threadfence_block();
+            __syncwarp();
+            if (lane == 0) *sm.q_head(w) = next;  // the taken entries' slots are free again
         }
-        const int64_t o = (int64_t)(uint32_t)__float_as_int(ent[3 * K]);
-        dual_project<K>(qe, thr);
+        if (!__any_sync(0xffffffffu, active)) {
+            if (__shfl_sync(0xffffffffu, *abort, 0)) break;
+            // a row warp publishes its last entries before it counts itself done
+            const bool finished =
+                __shfl_sync(0xffffffffu, (int)(*done_v == T::q_writers(w) && *tail_v == next), 0) != 0;
+            if (finished) break;
+            if (++idle_rounds > kIdleRounds) {
+                *abort = 1;
+                break;
+            }
+            __nanosleep(200);
+            continue;
+        }
+        idle_rounds = 0;
+        if (active) {
+            const bool exit = dykstra_sweep<K>(qe, P, thr);
+            if (exit || ++sweeps == 20) {
 #pragma unroll
-        for (int i = 0; i < K - 1; ++i)
+                for (int i = 0; i < K - 1; ++i)
 #pragma unroll
-            for (int a = 0; a < 3; ++a) Xout[(3 * i + a) * tp.plane_w + o] = Store<ST>::st(qe[i][a]);
+                    for (int a = 0; a < 3; ++a) Xout[(3 * i + a) * tp.plane_w + o] = Store<ST>::st(qe[i][a]);
+                active = false;
+            }
+        }
     }
-    __syncwarp();
 }
 
 // Stage B: dual step at ring position p (slot sc; slot sn holds plane p+1)
 // for VPT slices n0+VPT*q .. of tile row rr.  Called by every lane of the row
-// warps (warp-wide gathers); qhead/qcount describe the warp's ring queue.
+// warps (warp-wide ballots); voxels that need the projection loop go to the
+// block's queue.
 template <int K, int R, int NT, int VPT, typename ST>
 __device__ __forceinline__ void stage_b_chunk(const TiledSmem<K, R, NT, VPT, ST> &sm, const TiledParams &tp, int p,
                                               int sc, int sn, int r0, int rr, int n0, int q, float tau2,
-                                              DykstraThresholds thr, ST *__restrict__ Xout, int &qhead,
-                                              int &qcount)
+                                              DykstraThresholds thr, ST *__restrict__ Xout)
 {
     using S = TileShape<K, R, NT, VPT, ST>;
     using T = TiledSmem<K, R, NT, VPT, ST>;
@@ -473,30 +568,54 @@ __device__ __forceinline__ void stage_b_chunk(const TiledSmem<K, R, NT, VPT, ST>
         }
     }
 
-    // voxels that need the loop go to the ring queue; a full pass runs as soon
-    // as 32 are waiting
-    float *qq = sm.queue(threadIdx.x >> 5);
+    // voxels that need the loop go to the block's queue (the Dykstra warp runs
+    // them); when it is full, the lane runs the loop itself
 #pragma unroll
     for (int j = 0; j < VPT; ++j) {
         const bool mine = (need >> j) & 1u;
         const unsigned bal = __ballot_sync(0xffffffffu, mine);
         if (bal == 0u) continue;
-        if (mine) {
-            const int slot = (qhead + qcount + __popc(bal & ((1u << lane) - 1u))) & (S::QCAP - 1);
-            float *e = qq + slot * S::QSTRIDE;
-#pragma unroll
-            for (int i = 0; i < K; ++i) {
-                e[3 * i] = qv[j][i][0];
-                e[3 * i + 1] = qv[j][i][1];
-                e[3 * i + 2] = qv[j][i][2];
+        const uint32_t n = (uint32_t)__popc(bal);
+        uint32_t base = 0;
+        bool queued = false;
+        const int w = (threadIdx.x >> 5) % S::NW;
+        if (lane == 0) {
+            uint32_t *tail = sm.q_tail(w);
+            uint32_t t = *reinterpret_cast<volatile uint32_t *>(tail);
+            for (int tries = 0; tries < 64; ++tries) {
+                if (t + n - *sm.q_head(w) > (uint32_t)S::QN) break;  // no room
+                const uint32_t prev = atomicCAS(tail, t, t + n);
+                if (prev == t) {
+                    queued = true;
+                    base = t;
+                    break;
+                }
+                t = prev;
             }
-            e[3 * K] = __int_as_float((int)(o + j));
         }
-        qcount += __popc(bal);
-        if (qcount >= 32) {
-            drain_queue<K, R, NT, VPT, ST>(qq, qhead, 32, tp, thr, Xout);
-            qhead = (qhead + 32) & (S::QCAP - 1);
-            qcount -= 32;
+        queued = __shfl_sync(0xffffffffu, queued, 0);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (mine) {
+            if (queued) {
+                const uint32_t ticket = base + (uint32_t)__popc(bal & ((1u << lane) - 1u));
+                float *e = sm.queue_entry(w, ticket);
+#pragma unroll
+                for (int i = 0; i < K; ++i) {
+                    e[3 * i] = qv[j][i][0];
+                    e[3 * i + 1] = qv[j][i][1];
+                    e[3 * i + 2] = qv[j][i][2];
+                }
+                e[3 * K] = __int_as_float((int)(o + j));
+                __threadfence_block();
+                *sm.queue_seq(w, ticket) = ticket + 1u;
+            } else {
+                dual_project<K>(qv[j], thr);
+#pragma unroll
+                for (int i = 0; i < K - 1; ++i)
+#pragma unroll
+                    for (int a = 0; a < 3; ++a)
+                        Xout[(3 * i + a) * tp.plane_w + o + j] = Store<ST>::st(qv[j][i][a]);
+            }
         }
     }
     if (!live) return;
@@ -551,6 +670,11 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
             mbar_init(sm.empty(i), S::MAIN_WARPS + S::HALO_WARPS);
         }
         *abort = 0;
+        for (int w = 0; w < S::NW; ++w) {
+            *sm.q_tail(w) = 0u;
+            *sm.q_head(w) = 0u;
+            *sm.q_done(w) = 0u;
+        }
         mbar_fence_init();
     }
     for (int i = tid; i <= P + 1; i += blockDim.x) {
@@ -561,6 +685,7 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
         float *vb = sm.vb_plane(0);
         for (int i = tid; i < S::D * S::VB_SLOT / 4; i += blockDim.x) vb[i] = 0.0f;
     }
+    for (int i = tid; i < S::NW * S::QN; i += blockDim.x) *sm.queue_seq(i / S::QN, (uint32_t)i) = 0u;
     if (ca - 1 < tp.col_begin) {  // no plane before the first column: its Xi slot reads as zeros
         uint32_t *x0 = reinterpret_cast<uint32_t *>(sm.xi_slot(0));
         for (int i = tid; i < S::XI_SLOT / 4; i += blockDim.x) x0[i] = 0u;
@@ -607,6 +732,8 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
                 if (++slot == S::D) slot = 0, ph ^= 1u;
             }
         }
+    } else if (warp >= S::DYKSTRA_WARP) {
+        dykstra_worker<K, R, NT, VPT, ST>(sm, warp - S::DYKSTRA_WARP, tp, thr, Xout, abort);
     } else {
         const bool is_main = warp < S::MAIN_WARPS;
         const int hq = tid - S::MAIN;  // chunk of the halo row (halo warps)
@@ -615,7 +742,6 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
         const bool chunk_a = is_main || hq < S::Q;
         const bool nhalo = !is_main && hq <= R;  // lanes of the first halo warp
         bool ok = true;
-        int qhead = 0, qcount = 0;  // the warp's queue of voxels waiting for the Dykstra loop
         // ring slots of positions p-1, p, p+1 and the barrier parities of p-1, p
         int s_prev = S::D - 1, s_cur = 0, s_next = 1;
         uint32_t ph_prev = 1, ph_cur = 0;
@@ -636,8 +762,7 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
                     // dual step at position p-1 once every warp's Vbar of that plane is in
                     ok = mbar_wait_warp(sm.ready(s_prev), ph_prev, abort);
                     if (!ok) break;
-                    stage_b_chunk<K, R, NT, VPT, ST>(sm, tp, p - 1, s_prev, s_cur, r0, rr, n0, q, tau2, thr, Xout, qhead,
-                                                 qcount);
+                    stage_b_chunk<K, R, NT, VPT, ST>(sm, tp, p - 1, s_prev, s_cur, r0, rr, n0, q, tau2, thr, Xout);
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(sm.empty(s_prev));
@@ -652,9 +777,15 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
         if (ok && is_main && c_last == cb - 1) {
             ok = mbar_wait_warp(sm.ready(s_prev), ph_prev, abort);
             if (ok)
-                stage_b_chunk<K, R, NT, VPT, ST>(sm, tp, P, s_prev, s_cur, r0, rr, n0, q, tau2, thr, Xout, qhead, qcount);
+                stage_b_chunk<K, R, NT, VPT, ST>(sm, tp, P, s_prev, s_cur, r0, rr, n0, q, tau2, thr, Xout);
         }
-        if (ok && is_main && qcount > 0) drain_queue<K, R, NT, VPT, ST>(sm.queue(warp), qhead, qcount, tp, thr, Xout);
+        if (is_main) {  // this warp queues nothing more (also after an abort)
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence_block();
+                atomicAdd(sm.q_done(warp % S::NW), 1u);
+            }
+        }
     }
     __syncthreads();
     if (tid == 0 && *abort) atomicExch(err, 1);

@@ -108,6 +108,53 @@ __device__ __forceinline__ bool dual_first_sweep_is_identity(const float (&q)[K]
     return !any_long;
 }
 
+// One sweep of Dykstra's loop over the pairs (i1 < i2) with corrections P;
+// true when the loop exits after it (every step shorter than 1e-6).
+template <int K>
+__device__ __forceinline__ bool dykstra_sweep(float (&q)[K][3], float (&P)[K * (K - 1) / 2][3],
+                                              DykstraThresholds thr)
+{
+    float max_dd = 0.0f;
+    int p = 0;
+#pragma unroll
+    for (int i1 = 0; i1 < K - 1; ++i1) {
+#pragma unroll
+        for (int i2 = i1 + 1; i2 < K; ++i2, ++p) {
+            const float h0 = (q[i2][0] - q[i1][0]) + P[p][0];
+            const float h1 = (q[i2][1] - q[i1][1]) + P[p][1];
+            const float h2 = (q[i2][2] - q[i1][2]) + P[p][2];
+            float s = h0 * h0;
+            s = fmaf(h1, h1, s);
+            s = fmaf(h2, h2, s);
+            float n0 = 0.0f, n1 = 0.0f, n2 = 0.0f;
+            if (s > thr.len_gt_one) {
+                const float l = __fsqrt_rn(s);
+                const float lm1 = l - 1.0f;
+                n0 = __fdiv_rn(lm1 * h0, l);
+                n1 = __fdiv_rn(lm1 * h1, l);
+                n2 = __fdiv_rn(lm1 * h2, l);
+            }
+            const float d0 = 0.5f * (n0 - P[p][0]);
+            const float d1 = 0.5f * (n1 - P[p][1]);
+            const float d2 = 0.5f * (n2 - P[p][2]);
+            float dd = d0 * d0;
+            dd = fmaf(d1, d1, dd);
+            dd = fmaf(d2, d2, dd);
+            max_dd = fmax_ref(dd, max_dd);
+            q[i1][0] = q[i1][0] + d0;
+            q[i1][1] = q[i1][1] + d1;
+            q[i1][2] = q[i1][2] + d2;
+            q[i2][0] = q[i2][0] - d0;
+            q[i2][1] = q[i2][1] - d1;
+            q[i2][2] = q[i2][2] - d2;
+            P[p][0] = n0;
+            P[p][1] = n1;
+            P[p][2] = n2;
+        }
+    }
+    return max_dd < thr.exit_below;
+}
+
 template <int K>
 __device__ __forceinline__ int dual_project(float (&q)[K][3], DykstraThresholds thr)
 {
@@ -116,47 +163,8 @@ __device__ __forceinline__ int dual_project(float (&q)[K][3], DykstraThresholds 
 #pragma unroll
     for (int p = 0; p < kPairs; ++p) P[p][0] = P[p][1] = P[p][2] = 0.0f;
     int sweeps;
-    for (sweeps = 1; sweeps <= 20; ++sweeps) {
-        float max_dd = 0.0f;
-        int p = 0;
-#pragma unroll
-        for (int i1 = 0; i1 < K - 1; ++i1) {
-#pragma unroll
-            for (int i2 = i1 + 1; i2 < K; ++i2, ++p) {
-                const float h0 = (q[i2][0] - q[i1][0]) + P[p][0];
-                const float h1 = (q[i2][1] - q[i1][1]) + P[p][1];
-                const float h2 = (q[i2][2] - q[i1][2]) + P[p][2];
-                float s = h0 * h0;
-                s = fmaf(h1, h1, s);
-                s = fmaf(h2, h2, s);
-                float n0 = 0.0f, n1 = 0.0f, n2 = 0.0f;
-                if (s > thr.len_gt_one) {
-                    const float l = __fsqrt_rn(s);
-                    const float lm1 = l - 1.0f;
-                    n0 = __fdiv_rn(lm1 * h0, l);
-                    n1 = __fdiv_rn(lm1 * h1, l);
-                    n2 = __fdiv_rn(lm1 * h2, l);
-                }
-                const float d0 = 0.5f * (n0 - P[p][0]);
-                const float d1 = 0.5f * (n1 - P[p][1]);
-                const float d2 = 0.5f * (n2 - P[p][2]);
-                float dd = d0 * d0;
-                dd = fmaf(d1, d1, dd);
-                dd = fmaf(d2, d2, dd);
-                max_dd = fmax_ref(dd, max_dd);
-                q[i1][0] = q[i1][0] + d0;
-                q[i1][1] = q[i1][1] + d1;
-                q[i1][2] = q[i1][2] + d2;
-                q[i2][0] = q[i2][0] - d0;
-                q[i2][1] = q[i2][1] - d1;
-                q[i2][2] = q[i2][2] - d2;
-                P[p][0] = n0;
-                P[p][1] = n1;
-                P[p][2] = n2;
-            }
-        }
-        if (max_dd < thr.exit_below) break;
-    }
+    for (sweeps = 1; sweeps <= 20; ++sweeps)
+        if (dykstra_sweep<K>(q, P, thr)) break;
     return sweeps > 20 ? 20 : sweeps;
 }
 
