@@ -47,7 +47,7 @@ METRIC = "Potts PD Gvox-iter/s at k=3, %HBM peak; BF16-store vs FP32 at ≤1e-4 
 UNIT = "Gvox-iter/s"
 K_LABELS = 3
 LAMBDA = 30.0
-RADIUS = {"config1": 370.0, "config2": 370.0, "config0": 60.0, "mid": 180.0}
+RADIUS = {"config1": 370.0, "config2": 370.0, "config0": 60.0, "mid": 180.0, "mid4": 180.0}
 STORE_BYTES = {"f32": 4, "bf16": 2, "f16": 2}
 
 
@@ -64,7 +64,7 @@ def parse_args():
                    help="state storage of the timed solves")
     p.add_argument("--no-storage-compare", action="store_true",
                    help="skip the FP32-plain / BF16 / FP16 comparison solves")
-    p.add_argument("--workload", choices=["config1", "config2", "config0", "mid"], default="config1",
+    p.add_argument("--workload", choices=["config1", "config2", "config0", "mid", "mid4"], default="config1",
                    help="config1: 768x768x1024 r=370 (the benchmark); config0: 128^3 r=60; "
                         "mid: 384x384x256 r=180 (profiling size, state > L2)")
     p.add_argument("--no-e2e", action="store_true")
@@ -297,7 +297,8 @@ def run_ours(args, dist_: Dist) -> None:
     elif args.workload == "config0":
         ph = config0_phantom(seed=dist_.rank, device=dev)
     else:
-        ph = make_phantom(256, 384, 384, 180.0, seed=dist_.rank, radius_range=(6.0, 30.0), noise=7e-3, device=dev)
+        ph = make_phantom(256, 384, 384, 180.0, seed=dist_.rank, radius_range=(6.0, 30.0), noise=7e-3, device=dev,
+                          k=4 if args.workload == "mid4" else 3)
     m, u, ci = ph.mapping, ph.u, ph.ci
     k = len(ci)
     truth = ph.truth

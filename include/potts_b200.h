@@ -69,7 +69,7 @@ enum potts_variant {
  * even), also the Vbar the fused form keeps on chip, so that the fused and the
  * split forms give the same bits.  The reference stores FP32 only
  * (potts-min-partition.cpp:586-600); the 16-bit formats halve the bytes per
- * iteration.  Only the default tile shape of each K is compiled for them. */
+ * iteration.  Each format has its own list of compiled tile shapes. */
 enum potts_storage {
     POTTS_STORE_F32 = 0,  /* FP32, as the reference */
     POTTS_STORE_BF16 = 1, /* bfloat16 (8-bit mantissa) */

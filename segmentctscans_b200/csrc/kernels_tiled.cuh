@@ -57,10 +57,10 @@ namespace potts {
 
 // Per column: x = line of row start_row[col], y = first row, z = one past the
 // last row (y = z = 0 for an empty column).
-// Per work item: x = r0 (first row of the tile), y = n0, z = ca, w = cb.
+// Per volume (a work item is x = r0, the first row of the tile, y = n0,
+// z = ca, w = cb).
 struct TiledParams {
     const int4 *cols;
-    const int4 *work;
     int col_begin, col_end;
     int ns;         // slab extent along n
     int nstride_w;  // stride of the state arrays
@@ -212,6 +212,7 @@ struct TiledSmem {
     {
         return reinterpret_cast<volatile int *>(base + S::OFF_BAR + 3 * S::D * 8);
     }
+
     // element (comp, box row, box slice) of an Xi plane (slice 0 = n0 - XH), of
     // a stored V plane, and of a u / Vbar plane (slice 0 = n0 in both)
     __device__ __forceinline__ static int xi_at(int comp, int rr, int nn) { return (comp * (R + 2) + rr) * S::NX + nn; }
@@ -641,12 +642,28 @@ __device__ __forceinline__ void stage_b_chunk(const TiledSmem<K, R, NT, VPT, ST>
     }
 }
 
+// Everything a launch needs about one volume: tensor maps of both ping-pong
+// halves of Xi and V and of u, its tables, its state buffers, its phase
+// parameters and its convergence trace.  Lives in device memory (one entry
+// per volume of a batch); 64-byte aligned through CUtensorMap.
+template <int K, typename ST>
+struct FusedVolume {
+    CUtensorMap xi[2], v[2], u;
+    TiledParams tp;
+    ST *xi_buf[2], *v_buf[2];
+    PhaseParams<K> pp;
+    float *dq;  // per-iteration max |dV|^2 of this volume, or null
+};
+
+// One block per work item: a tile row range x slice range marching over up
+// to 64 columns of one volume (work_vol[item], or volume 0 when work_vol is
+// null); the items of every volume of a batch share one launch, and the
+// block scheduler hands them out as blocks finish.  The launch turns
+// (Xi^m, V^{m-1}) in half `in` into (Xi^{m+1}, V^m) in half in ^ 1; it = m - 1.
 template <int K, int R, int NT, int VPT, typename ST>
 __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
-    fused_tiled_kernel(const __grid_constant__ CUtensorMap tm_xi, const __grid_constant__ CUtensorMap tm_v,
-                       const __grid_constant__ CUtensorMap tm_u, TiledParams tp, ST *__restrict__ Xout,
-                       ST *__restrict__ Vout, PhaseParams<K> pp, float tau2, DykstraThresholds thr, float *dq,
-                       int *err)
+    fused_tiled_kernel(const FusedVolume<K, ST> *__restrict__ vols, const int4 *__restrict__ work,
+                       const int *__restrict__ work_vol, int in, int it, float tau2, DykstraThresholds thr, int *err)
 {
     using S = TileShape<K, R, NT, VPT, ST>;
     using T = TiledSmem<K, R, NT, VPT, ST>;
@@ -655,141 +672,164 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
     // align to 128 bytes by pointer arithmetic on the shared array itself, so
     // that the compiler keeps every access a shared-memory access
     sm.base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
-
-    const int4 wk = tp.work[blockIdx.x];
-    const int r0 = wk.x, n0 = wk.y, ca = wk.z, cb = wk.w;
-    const int c_last = cb < tp.col_end - 1 ? cb : tp.col_end - 1;
-    const int P = c_last - ca + 1;  // ring position of the last plane
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     volatile int *abort = sm.abort_flag();
-
-    if (tid == 0) {
-        for (int i = 0; i < S::D; ++i) {
-            mbar_init(sm.full(i), 1);
-            mbar_init(sm.ready(i), S::MAIN_WARPS + S::HALO_WARPS);
-            mbar_init(sm.empty(i), S::MAIN_WARPS + S::HALO_WARPS);
+    {
+        if (tid == 0) {
+            for (int i = 0; i < S::D; ++i) {
+                mbar_init(sm.full(i), 1);
+                mbar_init(sm.ready(i), S::MAIN_WARPS + S::HALO_WARPS);
+                mbar_init(sm.empty(i), S::MAIN_WARPS + S::HALO_WARPS);
+            }
+            *abort = 0;
+            for (int w = 0; w < S::NW; ++w) {
+                *sm.q_tail(w) = 0u;
+                *sm.q_head(w) = 0u;
+                *sm.q_done(w) = 0u;
+            }
+            mbar_fence_init();
         }
-        *abort = 0;
-        for (int w = 0; w < S::NW; ++w) {
-            *sm.q_tail(w) = 0u;
-            *sm.q_head(w) = 0u;
-            *sm.q_done(w) = 0u;
-        }
-        mbar_fence_init();
-    }
-    for (int i = tid; i <= P + 1; i += blockDim.x) {
-        const int c = ca - 1 + i;
-        sm.cols()[i] = (c >= tp.col_begin && c < tp.col_end) ? tp.cols[c] : make_int4(0, 0, 0, 0);
-    }
-    {  // Vbar planes start as zeros: a missing neighbour's value is multiplied by 0, so it must be finite
-        float *vb = sm.vb_plane(0);
-        for (int i = tid; i < S::D * S::VB_SLOT / 4; i += blockDim.x) vb[i] = 0.0f;
-    }
-    for (int i = tid; i < S::NW * S::QN; i += blockDim.x) *sm.queue_seq(i / S::QN, (uint32_t)i) = 0u;
-    if (ca - 1 < tp.col_begin) {  // no plane before the first column: its Xi slot reads as zeros
-        uint32_t *x0 = reinterpret_cast<uint32_t *>(sm.xi_slot(0));
-        for (int i = tid; i < S::XI_SLOT / 4; i += blockDim.x) x0[i] = 0u;
-    }
-    __syncthreads();
+        const int item = blockIdx.x;
+        const FusedVolume<K, ST> *vol = vols + (work_vol ? work_vol[item] : 0);
+        TiledParams tp = vol->tp;
+        tp.it = it;
+        const PhaseParams<K> pp = vol->pp;
+        ST *const Xout = vol->xi_buf[in ^ 1];
+        ST *const Vout = vol->v_buf[in ^ 1];
+        const CUtensorMap *tm_xi = &vol->xi[in], *tm_v = &vol->v[in], *tm_u = &vol->u;
 
-    float dqmax = 0.0f;
-    if (warp == S::PRODUCER_WARP) {
-        if (lane == 0) {
-            tma_prefetch_desc(&tm_xi);
-            tma_prefetch_desc(&tm_v);
-            tma_prefetch_desc(&tm_u);
-            // slot and phase parity of ring position p; waits for the release
-            // of the plane D positions back in the same slot
-            int slot = 0;
-            uint32_t ph = 0;
-            for (int p = 0; p <= P; ++p) {
-                if (p >= S::D && !mbar_wait_thread(sm.empty(slot), ph ^ 1u, abort)) break;
-                const int c = ca - 1 + p;
-                if (p == 0 && c < tp.col_begin) {  // no plane before the first column
-                    mbar_arrive(sm.full(0));
-                } else {
-                    const int4 ci = sm.cols()[p];
-                    const int line = ci.x + (r0 - 1 - ci.y);  // line of row r0-1 in column c
-                    const bool xi_only = p == 0;
-                    mbar_arrive_expect_tx(sm.full(slot),
-                                          S::XI_BYTES + (xi_only ? 0u : (uint32_t)(S::V_BYTES + S::U_BYTES)));
-                    tma_load_3d(sm.xi_slot(slot), &tm_xi, sm.full(slot), n0 - S::XH, line, 0);
-                    if (!xi_only) {
-                        tma_load_3d(sm.v_slot(slot), &tm_v, sm.full(slot), n0, line + 1, 0);
-                        tma_load_2d(sm.u_slot(slot), &tm_u, sm.full(slot), tp.u_x0 + n0, line + 1);
+        const int4 wk = work[item];
+        const int r0 = wk.x, n0 = wk.y, ca = wk.z, cb = wk.w;
+        const int c_last = cb < tp.col_end - 1 ? cb : tp.col_end - 1;
+        const int P = c_last - ca + 1;  // ring position of the last plane
+
+        for (int i = tid; i <= P + 1; i += blockDim.x) {
+            const int c = ca - 1 + i;
+            sm.cols()[i] = (c >= tp.col_begin && c < tp.col_end) ? tp.cols[c] : make_int4(0, 0, 0, 0);
+        }
+        {  // Vbar planes start as zeros: a missing neighbour's value is multiplied by 0, so it must be finite
+            float *vb = sm.vb_plane(0);
+            for (int i = tid; i < S::D * S::VB_SLOT / 4; i += blockDim.x) vb[i] = 0.0f;
+        }
+        for (int i = tid; i < S::NW * S::QN; i += blockDim.x) *sm.queue_seq(i / S::QN, (uint32_t)i) = 0u;
+        if (ca - 1 < tp.col_begin) {  // no plane before the first column: its Xi slot reads as zeros
+            uint32_t *x0 = reinterpret_cast<uint32_t *>(sm.xi_slot(0));
+            for (int i = tid; i < S::XI_SLOT / 4; i += blockDim.x) x0[i] = 0u;
+        }
+        __syncthreads();
+
+        float dqmax = 0.0f;
+        if (warp == S::PRODUCER_WARP) {
+            if (lane == 0) {
+                // the maps were written by copies before the launch
+                tma_fence_acquire_desc(tm_xi);
+                tma_fence_acquire_desc(tm_v);
+                tma_fence_acquire_desc(tm_u);
+                tma_prefetch_desc(tm_xi);
+                tma_prefetch_desc(tm_v);
+                tma_prefetch_desc(tm_u);
+                // slot and phase parity of ring position p; waits for the release
+                // of the plane D positions back in the same slot
+                int slot = 0;
+                uint32_t ph = 0;
+                int issued = 0;  // positions whose loads are in flight or done
+                for (int p = 0; p <= P; ++p) {
+                    if (p >= S::D && !mbar_wait_thread(sm.empty(slot), ph ^ 1u, abort)) break;
+                    const int c = ca - 1 + p;
+                    if (p == 0 && c < tp.col_begin) {  // no plane before the first column
+                        mbar_arrive(sm.full(0));
+                    } else {
+                        const int4 ci = sm.cols()[p];
+                        const int line = ci.x + (r0 - 1 - ci.y);  // line of row r0-1 in column c
+                        const bool xi_only = p == 0;
+                        mbar_arrive_expect_tx(sm.full(slot),
+                                              S::XI_BYTES + (xi_only ? 0u : (uint32_t)(S::V_BYTES + S::U_BYTES)));
+                        tma_load_3d(sm.xi_slot(slot), tm_xi, sm.full(slot), n0 - S::XH, line, 0);
+                        if (!xi_only) {
+                            tma_load_3d(sm.v_slot(slot), tm_v, sm.full(slot), n0, line + 1, 0);
+                            tma_load_2d(sm.u_slot(slot), tm_u, sm.full(slot), tp.u_x0 + n0, line + 1);
+                        }
                     }
+                    issued = p + 1;
+                    // L2 prefetch of the plane tp.prefetch positions ahead (the
+                    // ring's depth bounds what is in flight into shared memory)
+                    const int pf = p + tp.prefetch;
+                    if (tp.prefetch > 0 && pf <= P && ca - 1 + pf >= tp.col_begin) {
+                        const int4 cf = sm.cols()[pf];
+                        const int lf = cf.x + (r0 - 1 - cf.y);
+                        tma_prefetch_l2_3d(tm_xi, n0 - S::XH, lf, 0);
+                        tma_prefetch_l2_3d(tm_v, n0, lf + 1, 0);
+                        tma_prefetch_l2_2d(tm_u, tp.u_x0 + n0, lf + 1);
+                    }
+                    if (++slot == S::D) slot = 0, ph ^= 1u;
                 }
-                // L2 prefetch of the plane tp.prefetch positions ahead (the
-                // ring's depth bounds what is in flight into shared memory)
-                const int pf = p + tp.prefetch;
-                if (tp.prefetch > 0 && pf <= P && ca - 1 + pf >= tp.col_begin) {
-                    const int4 cf = sm.cols()[pf];
-                    const int lf = cf.x + (r0 - 1 - cf.y);
-                    tma_prefetch_l2_3d(&tm_xi, n0 - S::XH, lf, 0);
-                    tma_prefetch_l2_3d(&tm_v, n0, lf + 1, 0);
-                    tma_prefetch_l2_2d(&tm_u, tp.u_x0 + n0, lf + 1);
+                if (*abort) {
+                    // the consumers gave up: wait (bounded) for the loads still in
+                    // flight so that none lands after this block moves on
+                    for (int q = issued > S::D ? issued - S::D : 0; q < issued; ++q)
+                        mbar_wait_bounded(sm.full(q % S::D), (uint32_t)((q / S::D) & 1), kDrainTries);
                 }
-                if (++slot == S::D) slot = 0, ph ^= 1u;
             }
-        }
-    } else if (warp >= S::DYKSTRA_WARP) {
-        dykstra_worker<K, R, NT, VPT, ST>(sm, warp - S::DYKSTRA_WARP, tp, thr, Xout, abort);
-    } else {
-        const bool is_main = warp < S::MAIN_WARPS;
-        const int hq = tid - S::MAIN;  // chunk of the halo row (halo warps)
-        const int rr = is_main ? tid / S::Q : R;
-        const int q = is_main ? tid % S::Q : hq;
-        const bool chunk_a = is_main || hq < S::Q;
-        const bool nhalo = !is_main && hq <= R;  // lanes of the first halo warp
-        bool ok = true;
-        // ring slots of positions p-1, p, p+1 and the barrier parities of p-1, p
-        int s_prev = S::D - 1, s_cur = 0, s_next = 1;
-        uint32_t ph_prev = 1, ph_cur = 0;
-        for (int p = 0; p <= P && ok; ++p) {
-            if (p > 0) {
-                if (p == 1) ok = mbar_wait_warp(sm.full(0), 0, abort);
-                if (ok) ok = mbar_wait_warp(sm.full(s_cur), ph_cur, abort);
-                if (!ok) break;
-                if (chunk_a)
-                    stage_a_chunk<K, R, NT, VPT, ST>(sm, tp, pp, p, s_cur, s_prev, r0, rr, n0, q,
-                                                 is_main && ca - 1 + p < cb, Vout, dqmax);
-                if (nhalo) stage_a_nhalo<K, R, NT, VPT, ST>(sm, tp, pp, p, s_cur, s_prev, r0, hq, n0);
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(sm.ready(s_cur));
-            if (p > 0) {
-                if (is_main && p >= 2) {
-                    // dual step at position p-1 once every warp's Vbar of that plane is in
-                    ok = mbar_wait_warp(sm.ready(s_prev), ph_prev, abort);
+        } else if (warp >= S::DYKSTRA_WARP) {
+            dykstra_worker<K, R, NT, VPT, ST>(sm, warp - S::DYKSTRA_WARP, tp, thr, Xout, abort);
+        } else {
+            const bool is_main = warp < S::MAIN_WARPS;
+            const int hq = tid - S::MAIN;  // chunk of the halo row (halo warps)
+            const int rr = is_main ? tid / S::Q : R;
+            const int q = is_main ? tid % S::Q : hq;
+            const bool chunk_a = is_main || hq < S::Q;
+            const bool nhalo = !is_main && hq <= R;  // lanes of the first halo warp
+            bool ok = true;
+            // ring slots of positions p-1, p, p+1 and the barrier parities of p-1, p
+            int s_prev = S::D - 1, s_cur = 0, s_next = 1;
+            uint32_t ph_prev = 1, ph_cur = 0;
+            for (int p = 0; p <= P && ok; ++p) {
+                if (p > 0) {
+                    if (p == 1) ok = mbar_wait_warp(sm.full(0), 0, abort);
+                    if (ok) ok = mbar_wait_warp(sm.full(s_cur), ph_cur, abort);
                     if (!ok) break;
-                    stage_b_chunk<K, R, NT, VPT, ST>(sm, tp, p - 1, s_prev, s_cur, r0, rr, n0, q, tau2, thr, Xout);
+                    if (chunk_a)
+                        stage_a_chunk<K, R, NT, VPT, ST>(sm, tp, pp, p, s_cur, s_prev, r0, rr, n0, q,
+                                                         is_main && ca - 1 + p < cb, Vout, dqmax);
+                    if (nhalo) stage_a_nhalo<K, R, NT, VPT, ST>(sm, tp, pp, p, s_cur, s_prev, r0, hq, n0);
                 }
                 __syncwarp();
-                if (lane == 0) mbar_arrive(sm.empty(s_prev));
+                if (lane == 0) mbar_arrive(sm.ready(s_cur));
+                if (p > 0) {
+                    if (is_main && p >= 2) {
+                        // dual step at position p-1 once every warp's Vbar of that plane is in
+                        ok = mbar_wait_warp(sm.ready(s_prev), ph_prev, abort);
+                        if (!ok) break;
+                        stage_b_chunk<K, R, NT, VPT, ST>(sm, tp, p - 1, s_prev, s_cur, r0, rr, n0, q, tau2, thr,
+                                                         Xout);
+                    }
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(sm.empty(s_prev));
+                }
+                s_prev = s_cur;
+                ph_prev = ph_cur;
+                s_cur = s_next;
+                if (s_cur == 0) ph_cur ^= 1u;
+                s_next = (s_next + 1 == S::D) ? 0 : s_next + 1;
             }
-            s_prev = s_cur;
-            ph_prev = ph_cur;
-            s_cur = s_next;
-            if (s_cur == 0) ph_cur ^= 1u;
-            s_next = (s_next + 1 == S::D) ? 0 : s_next + 1;
-        }
-        // the last column of the volume has no plane after it (s_prev now holds position P)
-        if (ok && is_main && c_last == cb - 1) {
-            ok = mbar_wait_warp(sm.ready(s_prev), ph_prev, abort);
-            if (ok)
-                stage_b_chunk<K, R, NT, VPT, ST>(sm, tp, P, s_prev, s_cur, r0, rr, n0, q, tau2, thr, Xout);
-        }
-        if (is_main) {  // this warp queues nothing more (also after an abort)
-            __syncwarp();
-            if (lane == 0) {
-                __threadfence_block();
-                atomicAdd(sm.q_done(warp % S::NW), 1u);
+            // the last column of the volume has no plane after it (s_prev now holds position P)
+            if (ok && is_main && c_last == cb - 1) {
+                ok = mbar_wait_warp(sm.ready(s_prev), ph_prev, abort);
+                if (ok)
+                    stage_b_chunk<K, R, NT, VPT, ST>(sm, tp, P, s_prev, s_cur, r0, rr, n0, q, tau2, thr, Xout);
+            }
+            if (is_main) {  // this warp queues nothing more (also after an abort)
+                __syncwarp();
+                if (lane == 0) {
+                    __threadfence_block();
+                    atomicAdd(sm.q_done(warp % S::NW), 1u);
+                }
             }
         }
+        __syncthreads();
+        if (tid == 0 && *abort) atomicExch(err, 1);
+        if (vol->dq) block_max_to(dqmax, vol->dq + it);
     }
-    __syncthreads();
-    if (tid == 0 && *abort) atomicExch(err, 1);
-    if (dq) block_max_to(dqmax, dq);
 }
 
 // Copies the slab's part of u into a buffer with the state's stride, so that

@@ -196,7 +196,8 @@ struct potts_context {
     float *pinned_dq = nullptr;
     // tiled-kernel tables: per column (depends on the mapping) and the work
     // items of the last (slab extent, tile shape) planned
-    DevBuf cols, work;
+    DevBuf cols, work, vols;
+    int n_sm = 0;  // multiprocessors of the device
     bool cols_valid = false;
     int work_key[5] = {-1, -1, -1, -1, -1};
     int n_work = 0;
@@ -401,34 +402,39 @@ struct TileChoice {
     int rows, slices, vpt, segment;
 };
 
-// Tile shapes compiled per K (rows x slices x voxels per thread); the first
-// entry is the default.
-template <int K>
+// Tile shapes compiled per K and state width (rows x slices x voxels per
+// thread; W = 4 for FP32, 2 for the 16-bit formats); the first entry is the
+// default.
+template <int K, int W>
 struct TileShapes;
-template <> struct TileShapes<2> { static constexpr int n = 2; static constexpr int r[n] = {8, 8}, t[n] = {128, 64}, v[n] = {2, 4}; };
-template <> struct TileShapes<3> { static constexpr int n = 4; static constexpr int r[n] = {16, 8, 8, 8}, t[n] = {64, 128, 64, 128}, v[n] = {2, 2, 2, 4}; };
-template <> struct TileShapes<4> { static constexpr int n = 2; static constexpr int r[n] = {8, 4}, t[n] = {64, 128}, v[n] = {4, 4}; };
-template <> struct TileShapes<5> { static constexpr int n = 1; static constexpr int r[n] = {4}, t[n] = {64}, v[n] = {4}; };
-template <> struct TileShapes<6> { static constexpr int n = 1; static constexpr int r[n] = {4}, t[n] = {64}, v[n] = {4}; };
+template <int W> struct TileShapes<2, W> { static constexpr int n = 2; static constexpr int r[n] = {8, 8}, t[n] = {128, 64}, v[n] = {2, 4}; };
+template <> struct TileShapes<3, 4> { static constexpr int n = 4; static constexpr int r[n] = {16, 8, 8, 8}, t[n] = {64, 128, 64, 128}, v[n] = {2, 2, 2, 4}; };
+template <> struct TileShapes<3, 2> { static constexpr int n = 2; static constexpr int r[n] = {16, 8}, t[n] = {64, 128}, v[n] = {2, 2}; };
+template <> struct TileShapes<4, 4> { static constexpr int n = 3; static constexpr int r[n] = {8, 8, 4}, t[n] = {64, 64, 128}, v[n] = {2, 4, 4}; };
+template <> struct TileShapes<4, 2> { static constexpr int n = 1; static constexpr int r[n] = {8}, t[n] = {64}, v[n] = {2}; };
+template <int W> struct TileShapes<5, W> { static constexpr int n = 2; static constexpr int r[n] = {4, 8}, t[n] = {64, 64}, v[n] = {4, 2}; };
+template <> struct TileShapes<6, 4> { static constexpr int n = 1; static constexpr int r[n] = {4}, t[n] = {64}, v[n] = {4}; };
+template <> struct TileShapes<6, 2> { static constexpr int n = 2; static constexpr int r[n] = {4, 8}, t[n] = {64, 64}, v[n] = {4, 2}; };
 
-// n_compiled: how many of the shapes (from the first) are compiled for the
-// storage format.
-template <int K>
-int choose_tile(const potts_options &o, int n_compiled, TileChoice *tc)
+template <int K, typename ST>
+using ShapesOf = TileShapes<K, (int)sizeof(ST) == 4 ? 4 : 2>;
+
+template <int K, typename ST>
+int choose_tile(const potts_options &o, TileChoice *tc)
 {
-    tc->rows = TileShapes<K>::r[0];
-    tc->slices = TileShapes<K>::t[0];
-    tc->vpt = TileShapes<K>::v[0];
+    using TS = ShapesOf<K, ST>;
+    tc->rows = TS::r[0];
+    tc->slices = TS::t[0];
+    tc->vpt = TS::v[0];
     tc->segment = o.segment_cols > 0 ? o.segment_cols : 64;
     if (tc->segment > 64) return fail(POTTS_EINVAL, "segment_cols must be <= 64");
     if (o.tile_rows > 0 || o.tile_slices > 0 || o.tile_vpt > 0) {
-        for (int i = 0; i < n_compiled; ++i)
-            if ((o.tile_rows <= 0 || o.tile_rows == TileShapes<K>::r[i]) &&
-                (o.tile_slices <= 0 || o.tile_slices == TileShapes<K>::t[i]) &&
-                (o.tile_vpt <= 0 || o.tile_vpt == TileShapes<K>::v[i])) {
-                tc->rows = TileShapes<K>::r[i];
-                tc->slices = TileShapes<K>::t[i];
-                tc->vpt = TileShapes<K>::v[i];
+        for (int i = 0; i < TS::n; ++i)
+            if ((o.tile_rows <= 0 || o.tile_rows == TS::r[i]) && (o.tile_slices <= 0 || o.tile_slices == TS::t[i]) &&
+                (o.tile_vpt <= 0 || o.tile_vpt == TS::v[i])) {
+                tc->rows = TS::r[i];
+                tc->slices = TS::t[i];
+                tc->vpt = TS::v[i];
                 return POTTS_OK;
             }
         return fail(POTTS_EINVAL,
@@ -437,25 +443,25 @@ int choose_tile(const potts_options &o, int n_compiled, TileChoice *tc)
     return POTTS_OK;
 }
 
-// Per-column table and work items (x = first row, y = first slice, z/w = column range).
-int plan_tiles(potts_context *ctx, int ns, const TileChoice &tc)
+// Per-column table of the fused kernel: x = first line, y/z = row range.
+std::vector<int4> column_table(const potts_mapping &m)
 {
-    const MappingCopy &mc = ctx->mapping;
-    const potts_mapping &m = mc.m;
-    if (!ctx->cols_valid) {
-        std::vector<int4> cols(std::max<uint32_t>(m.cols, 1), make_int4(0, 0, 0, 0));
-        for (uint32_t c = 0; c < m.cols; ++c) {
-            const int64_t cnt = (int64_t)(m.base[c + 1] - m.base[c]) / m.nstride;
-            cols[c].x = (int)(m.base[c] / m.nstride);
-            cols[c].y = cnt > 0 ? (int)m.start_row[c] : 0;
-            cols[c].z = cnt > 0 ? (int)(m.start_row[c] + cnt) : 0;
-        }
-        POTTS_TRY(ensure(ctx, ctx->cols, sizeof(int4) * cols.size()));
-        POTTS_CUDA(cudaMemcpy(ctx->cols.p, cols.data(), sizeof(int4) * cols.size(), cudaMemcpyHostToDevice));
-        ctx->cols_valid = true;
+    std::vector<int4> cols(std::max<uint32_t>(m.cols, 1), make_int4(0, 0, 0, 0));
+    for (uint32_t c = 0; c < m.cols; ++c) {
+        const int64_t cnt = (int64_t)(m.base[c + 1] - m.base[c]) / m.nstride;
+        cols[c].x = (int)(m.base[c] / m.nstride);
+        cols[c].y = cnt > 0 ? (int)m.start_row[c] : 0;
+        cols[c].z = cnt > 0 ? (int)(m.start_row[c] + cnt) : 0;
     }
-    const int key[5] = {ns, tc.rows, tc.slices, tc.segment, (int)mc.n_lines};
-    if (std::equal(key, key + 5, ctx->work_key)) return POTTS_OK;
+    return cols;
+}
+
+// Work items of the fused kernel (x = first row, y = first slice, z/w =
+// column range), ordered so that items sharing columns run together (halo
+// rows of neighbouring tiles meet in L2), the slice tiles of the same rows side
+// by side.
+std::vector<int4> work_items(const potts_mapping &m, int ns, const TileChoice &tc)
+{
     int row_lo = INT32_MAX, row_hi = 0;
     for (uint32_t c = m.col_begin; c < m.col_end; ++c) {
         const int64_t cnt = (int64_t)(m.base[c + 1] - m.base[c]) / m.nstride;
@@ -484,32 +490,49 @@ int plan_tiles(potts_context *ctx, int ns, const TileChoice &tc)
             }
         }
     }
-    // items sharing columns run together (halo rows of neighbouring tiles meet
-    // in L2), the slice tiles of the same rows side by side
     std::sort(items.begin(), items.end(), [](const Item &a, const Item &b) {
         if (a.ca != b.ca) return a.ca < b.ca;
         if (a.r0 != b.r0) return a.r0 < b.r0;
         return a.n0 < b.n0;
     });
-    std::vector<int4> work(std::max<size_t>(items.size(), 1));
+    std::vector<int4> work(items.size());
     for (size_t i = 0; i < items.size(); ++i) work[i] = make_int4(items[i].r0, items[i].n0, items[i].ca, items[i].cb);
-    POTTS_TRY(ensure(ctx, ctx->work, sizeof(int4) * work.size()));
-    POTTS_CUDA(cudaMemcpy(ctx->work.p, work.data(), sizeof(int4) * work.size(), cudaMemcpyHostToDevice));
+    return work;
+}
+
+// Column table and work items of the context's mapping on the device.
+int plan_tiles(potts_context *ctx, int ns, const TileChoice &tc)
+{
+    const MappingCopy &mc = ctx->mapping;
+    if (!ctx->cols_valid) {
+        const std::vector<int4> cols = column_table(mc.m);
+        POTTS_TRY(ensure(ctx, ctx->cols, sizeof(int4) * cols.size()));
+        POTTS_CUDA(cudaMemcpy(ctx->cols.p, cols.data(), sizeof(int4) * cols.size(), cudaMemcpyHostToDevice));
+        ctx->cols_valid = true;
+    }
+    const int key[5] = {ns, tc.rows, tc.slices, tc.segment, (int)mc.n_lines};
+    if (std::equal(key, key + 5, ctx->work_key)) return POTTS_OK;
+    const std::vector<int4> work = work_items(mc.m, ns, tc);
+    POTTS_TRY(ensure(ctx, ctx->work, sizeof(int4) * std::max<size_t>(work.size(), 1)));
+    if (!work.empty())
+        POTTS_CUDA(cudaMemcpy(ctx->work.p, work.data(), sizeof(int4) * work.size(), cudaMemcpyHostToDevice));
     std::copy(key, key + 5, ctx->work_key);
-    ctx->n_work = (int)items.size();
+    ctx->n_work = (int)work.size();
     return POTTS_OK;
 }
 
+template <int K, typename ST>
 struct FusedPlan {
-    CUtensorMap xi[2], v[2], u;
-    potts::TiledParams tp;
+    potts::FusedVolume<K, ST> vol;  // host copy of the volume's descriptor
     int n_work = 0;
     TileChoice tile{};
 };
 
+// One launch of the fused kernel over n_work items (work / work_vol on the
+// device), volumes in `vols`.
 template <int K, int R, int NT, int VPT, typename ST>
-int launch_tiled_shape(potts_context *ctx, const FusedPlan &fp, int in, ST *Xout, ST *Vout,
-                       const PhaseParams<K> &pp, float tau2, float *dq)
+int launch_tiled_shape(potts_context *ctx, const potts::FusedVolume<K, ST> *vols, const int4 *work,
+                       const int *work_vol, int n_work, int in, int it, float tau2)
 {
     using S = potts::TileShape<K, R, NT, VPT, ST>;
     static bool attr_set = false;
@@ -518,45 +541,41 @@ int launch_tiled_shape(potts_context *ctx, const FusedPlan &fp, int in, ST *Xout
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM_ALLOC));
         attr_set = true;
     }
-    if (fp.n_work == 0) return POTTS_OK;
-    potts::fused_tiled_kernel<K, R, NT, VPT, ST><<<fp.n_work, S::THREADS, S::SMEM_ALLOC, ctx->stream>>>(
-        fp.xi[in], fp.v[in], fp.u, fp.tp, Xout, Vout, pp, tau2, ctx->thr, dq, (int *)ctx->err.p);
+    if (n_work == 0) return POTTS_OK;
+    potts::fused_tiled_kernel<K, R, NT, VPT, ST><<<n_work, S::THREADS, S::SMEM_ALLOC, ctx->stream>>>(
+        vols, work, work_vol, in, it, tau2, ctx->thr, (int *)ctx->err.p);
     POTTS_CUDA(cudaGetLastError());
     return POTTS_OK;
 }
 
-// FP32 storage compiles every tile shape of K; the 16-bit formats the default one.
-template <int K, typename ST>
-constexpr int compiled_shapes()
-{
-    return std::is_same<ST, float>::value ? TileShapes<K>::n : 1;
-}
-
 template <int K, typename ST, int I = 0>
-int launch_tiled(potts_context *ctx, const FusedPlan &fp, int in, ST *Xout, ST *Vout, const PhaseParams<K> &pp,
-                 float tau2, float *dq)
+int launch_tiled(potts_context *ctx, const TileChoice &tile, const potts::FusedVolume<K, ST> *vols,
+                 const int4 *work, const int *work_vol, int n_work, int in, int it, float tau2)
 {
-    if constexpr (I < compiled_shapes<K, ST>()) {
-        constexpr int R = TileShapes<K>::r[I], NT = TileShapes<K>::t[I], VPT = TileShapes<K>::v[I];
-        if (fp.tile.rows == R && fp.tile.slices == NT && fp.tile.vpt == VPT)
-            return launch_tiled_shape<K, R, NT, VPT, ST>(ctx, fp, in, Xout, Vout, pp, tau2, dq);
-        return launch_tiled<K, ST, I + 1>(ctx, fp, in, Xout, Vout, pp, tau2, dq);
+    using TS = ShapesOf<K, ST>;
+    if constexpr (I < TS::n) {
+        constexpr int R = TS::r[I], NT = TS::t[I], VPT = TS::v[I];
+        if (tile.rows == R && tile.slices == NT && tile.vpt == VPT)
+            return launch_tiled_shape<K, R, NT, VPT, ST>(ctx, vols, work, work_vol, n_work, in, it, tau2);
+        return launch_tiled<K, ST, I + 1>(ctx, tile, vols, work, work_vol, n_work, in, it, tau2);
     } else {
         return fail(POTTS_EINVAL, "no compiled tile shape matches");
     }
 }
 
+// Descriptor of one volume for the fused kernel: tensor maps of both halves
+// of the state and of u (read from ubase with row stride ustride, slice ux0 =
+// slice 0 of the volume), its column table and phase parameters.
 template <int K, typename ST>
-int prepare_fused(potts_context *ctx, const Geometry &g, const ST *const xi[2], const ST *const v[2],
-                  const float *d_u, const potts_options &o, FusedPlan *fp)
+int build_volume(const Geometry &g, const int4 *d_cols, int col_begin, int col_end, const ST *const xi[2],
+                 const ST *const v[2], const float *ubase, uint64_t ustride, int ux0, const TileChoice &tile,
+                 const PhaseParams<K> &pp, float *dq, int prefetch, potts::FusedVolume<K, ST> *vol)
 {
-    POTTS_TRY(choose_tile<K>(o, compiled_shapes<K, ST>(), &fp->tile));
     if (g.plane_w >= (int64_t(1) << 31))
         return fail(POTTS_EINVAL, "a state plane of 2^31 voxels or more needs slabs (set slab_w)");
-    const int R = fp->tile.rows, NT = fp->tile.slices;
-    POTTS_TRY(plan_tiles(ctx, g.ns, fp->tile));
-    fp->n_work = ctx->n_work;
-    const uint64_t L = (uint64_t)g.n_lines;
+    std::memset(vol, 0, sizeof(*vol));
+    const int R = tile.rows, NT = tile.slices;
+    const uint64_t L = (uint64_t)std::max<int64_t>(g.n_lines, 1);
     // boxes as in potts::TileShape: Xi slices n0-XH .. n0+NT+XH-1, V slices
     // n0 .. n0+NT+3 (FP32) or n0+NT+7 (16-bit), whole 16-byte rows
     constexpr uint64_t es = sizeof(ST);
@@ -565,43 +584,69 @@ int prepare_fused(potts_context *ctx, const Geometry &g, const ST *const xi[2], 
         const uint64_t dx[3] = {(uint64_t)g.nstride_w, L, (uint64_t)(3 * (K - 1))};
         const uint64_t sx[2] = {(uint64_t)g.nstride_w * es, (uint64_t)g.plane_w * es};
         const uint32_t bx[3] = {(uint32_t)(NT + 2 * XH), (uint32_t)(R + 2), (uint32_t)(3 * (K - 1))};
-        POTTS_TRY(encode_map(&fp->xi[b], StoreInfo<ST>::dt, xi[b], 3, dx, sx, bx));
+        POTTS_TRY(encode_map(&vol->xi[b], StoreInfo<ST>::dt, xi[b], 3, dx, sx, bx));
         const uint64_t dv[3] = {(uint64_t)g.nstride_w, L, (uint64_t)(K - 1)};
         const uint32_t bv[3] = {(uint32_t)(NT + (es == 4 ? 4 : 8)), (uint32_t)(R + 1), (uint32_t)(K - 1)};
-        POTTS_TRY(encode_map(&fp->v[b], StoreInfo<ST>::dt, v[b], 3, dv, sx, bv));
-    }
-    // u: read in place when the slab's slices start on a 16-byte boundary,
-    // else staged into a buffer with the state's stride
-    const float *ubase = d_u;
-    uint64_t ustride = (uint64_t)g.nstride_in;
-    int ux0 = g.slab_start;
-    if (g.slab_start % 4 != 0 || reinterpret_cast<uintptr_t>(d_u) % 16 != 0) {
-        POTTS_TRY(ensure(ctx, ctx->ustage, sizeof(float) * (size_t)g.plane_w));
-        const int chunks = (g.ns + potts::kPlainThreads - 1) / potts::kPlainThreads;
-        potts::stage_u_kernel<<<(unsigned)(g.n_lines * chunks), potts::kPlainThreads, 0, ctx->stream>>>(
-            g, d_u, (float *)ctx->ustage.p);
-        ctx->total_launches += 1;
-        POTTS_CUDA(cudaGetLastError());
-        ubase = (const float *)ctx->ustage.p;
-        ustride = (uint64_t)g.nstride_w;
-        ux0 = 0;
+        POTTS_TRY(encode_map(&vol->v[b], StoreInfo<ST>::dt, v[b], 3, dv, sx, bv));
+        vol->xi_buf[b] = const_cast<ST *>(xi[b]);
+        vol->v_buf[b] = const_cast<ST *>(v[b]);
     }
     const uint64_t du[2] = {ustride, L};
     const uint64_t su[1] = {ustride * 4};
     const uint32_t bu[2] = {(uint32_t)(NT + 4), (uint32_t)(R + 1)};
-    POTTS_TRY(encode_map(&fp->u, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, ubase, 2, du, su, bu));
-    fp->tp.cols = (const int4 *)ctx->cols.p;
-    fp->tp.work = (const int4 *)ctx->work.p;
-    fp->tp.col_begin = (int)ctx->mapping.m.col_begin;
-    fp->tp.col_end = (int)ctx->mapping.m.col_end;
-    fp->tp.ns = g.ns;
-    fp->tp.nstride_w = g.nstride_w;
-    fp->tp.plane_w = g.plane_w;
-    fp->tp.u_x0 = ux0;
-    fp->tp.n_base = g.slab_start;
-    fp->tp.it = 0;
-    fp->tp.prefetch = o.prefetch < 0 ? 0 : (o.prefetch == 0 ? kDefaultPrefetch : o.prefetch);
+    POTTS_TRY(encode_map(&vol->u, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, ubase, 2, du, su, bu));
+    vol->tp.cols = d_cols;
+    vol->tp.col_begin = col_begin;
+    vol->tp.col_end = col_end;
+    vol->tp.ns = g.ns;
+    vol->tp.nstride_w = g.nstride_w;
+    vol->tp.plane_w = g.plane_w;
+    vol->tp.u_x0 = ux0;
+    vol->tp.n_base = g.slab_start;
+    vol->tp.it = 0;
+    vol->tp.prefetch = prefetch < 0 ? 0 : (prefetch == 0 ? kDefaultPrefetch : prefetch);
+    vol->pp = pp;
+    vol->dq = dq;
     return POTTS_OK;
+}
+
+// u of a slab as the fused kernel reads it: in place when the slab's slices
+// start on a 16-byte boundary, else staged into `stage` with the state's stride.
+int fused_u_source(potts_context *ctx, const Geometry &g, const float *d_u, DevBuf &stage, const float **ubase,
+                   uint64_t *ustride, int *ux0)
+{
+    *ubase = d_u;
+    *ustride = (uint64_t)g.nstride_in;
+    *ux0 = g.slab_start;
+    if (g.slab_start % 4 != 0 || g.nstride_in % 4 != 0 || reinterpret_cast<uintptr_t>(d_u) % 16 != 0) {
+        POTTS_TRY(ensure(ctx, stage, sizeof(float) * (size_t)std::max<int64_t>(g.plane_w, 1)));
+        const int chunks = (g.ns + potts::kPlainThreads - 1) / potts::kPlainThreads;
+        if (g.n_lines > 0)
+            potts::stage_u_kernel<<<(unsigned)(g.n_lines * chunks), potts::kPlainThreads, 0, ctx->stream>>>(
+                g, d_u, (float *)stage.p);
+        ctx->total_launches += 1;
+        POTTS_CUDA(cudaGetLastError());
+        *ubase = (const float *)stage.p;
+        *ustride = (uint64_t)g.nstride_w;
+        *ux0 = 0;
+    }
+    return POTTS_OK;
+}
+
+template <int K, typename ST>
+int prepare_fused(potts_context *ctx, const Geometry &g, const ST *const xi[2], const ST *const v[2],
+                  const float *d_u, const potts_options &o, const PhaseParams<K> &pp, float *dq, FusedPlan<K, ST> *fp)
+{
+    POTTS_TRY((choose_tile<K, ST>(o, &fp->tile)));
+    POTTS_TRY(plan_tiles(ctx, g.ns, fp->tile));
+    fp->n_work = ctx->n_work;
+    const float *ubase;
+    uint64_t ustride;
+    int ux0;
+    POTTS_TRY(fused_u_source(ctx, g, d_u, ctx->ustage, &ubase, &ustride, &ux0));
+    return build_volume<K, ST>(g, (const int4 *)ctx->cols.p, (int)ctx->mapping.m.col_begin,
+                               (int)ctx->mapping.m.col_end, xi, v, ubase, ustride, ux0, fp->tile, pp, dq, o.prefetch,
+                               &fp->vol);
 }
 
 // One slab: init, iters iterations, argmax of [res_begin, res_end).
@@ -642,9 +687,13 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
         // the tiled kernel reads (and multiplies by zero) padding and stale
         // neighbours: keep all of the state finite
         POTTS_CUDA(cudaMemsetAsync(st.xi[0], 0, sizeof(ST) * 8 * (K - 1) * (size_t)g.plane_w, s));
-        FusedPlan fp;
+        FusedPlan<K, ST> fp;
         const ST *xs[2] = {st.xi[0], st.xi[1]}, *vs[2] = {st.v[0], st.v[1]};
-        if (iters > 1) POTTS_TRY((prepare_fused<K, ST>(ctx, g, xs, vs, d_u, o, &fp)));
+        if (iters > 1) {
+            POTTS_TRY((prepare_fused<K, ST>(ctx, g, xs, vs, d_u, o, pp, dq, &fp)));
+            POTTS_TRY(ensure(ctx, ctx->vols, sizeof(fp.vol)));
+            POTTS_CUDA(cudaMemcpyAsync(ctx->vols.p, &fp.vol, sizeof(fp.vol), cudaMemcpyHostToDevice, s));
+        }
         potts::init_kernel<K, ST><<<nb, potts::kPlainThreads, 0, s>>>(g, d_u, st.v[0], (ST *)nullptr, pp);
         ctx->total_launches += 1;
         POTTS_CUDA(cudaMemsetAsync(st.xi[0], 0, xi_bytes, s));
@@ -657,8 +706,8 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
             POTTS_TRY(seg_begin(ctx));
             ctx->loop_launches += 1;
             ctx->total_launches += 1;
-            fp.tp.it = m - 1;
-            POTTS_TRY((launch_tiled<K, ST>)(ctx, fp, cur, st.xi[nxt], st.v[nxt], pp, tau2, dq ? dq + (m - 1) : nullptr));
+            POTTS_TRY((launch_tiled<K, ST>)(ctx, fp.tile, (const potts::FusedVolume<K, ST> *)ctx->vols.p,
+                                            (const int4 *)ctx->work.p, nullptr, fp.n_work, cur, m - 1, tau2));
             if (ge > 0 && m % ge == 0) POTTS_TRY(run_energy<K>(ctx, g, st.xi[cur], st.v[nxt], d_u, pp, energy + 3 * (m / ge - 1)));
             if (o.sync_monitor && dq) POTTS_TRY(monitor_sync<K>(ctx, m - 1));
             cur = nxt;
@@ -859,6 +908,7 @@ int context_init(int device, void *stream, bool use_stream, potts_context **out)
     auto *ctx = new potts_context();
     ctx->device = device;
     ctx->thr = compute_thresholds();
+    if (cudaDeviceGetAttribute(&ctx->n_sm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) ctx->n_sm = 1;
     if (use_stream) {
         ctx->stream = (cudaStream_t)stream;  // NULL: the device's default stream
     } else {
@@ -927,7 +977,7 @@ void potts_context_destroy(potts_context *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (DevBuf *b : {&ctx->lines, &ctx->state, &ctx->dq, &ctx->energy, &ctx->partial, &ctx->host_u,
-                      &ctx->host_res, &ctx->host_labels, &ctx->ustage, &ctx->err, &ctx->cols, &ctx->work})
+                      &ctx->host_res, &ctx->host_labels, &ctx->ustage, &ctx->err, &ctx->cols, &ctx->work, &ctx->vols})
         if (b->p) cudaFree(b->p);
     if (ctx->pinned_dq) cudaFreeHost(ctx->pinned_dq);
     for (cudaEvent_t e : ctx->seg_ev) cudaEventDestroy(e);

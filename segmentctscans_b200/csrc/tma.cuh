@@ -81,6 +81,21 @@ __device__ __forceinline__ bool mbar_wait_warp(uint64_t *bar, uint32_t parity, v
     return __all_sync(0xffffffffu, done) != 0;
 }
 
+// Bounded wait without the abort flag (used after an abort, for loads in flight).
+constexpr int kDrainTries = 200;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int tries)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    for (int i = 0; i < tries; ++i)
+        if (mbar_try_wait_sleep(bar, parity, kWaitSleepNs)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void mbar_inval(uint64_t *bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 // Single-thread form (for the producer lane).
 __device__ __forceinline__ bool mbar_wait_thread(uint64_t *bar, uint32_t parity, volatile int *abort)
 {
@@ -122,6 +137,13 @@ __device__ __forceinline__ void tma_prefetch_l2_3d(const void *tmap, int x, int 
 {
     asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];"
                  ::"l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
+
+// Acquire a tensor map that generic-proxy writes (host copies) produced.
+__device__ __forceinline__ void tma_fence_acquire_desc(const void *tmap)
+{
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(tmap))
                  : "memory");
 }
 

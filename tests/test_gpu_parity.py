@@ -184,7 +184,7 @@ def test_errors_are_reported(cuda_device):
 
 
 TILE_SHAPES = {2: [(8, 128, 2), (8, 64, 4)], 3: [(8, 128, 2), (16, 64, 2), (8, 64, 2), (8, 128, 4)],
-               4: [(8, 64, 4), (4, 128, 4)], 5: [(4, 64, 4)], 6: [(4, 64, 4)]}
+               4: [(8, 64, 2), (8, 64, 4), (4, 128, 4)], 5: [(4, 64, 4), (8, 64, 2)], 6: [(4, 64, 4)]}
 
 
 @pytest.mark.parametrize("K", [2, 3, 4, 5, 6])

@@ -67,21 +67,27 @@ def test_store_energy_trace_matches_oracle(cuda_device, oracle_mod, store):
     np.testing.assert_allclose(g.stats.energy_trace[:, 2], o.energy_trace[:, 2], rtol=1e-6, atol=1e-9)
 
 
+STORE_TILE_SHAPES = {2: [(8, 128, 2), (8, 64, 4)], 3: [(16, 64, 2), (8, 128, 2)], 4: [(8, 64, 2)],
+                     5: [(4, 64, 4), (8, 64, 2)], 6: [(4, 64, 4), (8, 64, 2)]}
+
+
 @pytest.mark.parametrize("store", STORES)
-def test_store_every_segment_length_and_edges(cuda_device, oracle_mod, store):
-    """Partial n-tiles (n = 150), halos, 1/3/64-column segments, K = 2 .. 6 default tiles."""
+def test_store_every_tile_shape_and_segment_length(cuda_device, oracle_mod, store):
+    """Partial n-tiles (n = 150), halos, 1/3/64-column segments, K = 2 .. 6, every compiled tile."""
     for K in (2, 3, 4, 5, 6):
         m, u, ci = random_volume(150, 37, 35, 16.3, K, seed=20 + K)
         o = oracle_mod.solve(m, u, ci, 30.0, TAU, TAU, 9, precision="f32", store=store)
-        for seg in (1, 3, 64):
-            g = potts.solve(m, u, ci, 30.0, TAU, TAU, 9, variant=0, segment_cols=seg, storage=store)
-            assert_same(m, g, o)
+        for rows, slices, vpt in STORE_TILE_SHAPES[K]:
+            for seg in (1, 3, 64):
+                g = potts.solve(m, u, ci, 30.0, TAU, TAU, 9, variant=0, segment_cols=seg, storage=store,
+                                tile_rows=rows, tile_slices=slices, tile_vpt=vpt)
+                assert_same(m, g, o)
 
 
 def test_store_rejects_uncompiled_tile_shape(cuda_device):
     m, u, ci = random_volume(16, 10, 10, 4.4, 3, seed=31)
     with pytest.raises(PottsError) as e:
-        potts.solve(m, u, ci, 30.0, TAU, TAU, 5, variant=0, tile_rows=8, tile_slices=128, tile_vpt=2,
+        potts.solve(m, u, ci, 30.0, TAU, TAU, 5, variant=0, tile_rows=8, tile_slices=64, tile_vpt=2,
                     storage="bf16")
     assert e.value.status == 1
     with pytest.raises(PottsError) as e:
