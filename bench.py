@@ -20,7 +20,11 @@ same input, with their speed and their label flips and V error against the
 FP32 solve (bit-identical to the FP32 plain form).
 
 --workload config2 runs the same volume with K = 4 (a fourth phase at
-4.6e-2 on 15% of the pores).
+4.6e-2 on 15% of the pores).  --workload config3 is the batched sweep: 48
+sub-volumes with sides drawn from 64..256 per axis, each with its own lambda
+and noise, K = 3, 400 iterations, one potts_batch (captured graphs, one
+fused launch per iteration over all volumes, autotuned tile); under torchrun
+the volumes are bin-packed over the ranks (longest first).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Under torchrun each rank solves its own phantom (weak scaling, no data-path
@@ -64,7 +68,8 @@ def parse_args():
                    help="state storage of the timed solves")
     p.add_argument("--no-storage-compare", action="store_true",
                    help="skip the FP32-plain / BF16 / FP16 comparison solves")
-    p.add_argument("--workload", choices=["config1", "config2", "config0", "mid", "mid4"], default="config1",
+    p.add_argument("--workload", choices=["config1", "config2", "config3", "config0", "mid", "mid4"],
+                   default="config1",
                    help="config1: 768x768x1024 r=370 (the benchmark); config0: 128^3 r=60; "
                         "mid: 384x384x256 r=180 (profiling size, state > L2)")
     p.add_argument("--no-e2e", action="store_true")
@@ -490,11 +495,167 @@ def storage_compare(args, dist_: Dist, ctx, m, u, ci, tau, stream, dev, fused_va
     return out
 
 
+def cpu_baseline_batch(specs, budget_s: float) -> dict:
+    from oracle import oracle
+    from segmentctscans_b200.phantom import batch_phantom
+
+    spec = min(specs, key=lambda s: s.n * s.rows * s.cols)
+    ph = batch_phantom(spec, device="cpu")
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    u = ph.u.numpy().copy()
+    tau = tau_baseline()
+    t0 = time.perf_counter()
+    oracle.solve(ph.mapping, u, ph.ci, spec.lam, tau, tau, 1, precision="f64", want_state=False)
+    t1 = time.perf_counter() - t0
+    iters = max(1, min(400, int(budget_s / max(t1, 1e-3))))
+    t0 = time.perf_counter()
+    oracle.solve(ph.mapping, u, ph.ci, spec.lam, tau, tau, iters, precision="f64", want_state=False)
+    t = time.perf_counter() - t0
+    vox = ph.mapping.data_size
+    return {"value": vox * iters / t / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"FP64 oracle, OpenMP {threads} threads: the smallest sub-volume of the sweep "
+                      f"({spec.n}x{spec.rows}x{spec.cols}, {vox} in-mask voxels), {iters} iterations, {t:.1f} s"}
+
+
+def run_batch(args, dist_: Dist) -> None:
+    """The batched sweep (config 3) through potts_batch."""
+    import numpy as np
+    import torch
+
+    from segmentctscans_b200 import potts
+    from segmentctscans_b200.phantom import batch_phantom, config3_specs
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    dev = torch.device("cuda", dist_.local)
+    torch.cuda.set_device(dev)
+    dist_.init("nccl")
+    iters = 400 if args.iters == 1000 else args.iters
+    specs = config3_specs(48, seed=0)
+    # longest-processing-time bin packing of the volumes over the ranks
+    est = [s.n * s.rows * s.cols for s in specs]
+    loads = [0] * dist_.world
+    owner = {}
+    for i in sorted(range(len(specs)), key=lambda i: -est[i]):
+        r = min(range(dist_.world), key=lambda r: loads[r])
+        owner[i] = r
+        loads[r] += est[i]
+    mine = [i for i in range(len(specs)) if owner[i] == dist_.rank]
+    stream = torch.cuda.current_stream(dev)
+    ctx = potts.make_context(dev.index, stream=stream.cuda_stream)
+    tau = tau_baseline()
+    vols, keep = [], []
+    for i in mine:
+        ph = batch_phantom(specs[i], device=dev)
+        m = ph.mapping
+        res = torch.empty(m.span, dtype=torch.float32, device=dev)
+        lab = torch.empty(m.span, dtype=torch.uint8, device=dev)
+        keep.append((ph, res, lab))
+        vols.append(potts.BatchVolume(m, ph.u.data_ptr(), ph.ci, specs[i].lam, res.data_ptr(), lab.data_ptr()))
+    tile_opts = {"tile_rows": args.tile_rows, "tile_slices": args.tile_slices, "segment_cols": args.segment,
+                 "tile_vpt": args.tile_vpt, "prefetch": args.prefetch}
+    autotune = int(not any(v for v in tile_opts.values() if v > 0))
+    batch = potts.Batch(ctx, vols, tau, tau, iters, storage=args.storage, autotune=autotune, **tile_opts)
+    info = batch.info()
+    vox_local = info.voxels
+    for _ in range(args.warmup):
+        batch.run(stats=False)
+    torch.cuda.synchronize(dev)
+    dist_.barrier()
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    stats = [batch.run(stats=True) for _ in range(args.steps)]
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    dist_.barrier()
+    clk = clocks.stop()
+    t_max = dist_.reduce(e0.elapsed_time(e1) / 1000.0, "max")
+    vox_all = dist_.reduce(float(vox_local), "sum")
+    value = vox_all * iters * args.steps / t_max / 1e9
+
+    launch_s = sum(s.loop_ms for s in stats) / 1000.0 / max(sum(s.loop_launches for s in stats), 1)
+    bpv = bytes_per_voxel_iter("fused", 3, args.storage)
+    achieved = bpv * vox_local / launch_s / 1e9
+    peaks = measured_peaks()
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None,
+                "kernel": "potts::fused_tiled_kernel (all volumes per launch)", "bytes_per_voxel_iter": bpv,
+                "avg_launch_ms": round(launch_s * 1000, 4),
+                "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)"}
+
+    e2e = None
+    if not args.no_e2e:
+        hu = [torch.empty(ph.mapping.span, dtype=torch.float32, pin_memory=True) for ph, _, _ in keep]
+        for h, (ph, _, _) in zip(hu, keep):
+            h.copy_(ph.u.cpu())
+        hres = [torch.empty(ph.mapping.span, dtype=torch.float32, pin_memory=True) for ph, _, _ in keep]
+        hlab = [torch.empty(ph.mapping.span, dtype=torch.uint8, pin_memory=True) for ph, _, _ in keep]
+
+        def e2e_step():
+            for h, (ph, _, _) in zip(hu, keep):
+                ph.u.copy_(h, non_blocking=True)
+            batch.run(stats=False)
+            for hr, hl, (ph, res, lab) in zip(hres, hlab, keep):
+                hr.copy_(res, non_blocking=True)
+                hl.copy_(lab, non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize(dev)
+        dist_.barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = time.perf_counter()
+        f0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        f1.record(stream)
+        torch.cuda.synchronize(dev)
+        w1 = time.perf_counter()
+        te = dist_.reduce(max(f0.elapsed_time(f1) / 1000.0, w1 - w0), "max")
+        spans = sum(ph.mapping.span for ph, _, _ in keep)
+        same = all(bool(torch.equal(hl, lab.cpu())) for hl, (_, _, lab) in zip(hlab, keep))
+        e2e = {"value": vox_all * iters * args.steps / te / 1e9, "unit": UNIT, "h2d_bytes_per_step": 4 * spans,
+               "d2h_bytes_per_step": 5 * spans, "matches_device_run": same}
+
+    cpu = None
+    if dist_.rank == 0 and dist_.world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_batch(specs, args.cpu_seconds)
+    launches = sum(s.total_launches for s in stats)
+    if dist_.rank == 0:
+        lams = [s.lam for s in specs]
+        out = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist_.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1000 * t_max / args.steps, 2), "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32" if args.storage == "f32" else f"f32 math, {args.storage} state", "data": "synthetic",
+            "config": {"workload": "potts_k3_batch48_sides64-256", "volumes": len(specs),
+                       "volumes_this_rank": len(mine), "in_mask_voxels": int(vox_all), "k": 3,
+                       "lambda_range": [round(min(lams), 3), round(max(lams), 3)], "tau": tau, "iters": iters,
+                       "storage": args.storage, "tile": list(info.tile), "autotuned": bool(autotune),
+                       "autotune_ms": round(info.autotune_ms, 1), "work_items": info.n_work,
+                       "graph_launches": info.graph_launches,
+                       "parallelism": f"volumes bin-packed over {dist_.world} ranks" if dist_.world > 1 else "single",
+                       "l2": "inputs larger than L2 (state ~8 GB)"},
+            "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clk, "cpu_baseline": cpu,
+            "quality": {"final_sqrt_max_dV2": stats[-1].dq_last},
+        }
+        print(json.dumps(out), flush=True)
+    batch.close()
+    ctx.close()
+    dist_.close()
+
+
 def main():
     args = parse_args()
     d = Dist()
     if args.impl == "reference":
         run_reference(args, d)
+        return
+    if args.workload == "config3":
+        run_batch(args, d)
         return
     run_ours(args, d)
 

@@ -89,6 +89,8 @@ typedef struct potts_options {
     int tile_vpt;     /* fused form: consecutive slices per thread, 2 or 4 (0 = default for K) */
     int prefetch;     /* fused form: planes the load ring prefetches into L2 ahead of its loads
                          (0 = default, < 0 = none, at most 16) */
+    int autotune;     /* batches: 1 = time every compiled tile shape and segment length on the batch
+                         and keep the fastest (used when no tile option is set); 0 = default tile */
 } potts_options;
 
 typedef struct potts_stats {
@@ -192,6 +194,58 @@ int potts_solve_host(potts_context *ctx, const potts_mapping *map, const float *
 #define POTTS_STATIC_MAX_COLS 16384
 int potts_energies_static(const potts_mapping *map, const float *d_u, int K, const float *ci, float lambda,
                           const float *d_V, const float *d_Xi, void *stream, double *h_out);
+
+/* ---------------------------------------------------------------------------
+ * Batched solves.  No counterpart in the reference, whose caller solves one
+ * volume per process run (potts-model/potts-model.cpp:139-179); the batch runs
+ * a lambda / label sweep over many independent volumes of uneven size at once.
+ *
+ * potts_batch_create plans n volumes (each its own cylinder mapping, device u,
+ * K labels and lambda; K, tau1, tau2, iters and the storage format are common)
+ * and captures the whole schedule as three CUDA graphs on the context's
+ * stream: set-up (per volume the u staging, init and first dual step),
+ * iterations (iters - 1 launches, each ONE launch of the fused kernel over the
+ * work items of every volume) and finish (per volume the last primal step and
+ * the argmax).  Every potts_batch_run replays them back to back (events
+ * between them time the iterations): it reads each volume's u and writes its
+ * outputs again (u may change between runs; the pointers may not).  The fused
+ * form only (opts->variant is ignored), no slabs (the state of all volumes must
+ * fit in device memory, else POTTS_ENOMEM), gap_every is ignored.  Tile shape:
+ * the options', or with opts->autotune = 1 the fastest compiled shape and
+ * segment length measured on the batch (results do not depend on it).
+ * ------------------------------------------------------------------------- */
+typedef struct potts_batch potts_batch;
+
+typedef struct potts_batch_volume {
+    potts_mapping map; /* copied by potts_batch_create */
+    const float *d_u;  /* device, map's span; read by every run */
+    const float *ci;   /* [K] host labels, copied */
+    float lambda;
+    float *d_res;      /* optional device outputs in map's layout: ci[argmax] */
+    uint8_t *d_labels; /* optional: argmax index */
+    float *d_V;        /* optional: K-1 planes of map's span */
+} potts_batch_volume;
+
+typedef struct potts_batch_info {
+    int n_volumes;
+    int n_work;         /* work items of one iteration launch (all volumes) */
+    int tile_rows, tile_slices, tile_vpt, segment_cols; /* the tile shape in use */
+    uint64_t voxels;    /* in-mask voxels of all volumes */
+    uint64_t state_bytes;
+    int graph_launches; /* kernel launches in the captured graph */
+    double autotune_ms; /* device time spent autotuning (0 without) */
+} potts_batch_info;
+
+int potts_batch_create(potts_context *ctx, int n_volumes, const potts_batch_volume *volumes, int K, float tau1,
+                       float tau2, int iters, const potts_options *opts, potts_batch **out);
+/* Replays the graph on the context's stream.  With stats: waits, then reports
+ * solve_ms (the graph), loop_ms (its iteration launches), iters, the number of
+ * volumes in n_slabs, dq_last / dq_trace as the maximum over the volumes. */
+int potts_batch_run(potts_batch *batch, potts_stats *stats);
+int potts_batch_get_info(const potts_batch *batch, potts_batch_info *info);
+/* Per-volume trace of max |dV|^2 of the last run (needs track_dq): host [n_volumes * iters]. */
+int potts_batch_read_dq(potts_batch *batch, float *host);
+void potts_batch_destroy(potts_batch *batch);
 
 /* Mask constructor of layout_cylinder::mapping_storage (include/layout_cylinder.h:152-195):
  * fills start_row[cols] and base[cols+1], returns the span (base[cols]). */

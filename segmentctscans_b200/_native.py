@@ -30,7 +30,7 @@ class PottsOptions(ctypes.Structure):
         ("variant", ctypes.c_int), ("storage", ctypes.c_int), ("gap_every", ctypes.c_int),
         ("slab_w", ctypes.c_int), ("track_dq", ctypes.c_int), ("sync_monitor", ctypes.c_int),
         ("tile_rows", ctypes.c_int), ("tile_slices", ctypes.c_int), ("segment_cols", ctypes.c_int),
-        ("tile_vpt", ctypes.c_int), ("prefetch", ctypes.c_int),
+        ("tile_vpt", ctypes.c_int), ("prefetch", ctypes.c_int), ("autotune", ctypes.c_int),
     ]
 
 
@@ -40,6 +40,23 @@ class PottsStats(ctypes.Structure):
         ("dq_last", ctypes.c_float), ("solve_ms", ctypes.c_double), ("loop_ms", ctypes.c_double),
         ("loop_launches", ctypes.c_int), ("total_launches", ctypes.c_int), ("state_bytes", ctypes.c_uint64),
         ("dq_trace", ctypes.POINTER(ctypes.c_float)), ("energy_trace", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+class PottsBatchVolume(ctypes.Structure):
+    _fields_ = [
+        ("map", PottsMapping), ("d_u", ctypes.c_void_p), ("ci", ctypes.POINTER(ctypes.c_float)),
+        ("lambda_", ctypes.c_float), ("d_res", ctypes.c_void_p), ("d_labels", ctypes.c_void_p),
+        ("d_V", ctypes.c_void_p),
+    ]
+
+
+class PottsBatchInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_volumes", ctypes.c_int), ("n_work", ctypes.c_int), ("tile_rows", ctypes.c_int),
+        ("tile_slices", ctypes.c_int), ("tile_vpt", ctypes.c_int), ("segment_cols", ctypes.c_int),
+        ("voxels", ctypes.c_uint64), ("state_bytes", ctypes.c_uint64), ("graph_launches", ctypes.c_int),
+        ("autotune_ms", ctypes.c_double),
     ]
 
 
@@ -77,6 +94,11 @@ SIGNATURES = {
                                       ctypes.POINTER(_U32)]),
     "potts_get_stride": (_U32, [_U32]),
     "potts_energies_static": (_I, [_MP, _P, _I, _FP, _F, _P, _P, _P, ctypes.POINTER(ctypes.c_double)]),
+    "potts_batch_create": (_I, [_P, _I, ctypes.POINTER(PottsBatchVolume), _I, _F, _F, _I, _OP, ctypes.POINTER(_P)]),
+    "potts_batch_run": (_I, [_P, _SP]),
+    "potts_batch_get_info": (_I, [_P, ctypes.POINTER(PottsBatchInfo)]),
+    "potts_batch_read_dq": (_I, [_P, _FP]),
+    "potts_batch_destroy": (None, [_P]),
 }
 STATIC_MAX_COLS = 16384
 

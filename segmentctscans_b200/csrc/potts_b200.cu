@@ -927,6 +927,8 @@ int context_init(int device, void *stream, bool use_stream, potts_context **out)
     return POTTS_OK;
 }
 
+#include "batch.cuh"
+
 }  // namespace
 
 __attribute__((visibility("hidden"))) void potts_set_last_error(const std::string &msg) { g_last_error = msg; }
@@ -947,6 +949,7 @@ void potts_default_options(potts_options *o)
     o->segment_cols = 0;
     o->tile_vpt = 0;
     o->prefetch = 0;
+    o->autotune = 0;
 }
 
 const char *potts_status_string(int s)
@@ -1156,5 +1159,127 @@ uint64_t potts_cylinder_mapping(uint32_t rows, uint32_t cols, double xc, double 
 }
 
 uint32_t potts_get_stride(uint32_t n) { return get_stride(n); }
+
+int potts_batch_create(potts_context *ctx, int n_volumes, const potts_batch_volume *volumes, int K, float tau1,
+                       float tau2, int iters, const potts_options *opts, potts_batch **out)
+{
+    if (!out) return fail(POTTS_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (!ctx) return fail(POTTS_EINVAL, "context is NULL");
+    if (n_volumes <= 0 || !volumes) return fail(POTTS_EINVAL, "a batch needs at least one volume");
+    potts_options o;
+    potts_default_options(&o);
+    if (opts) o = *opts;
+    o.variant = POTTS_VARIANT_FUSED;
+    o.gap_every = 0;
+    o.slab_w = 0;
+    for (int i = 0; i < n_volumes; ++i) {
+        POTTS_TRY(check_params(K, volumes[i].ci, volumes[i].lambda, tau1, tau2, iters, o));
+        if (!volumes[i].d_u) return fail(POTTS_EINVAL, "a volume's u is NULL");
+    }
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    auto *b = new potts_batch();
+    b->ctx = ctx;
+    b->K = K;
+    b->storage = o.storage;
+    b->iters = iters;
+    b->tau1 = tau1;
+    b->tau2 = tau2;
+    b->opts = o;
+    b->vols.resize((size_t)n_volumes);
+    int rc = POTTS_OK;
+    for (int i = 0; i < n_volumes && rc == POTTS_OK; ++i) {
+        BatchVolume &bv = b->vols[(size_t)i];
+        rc = copy_mapping(&volumes[i].map, bv.mc);
+        bv.d_u = volumes[i].d_u;
+        bv.res = volumes[i].d_res;
+        bv.labels = volumes[i].d_labels;
+        bv.V = volumes[i].d_V;
+        for (int k = 0; k < K; ++k) bv.c[k] = volumes[i].ci[k];
+        bv.lambda = volumes[i].lambda;
+    }
+    if (rc == POTTS_OK) {
+        if (o.storage == POTTS_STORE_BF16)
+            rc = batch_build_store<__nv_bfloat16>(b);
+        else if (o.storage == POTTS_STORE_F16)
+            rc = batch_build_store<__half>(b);
+        else
+            rc = batch_build_store<float>(b);
+    }
+    if (rc != POTTS_OK) {
+        const std::string msg = g_last_error;
+        batch_free(b);
+        g_last_error = msg;
+        return rc;
+    }
+    *out = b;
+    return POTTS_OK;
+}
+
+int potts_batch_run(potts_batch *b, potts_stats *stats)
+{
+    if (!b || !b->exec[0]) return fail(POTTS_EINVAL, "batch is NULL");
+    potts_context *ctx = b->ctx;
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    POTTS_CUDA(cudaEventRecord(b->ev[0], ctx->stream));
+    POTTS_CUDA(cudaGraphLaunch(b->exec[0], ctx->stream));
+    POTTS_CUDA(cudaEventRecord(b->ev[2], ctx->stream));
+    POTTS_CUDA(cudaGraphLaunch(b->exec[1], ctx->stream));
+    POTTS_CUDA(cudaEventRecord(b->ev[3], ctx->stream));
+    POTTS_CUDA(cudaGraphLaunch(b->exec[2], ctx->stream));
+    POTTS_CUDA(cudaEventRecord(b->ev[1], ctx->stream));
+    if (!stats) return POTTS_OK;
+    POTTS_TRY(check_device_error(ctx));
+    float ms = 0.0f, lms = 0.0f;
+    POTTS_CUDA(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]));
+    POTTS_CUDA(cudaEventElapsedTime(&lms, b->ev[2], b->ev[3]));
+    stats->n_slabs = (int)b->vols.size();
+    stats->slab_w = 0;
+    stats->iters = b->iters;
+    stats->solve_ms = ms;
+    stats->loop_ms = lms;
+    stats->loop_launches = b->iters > 1 ? b->iters - 1 : 0;
+    stats->total_launches = b->graph_launches;
+    stats->state_bytes = b->state_bytes;
+    stats->dq_last = 0.0f;
+    if (b->dq.p && b->iters > 0) {
+        std::vector<float> all((size_t)b->iters * b->vols.size());
+        POTTS_CUDA(cudaMemcpy(all.data(), b->dq.p, sizeof(float) * all.size(), cudaMemcpyDeviceToHost));
+        std::vector<float> mx((size_t)b->iters, 0.0f);
+        for (size_t v = 0; v < b->vols.size(); ++v)
+            for (int i = 0; i < b->iters; ++i) mx[(size_t)i] = std::max(mx[(size_t)i], all[v * b->iters + i]);
+        stats->dq_last = std::sqrt(mx.back());
+        if (stats->dq_trace) std::memcpy(stats->dq_trace, mx.data(), sizeof(float) * mx.size());
+    }
+    return POTTS_OK;
+}
+
+int potts_batch_get_info(const potts_batch *b, potts_batch_info *info)
+{
+    if (!b || !info) return fail(POTTS_EINVAL, "batch or info is NULL");
+    info->n_volumes = (int)b->vols.size();
+    info->n_work = b->n_work;
+    info->tile_rows = b->tile.rows;
+    info->tile_slices = b->tile.slices;
+    info->tile_vpt = b->tile.vpt;
+    info->segment_cols = b->tile.segment;
+    info->voxels = b->voxels;
+    info->state_bytes = b->state_bytes;
+    info->graph_launches = b->graph_launches;
+    info->autotune_ms = b->autotune_ms;
+    return POTTS_OK;
+}
+
+int potts_batch_read_dq(potts_batch *b, float *host)
+{
+    if (!b || !host) return fail(POTTS_EINVAL, "batch or host is NULL");
+    if (!b->dq.p) return fail(POTTS_EINVAL, "the batch was created without track_dq");
+    POTTS_CUDA(cudaSetDevice(b->ctx->device));
+    POTTS_CUDA(cudaStreamSynchronize(b->ctx->stream));
+    POTTS_CUDA(cudaMemcpy(host, b->dq.p, sizeof(float) * (size_t)b->iters * b->vols.size(), cudaMemcpyDeviceToHost));
+    return POTTS_OK;
+}
+
+void potts_batch_destroy(potts_batch *b) { batch_free(b); }
 
 }  // extern "C"

@@ -165,3 +165,38 @@ def config2_phantom(seed: int = 0, device="cuda") -> Phantom:
     """Config-1 geometry with k = 4 (extra phase at 4.6e-2 on 15% of the pores)."""
     return make_phantom(1024, 768, 768, 370.0, seed=seed, radius_range=(6.0, 30.0), noise=7e-3, k=4,
                         device=device)
+
+
+@dataclass
+class BatchSpec:
+    """One sub-volume of the batched sweep: geometry, seed and its own lambda and noise."""
+    n: int
+    rows: int
+    cols: int
+    radius: float
+    sphere_radii: tuple
+    lam: float
+    noise: float
+    seed: int
+
+
+def config3_specs(count: int = 48, seed: int = 0) -> list[BatchSpec]:
+    """The batched sweep: sides drawn uniformly from 64..256 per axis, the 128^3 recipe scaled to
+    each size (cylinder radius 0.47 min(rows, cols), sphere radii U[4, 12] * side / 128 with
+    side the mean of rows and cols), lambda log-uniform in [10, 100], noise U[4e-3, 1.2e-2]."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for i in range(count):
+        n, rows, cols = (int(x) for x in rng.integers(64, 257, size=3))
+        side = 0.5 * (rows + cols)
+        scale = side / 128.0
+        lam = float(np.exp(rng.uniform(np.log(10.0), np.log(100.0))))
+        noise = float(rng.uniform(4e-3, 1.2e-2))
+        out.append(BatchSpec(n, rows, cols, 0.47 * min(rows, cols), (4.0 * scale, 12.0 * scale), lam, noise,
+                             seed * 1000 + i))
+    return out
+
+
+def batch_phantom(spec: BatchSpec, device="cuda") -> Phantom:
+    return make_phantom(spec.n, spec.rows, spec.cols, spec.radius, seed=spec.seed, radius_range=spec.sphere_radii,
+                        noise=spec.noise, device=device)

@@ -268,3 +268,96 @@ def solve(mapping: CylinderMapping, u: np.ndarray, ci: Sequence[float], lam: flo
     finally:
         if own:
             ctx.close()
+
+
+# --------------------------------------------------------------------------- batches
+@dataclass
+class BatchVolume:
+    """One volume of a batch: its mapping, device u and outputs (raw device addresses, 0 = none)."""
+    mapping: CylinderMapping
+    u_ptr: int
+    ci: Sequence[float]
+    lam: float
+    res_ptr: int = 0
+    labels_ptr: int = 0
+    V_ptr: int = 0
+
+
+@dataclass
+class BatchInfo:
+    n_volumes: int
+    n_work: int
+    tile: tuple
+    voxels: int
+    state_bytes: int
+    graph_launches: int
+    autotune_ms: float
+
+
+class Batch:
+    """A planned batch of independent volumes run as one captured CUDA graph (potts_batch_create).
+    The device buffers named by the volumes must outlive the batch."""
+
+    def __init__(self, ctx: CudaContext, volumes: Sequence[BatchVolume], tau1: float, tau2: float, iters: int,
+                 **options):
+        if not volumes:
+            raise ValueError("a batch needs at least one volume")
+        K = len(volumes[0].ci)
+        self.ctx = ctx
+        self.iters = int(iters)
+        self._keep = []
+        arr = (_native.PottsBatchVolume * len(volumes))()
+        for i, v in enumerate(volumes):
+            c = _ci_array(v.ci)
+            if c.size != K:
+                raise ValueError("every volume of a batch needs the same number of labels")
+            self._keep.append((v.mapping, c))
+            arr[i].map = v.mapping.as_c()
+            arr[i].d_u = ctypes.c_void_p(int(v.u_ptr))
+            arr[i].ci = c.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+            arr[i].lambda_ = float(v.lam)
+            arr[i].d_res = ctypes.c_void_p(int(v.res_ptr))
+            arr[i].d_labels = ctypes.c_void_p(int(v.labels_ptr))
+            arr[i].d_V = ctypes.c_void_p(int(v.V_ptr))
+        opts = _native.default_options(**options)
+        self.track_dq = bool(opts.track_dq)
+        h = ctypes.c_void_p()
+        check(_native.host_lib().potts_batch_create(ctx.handle, len(volumes), arr, K, float(tau1), float(tau2),
+                                                    int(iters), ctypes.byref(opts), ctypes.byref(h)))
+        self._h = h
+        self.n_volumes = len(volumes)
+
+    def run(self, stats: bool = True) -> Optional[SolveStats]:
+        """Replay the graph; with stats, wait and report (dq_trace: max over the volumes)."""
+        st, dq, en = _make_stats(self.iters, 0, stats)
+        check(_native.host_lib().potts_batch_run(self._h, ctypes.byref(st) if stats else None))
+        return _stats_out(st, dq, en) if stats else None
+
+    def info(self) -> BatchInfo:
+        i = _native.PottsBatchInfo()
+        check(_native.host_lib().potts_batch_get_info(self._h, ctypes.byref(i)))
+        return BatchInfo(i.n_volumes, i.n_work, (i.tile_rows, i.tile_slices, i.tile_vpt, i.segment_cols),
+                         int(i.voxels), int(i.state_bytes), i.graph_launches, float(i.autotune_ms))
+
+    def dq(self) -> np.ndarray:
+        """[n_volumes, iters] max |dV|^2 of every volume and iteration of the last run."""
+        out = np.zeros((self.n_volumes, self.iters), np.float32)
+        check(_native.host_lib().potts_batch_read_dq(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _native.host_lib().potts_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
