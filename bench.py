@@ -24,7 +24,12 @@ FP32 solve (bit-identical to the FP32 plain form).
 sub-volumes with sides drawn from 64..256 per axis, each with its own lambda
 and noise, K = 3, 400 iterations, one potts_batch (captured graphs, one
 fused launch per iteration over all volumes, autotuned tile); under torchrun
-the volumes are bin-packed over the ranks (longest first).
+the volumes are bin-packed over the ranks (longest first).  --workload config4
+is the differentiable solve: 192^3, r = 90, K = 3, 200 unrolled iterations,
+checkpoints every 20, cross-entropy of V against the true labels; value =
+voxel-iterations of forward + backward per second; the gradients of c, lambda
+and --fd-coords random u coordinates are checked against FP64 central
+differences of the oracle (step 1e-6 relative; also 1e-4 for u).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Under torchrun each rank solves its own phantom (weak scaling, no data-path
@@ -68,10 +73,12 @@ def parse_args():
                    help="state storage of the timed solves")
     p.add_argument("--no-storage-compare", action="store_true",
                    help="skip the FP32-plain / BF16 / FP16 comparison solves")
-    p.add_argument("--workload", choices=["config1", "config2", "config3", "config0", "mid", "mid4"],
+    p.add_argument("--workload", choices=["config1", "config2", "config3", "config4", "config0", "mid", "mid4"],
                    default="config1",
                    help="config1: 768x768x1024 r=370 (the benchmark); config0: 128^3 r=60; "
                         "mid: 384x384x256 r=180 (profiling size, state > L2)")
+    p.add_argument("--fd-coords", type=int, default=4,
+                   help="config4: random u coordinates checked against FP64 central differences")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
@@ -648,6 +655,116 @@ def run_batch(args, dist_: Dist) -> None:
     dist_.close()
 
 
+def run_adjoint(args, dist_: Dist) -> None:
+    """The differentiable solve (config 4) through potts_forward_ckpt / potts_backward."""
+    import numpy as np
+    import torch
+
+    from segmentctscans_b200 import potts
+    from segmentctscans_b200.phantom import make_phantom
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    dev = torch.device("cuda", dist_.local)
+    torch.cuda.set_device(dev)
+    dist_.init("nccl")
+    iters = 200 if args.iters == 1000 else args.iters
+    every, eps, lam = 20, 1e-3, LAMBDA
+    tau = tau_baseline()
+    ph = make_phantom(192, 192, 192, 90.0, seed=dist_.rank, radius_range=(4.0, 12.0), noise=7e-3, device=dev)
+    m, u, ci = ph.mapping, ph.u, ph.ci
+    truth = ph.truth
+    stream = torch.cuda.current_stream(dev)
+    ctx = potts.make_context(dev.index, stream=stream.cuda_stream)
+    gu = torch.zeros(m.span, dtype=torch.float32, device=dev)
+
+    def step():
+        with potts.Tape(ctx, m, u.data_ptr(), truth.data_ptr(), ci, lam, tau, tau, iters, every, eps) as t:
+            gc, gl = t.backward(gu.data_ptr())
+            return t.loss, gc, gl
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    dist_.barrier()
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        loss, gc, gl = step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    dist_.barrier()
+    clk = clocks.stop()
+    t_max = dist_.reduce(e0.elapsed_time(e1) / 1000.0, "max")
+    vox = m.data_size
+    value = dist_.reduce(float(vox) * iters * args.steps, "sum") / t_max / 1e9
+
+    check = None
+    if dist_.rank == 0 and args.fd_coords >= 0:
+        from oracle import oracle
+
+        oracle.set_threads(os.cpu_count() or 1)
+        u_h = u.cpu().numpy().copy()
+        t_h = truth.cpu().numpy()
+        mv = m.mask_values
+
+        def loss64(uu, cc, ll):
+            r = oracle.solve(m, uu, cc, ll, tau, tau, iters, precision="f64")
+            Vm = mv(r.V)
+            Vf = np.concatenate([Vm, 1.0 - Vm.sum(0, keepdims=True)])
+            tt = np.minimum(mv(t_h).astype(np.int64), len(ci) - 1)
+            return float(-np.mean(np.log(np.take_along_axis(Vf, tt[None], 0)[0] + eps)))
+
+        def cd(fun, x, rel):
+            h = rel * max(abs(x), 1e-2)
+            xp, xm = np.float32(x + h), np.float32(x - h)
+            return (fun(float(xp)) - fun(float(xm))) / (float(xp) - float(xm))
+
+        t0 = time.perf_counter()
+        rows = []
+        for i in range(len(ci)):
+            def fc(v, i=i):
+                c2 = list(ci)
+                c2[i] = v
+                return loss64(u_h, c2, lam)
+            g = cd(fc, ci[i], 1e-6)
+            rows.append({"param": f"c{i + 1}", "adjoint": float(gc[i]), "fd": g, "rel": abs(gc[i] - g) / abs(g)})
+        g = cd(lambda v: loss64(u_h, ci, v), lam, 1e-6)
+        rows.append({"param": "lambda", "adjoint": gl, "fd": g, "rel": abs(gl - g) / abs(g)})
+        gu_h = gu.cpu().numpy()
+        rng = np.random.default_rng(0)
+        idx = np.arange(m.span).reshape(m.n_lines, m.nstride)[:, : m.n_images].reshape(-1)
+        for j in rng.choice(idx, args.fd_coords, replace=False):
+            def fu(v, j=j):
+                u2 = u_h.copy()
+                u2[j] = v
+                return loss64(u2, ci, lam)
+            for rel in (1e-6, 1e-4):
+                g = cd(fu, float(u_h[j]), rel)
+                rows.append({"param": f"u[{int(j)}]", "step": rel, "adjoint": float(gu_h[j]), "fd": g,
+                             "rel": abs(gu_h[j] - g) / abs(g) if g != 0 else abs(gu_h[j])})
+        check = {"loss_fp64": loss64(u_h, ci, lam), "loss_gpu": loss, "fd_step_rel": 1e-6, "rows": rows,
+                 "max_rel_scalar": max(r["rel"] for r in rows[: len(ci) + 1]), "seconds": time.perf_counter() - t0}
+
+    if dist_.rank == 0:
+        out = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist_.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1000 * t_max / args.steps, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "potts_k3_192x192x192_r90_adjoint", "in_mask_voxels": vox, "k": 3,
+                       "lambda": lam, "tau": tau, "iters": iters, "checkpoint_every": every, "loss_eps": eps,
+                       "step": "forward with checkpoints + loss + backward (gradients of u, c, lambda)",
+                       "parallelism": f"replica x{dist_.world}" if dist_.world > 1 else "single"},
+            "roofline": None, "e2e": None, "gpu_launches": None, "clocks": clk, "cpu_baseline": None,
+            "gradient_check": check,
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    dist_.close()
+
+
 def main():
     args = parse_args()
     d = Dist()
@@ -656,6 +773,9 @@ def main():
         return
     if args.workload == "config3":
         run_batch(args, d)
+        return
+    if args.workload == "config4":
+        run_adjoint(args, d)
         return
     run_ours(args, d)
 

@@ -247,6 +247,29 @@ int potts_batch_get_info(const potts_batch *batch, potts_batch_info *info);
 int potts_batch_read_dq(potts_batch *batch, float *host);
 void potts_batch_destroy(potts_batch *batch);
 
+/* ---------------------------------------------------------------------------
+ * Differentiable solve.  No counterpart in the reference.
+ *
+ * potts_forward_ckpt runs `iters` iterations of the split form (FP32 state,
+ * one slab; the same bits as potts_solve_device) on one volume, keeps the state
+ * every ckpt_every iterations and after the last, and returns the segmentation
+ * loss   L = -(1/|mask|) sum_x log(V_t(x) + eps)   (t = d_truth's label index
+ * at x, V_K = 1 - sum V_i).  potts_backward recomputes each segment of
+ * ckpt_every iterations from its checkpoint and runs the reverse-mode kernels
+ * through it: dL/du into d_grad_u (device, map's span, zero outside the mask),
+ * dL/dc_i and dL/dlambda (host, accumulated in FP64).  The nearest-label
+ * initial state is piecewise constant in u and c and contributes nothing.
+ * d_u and d_truth are read again by potts_backward: they must stay valid and
+ * unchanged until then.  d_V (optional) receives V^iters (K-1 planes of span).
+ * ------------------------------------------------------------------------- */
+typedef struct potts_tape potts_tape;
+
+int potts_forward_ckpt(potts_context *ctx, const potts_mapping *map, const float *d_u, const uint8_t *d_truth, int K,
+                       const float *ci, float lambda, float tau1, float tau2, int iters, int ckpt_every, float eps,
+                       float *d_V, double *loss, potts_tape **out);
+int potts_backward(potts_tape *tape, float *d_grad_u, double *grad_ci, double *grad_lambda);
+void potts_tape_destroy(potts_tape *tape);
+
 /* Mask constructor of layout_cylinder::mapping_storage (include/layout_cylinder.h:152-195):
  * fills start_row[cols] and base[cols+1], returns the span (base[cols]). */
 uint64_t potts_cylinder_mapping(uint32_t rows, uint32_t cols, double xc, double yc, double r, uint32_t nstride,

@@ -99,6 +99,10 @@ SIGNATURES = {
     "potts_batch_get_info": (_I, [_P, ctypes.POINTER(PottsBatchInfo)]),
     "potts_batch_read_dq": (_I, [_P, _FP]),
     "potts_batch_destroy": (None, [_P]),
+    "potts_forward_ckpt": (_I, [_P, _MP, _P, _P, _I, _FP, _F, _F, _F, _I, _I, _F, _P,
+                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_P)]),
+    "potts_backward": (_I, [_P, _P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "potts_tape_destroy": (None, [_P]),
 }
 STATIC_MAX_COLS = 16384
 

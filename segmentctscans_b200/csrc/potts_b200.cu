@@ -14,6 +14,7 @@
 #include "../../include/potts_b200.h"
 #include "geometry.cuh"
 #include "kernels_plain.cuh"
+#include "kernels_adjoint.cuh"
 #include "kernels_tiled.cuh"
 #include "voxel.cuh"
 
@@ -927,6 +928,7 @@ int context_init(int device, void *stream, bool use_stream, potts_context **out)
     return POTTS_OK;
 }
 
+#include "adjoint.cuh"
 #include "batch.cuh"
 
 }  // namespace
@@ -1281,5 +1283,94 @@ int potts_batch_read_dq(potts_batch *b, float *host)
 }
 
 void potts_batch_destroy(potts_batch *b) { batch_free(b); }
+
+int potts_forward_ckpt(potts_context *ctx, const potts_mapping *map, const float *d_u, const uint8_t *d_truth, int K,
+                       const float *ci, float lambda, float tau1, float tau2, int iters, int ckpt_every, float eps,
+                       float *d_V, double *loss, potts_tape **out)
+{
+    if (!out) return fail(POTTS_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (!ctx) return fail(POTTS_EINVAL, "context is NULL");
+    potts_options o;
+    potts_default_options(&o);
+    POTTS_TRY(check_params(K, ci, lambda, tau1, tau2, iters, o));
+    if (!d_u || !d_truth) return fail(POTTS_EINVAL, "u or truth is NULL");
+    if (ckpt_every <= 0) return fail(POTTS_EINVAL, "ckpt_every must be >= 1");
+    if (!(eps > 0.0f) || !std::isfinite(eps)) return fail(POTTS_EINVAL, "eps must be positive");
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    auto *t = new potts_tape();
+    t->ctx = ctx;
+    int rc = copy_mapping(map, t->mc);
+    if (rc == POTTS_OK) {
+        t->K = K;
+        t->iters = iters;
+        t->every = std::min(ckpt_every, std::max(iters, 1));
+        t->n_ckpt = (iters + t->every - 1) / t->every + 1;
+        t->tau1 = tau1;
+        t->tau2 = tau2;
+        t->lambda = lambda;
+        t->eps = eps;
+        for (int i = 0; i < K; ++i) t->c[i] = ci[i];
+        t->d_u = d_u;
+        t->d_truth = d_truth;
+        const potts_mapping &m = t->mc.m;
+        t->g.n_lines = t->mc.n_lines;
+        t->g.nstride_w = (int)get_stride(m.n_images);
+        t->g.plane_w = t->mc.n_lines * (int64_t)t->g.nstride_w;
+        t->g.nstride_in = (int)m.nstride;
+        t->g.ns = (int)m.n_images;
+        t->g.slab_start = 0;
+        uint64_t vox = (uint64_t)t->mc.n_lines * m.n_images;
+        t->inv_count = vox > 0 ? 1.0 / (double)vox : 0.0;
+        rc = ensure(ctx, t->lines, sizeof(int4) * (size_t)std::max<int64_t>(t->mc.n_lines, 1));
+        if (rc == POTTS_OK && t->mc.n_lines > 0 &&
+            cudaMemcpy(t->lines.p, t->mc.lines.data(), sizeof(int4) * t->mc.n_lines, cudaMemcpyHostToDevice) !=
+                cudaSuccess)
+            rc = fail(POTTS_ECUDA, "copying the line table failed");
+        t->g.lines = static_cast<const int4 *>(t->lines.p);
+    }
+    if (rc == POTTS_OK) rc = tape_alloc(t);
+    if (rc == POTTS_OK && t->mc.n_lines > 0) {
+        switch (K) {
+        case 2: rc = tape_forward<2>(t, d_V, loss); break;
+        case 3: rc = tape_forward<3>(t, d_V, loss); break;
+        case 4: rc = tape_forward<4>(t, d_V, loss); break;
+        case 5: rc = tape_forward<5>(t, d_V, loss); break;
+        case 6: rc = tape_forward<6>(t, d_V, loss); break;
+        }
+    } else if (rc == POTTS_OK && loss) {
+        *loss = 0.0;
+    }
+    if (rc != POTTS_OK) {
+        const std::string msg = g_last_error;
+        tape_free(t);
+        g_last_error = msg;
+        return rc;
+    }
+    *out = t;
+    return POTTS_OK;
+}
+
+int potts_backward(potts_tape *t, float *d_grad_u, double *grad_ci, double *grad_lambda)
+{
+    if (!t || !d_grad_u) return fail(POTTS_EINVAL, "tape or grad_u is NULL");
+    POTTS_CUDA(cudaSetDevice(t->ctx->device));
+    if (t->mc.n_lines == 0) {
+        if (grad_lambda) *grad_lambda = 0.0;
+        if (grad_ci)
+            for (int i = 0; i < t->K; ++i) grad_ci[i] = 0.0;
+        return POTTS_OK;
+    }
+    switch (t->K) {
+    case 2: return tape_backward<2>(t, d_grad_u, grad_ci, grad_lambda);
+    case 3: return tape_backward<3>(t, d_grad_u, grad_ci, grad_lambda);
+    case 4: return tape_backward<4>(t, d_grad_u, grad_ci, grad_lambda);
+    case 5: return tape_backward<5>(t, d_grad_u, grad_ci, grad_lambda);
+    case 6: return tape_backward<6>(t, d_grad_u, grad_ci, grad_lambda);
+    }
+    return fail(POTTS_EINVAL, "K must be in [2, 6]");
+}
+
+void potts_tape_destroy(potts_tape *t) { tape_free(t); }
 
 }  // extern "C"

@@ -286,13 +286,12 @@ __device__ __forceinline__ void project_simplex(float (&q)[K])
 // exists.  Returns |q - V|^2 over all K labels.
 // ---------------------------------------------------------------------------
 template <int K>
-__device__ __forceinline__ float primal_voxel(float (&vnew)[K - 1], float (&vbar)[K - 1], const float (&v)[K - 1],
-                                              const float (&xi)[3 * (K - 1)], const float (&xin)[K - 1],
-                                              const float (&xir)[K - 1], const float (&xic)[K - 1], bool pn,
-                                              bool hn, bool pr, bool hr, bool pc, bool hc, float u,
-                                              const float (&c)[K], float lam, float tau1)
+__device__ __forceinline__ void primal_q(float (&q)[K], float (&vv)[K], const float (&v)[K - 1],
+                                         const float (&xi)[3 * (K - 1)], const float (&xin)[K - 1],
+                                         const float (&xir)[K - 1], const float (&xic)[K - 1], bool pn, bool hn,
+                                         bool pr, bool hr, bool pc, bool hc, float u, const float (&c)[K], float lam,
+                                         float tau1)
 {
-    float q[K], vv[K];
     float vk = 1.0f;
     float xk0 = 0.0f, xk1 = 0.0f, xk2 = 0.0f, xkn = 0.0f, xkr = 0.0f, xkc = 0.0f;
     const float fpn = pn ? 1.0f : 0.0f, fhn = hn ? 1.0f : 0.0f, fpr = pr ? 1.0f : 0.0f;
@@ -340,6 +339,17 @@ __device__ __forceinline__ float primal_voxel(float (&vnew)[K - 1], float (&vbar
         const float w = fmaf(-lam, d2, div);
         q[i] = fmaf(tau1, w, vi);
     }
+}
+
+template <int K>
+__device__ __forceinline__ float primal_voxel(float (&vnew)[K - 1], float (&vbar)[K - 1], const float (&v)[K - 1],
+                                              const float (&xi)[3 * (K - 1)], const float (&xin)[K - 1],
+                                              const float (&xir)[K - 1], const float (&xic)[K - 1], bool pn,
+                                              bool hn, bool pr, bool hr, bool pc, bool hc, float u,
+                                              const float (&c)[K], float lam, float tau1)
+{
+    float q[K], vv[K];
+    primal_q<K>(q, vv, v, xi, xin, xir, xic, pn, hn, pr, hr, pc, hc, u, c, lam, tau1);
     project_simplex<K>(q);
     float dq = 0.0f;
 #pragma unroll

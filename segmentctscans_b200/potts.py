@@ -361,3 +361,75 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+# --------------------------------------------------------------------------- differentiable solve
+class Tape:
+    """Forward pass with checkpoints of a differentiable solve (potts_forward_ckpt); `loss` is
+    -1/|mask| sum log(V_t + eps).  The device buffers u and truth must stay valid until backward()."""
+
+    def __init__(self, ctx: CudaContext, mapping: CylinderMapping, u_ptr: int, truth_ptr: int, ci: Sequence[float],
+                 lam: float, tau1: float, tau2: float, iters: int, ckpt_every: int = 20, eps: float = 1e-3,
+                 V_ptr: int = 0):
+        c = _ci_array(ci)
+        self.K = int(c.size)
+        self._mapping = mapping
+        loss = ctypes.c_double()
+        h = ctypes.c_void_p()
+        check(_native.host_lib().potts_forward_ckpt(
+            ctx.handle, ctypes.byref(mapping.as_c()), ctypes.c_void_p(int(u_ptr)), ctypes.c_void_p(int(truth_ptr)),
+            self.K, c.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(lam), float(tau1), float(tau2),
+            int(iters), int(ckpt_every), float(eps), ctypes.c_void_p(int(V_ptr)), ctypes.byref(loss),
+            ctypes.byref(h)))
+        self._h = h
+        self.loss = float(loss.value)
+
+    def backward(self, grad_u_ptr: int) -> tuple[np.ndarray, float]:
+        """dL/du into the device buffer at grad_u_ptr (the mapping's span); returns (dL/dc, dL/dlambda)."""
+        gc = np.zeros(self.K, np.float64)
+        gl = ctypes.c_double()
+        check(_native.host_lib().potts_backward(self._h, ctypes.c_void_p(int(grad_u_ptr)),
+                                                gc.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                ctypes.byref(gl)))
+        return gc, float(gl.value)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _native.host_lib().potts_tape_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def loss_and_grad(mapping: CylinderMapping, u: np.ndarray, truth: np.ndarray, ci: Sequence[float], lam: float,
+                  tau1: float, tau2: float, iters: int, *, ckpt_every: int = 20, eps: float = 1e-3,
+                  ctx: Optional[CudaContext] = None):
+    """Loss, dL/du (host, span), dL/dc and dL/dlambda of the unrolled solve on host arrays."""
+    import torch
+
+    own = ctx is None
+    ctx = ctx or make_context(0)
+    try:
+        dev = torch.device("cuda", ctx.device)
+        du = torch.from_numpy(np.ascontiguousarray(u, np.float32)).to(dev)
+        dt = torch.from_numpy(np.ascontiguousarray(truth, np.uint8)).to(dev)
+        gu = torch.zeros(mapping.span, dtype=torch.float32, device=dev)
+        torch.cuda.synchronize(dev)
+        with Tape(ctx, mapping, du.data_ptr(), dt.data_ptr(), ci, lam, tau1, tau2, iters, ckpt_every, eps) as t:
+            gc, gl = t.backward(gu.data_ptr())
+            loss = t.loss
+        ctx.synchronize()
+        return loss, gu.cpu().numpy(), gc, gl
+    finally:
+        if own:
+            ctx.close()
