@@ -730,9 +730,10 @@ def run_adjoint(args, dist_: Dist) -> None:
                 c2[i] = v
                 return loss64(u_h, c2, lam)
             g = cd(fc, ci[i], 1e-6)
-            rows.append({"param": f"c{i + 1}", "adjoint": float(gc[i]), "fd": g, "rel": abs(gc[i] - g) / abs(g)})
+            rows.append({"param": f"c{i + 1}", "adjoint": float(gc[i]), "fd": float(g),
+                         "rel": float(abs(gc[i] - g) / abs(g))})
         g = cd(lambda v: loss64(u_h, ci, v), lam, 1e-6)
-        rows.append({"param": "lambda", "adjoint": gl, "fd": g, "rel": abs(gl - g) / abs(g)})
+        rows.append({"param": "lambda", "adjoint": float(gl), "fd": float(g), "rel": float(abs(gl - g) / abs(g))})
         gu_h = gu.cpu().numpy()
         rng = np.random.default_rng(0)
         idx = np.arange(m.span).reshape(m.n_lines, m.nstride)[:, : m.n_images].reshape(-1)
@@ -743,9 +744,9 @@ def run_adjoint(args, dist_: Dist) -> None:
                 return loss64(u2, ci, lam)
             for rel in (1e-6, 1e-4):
                 g = cd(fu, float(u_h[j]), rel)
-                rows.append({"param": f"u[{int(j)}]", "step": rel, "adjoint": float(gu_h[j]), "fd": g,
-                             "rel": abs(gu_h[j] - g) / abs(g) if g != 0 else abs(gu_h[j])})
-        check = {"loss_fp64": loss64(u_h, ci, lam), "loss_gpu": loss, "fd_step_rel": 1e-6, "rows": rows,
+                rows.append({"param": f"u[{int(j)}]", "step": rel, "adjoint": float(gu_h[j]), "fd": float(g),
+                             "rel": float(abs(gu_h[j] - g) / abs(g) if g != 0 else abs(gu_h[j]))})
+        check = {"loss_fp64": loss64(u_h, ci, lam), "loss_gpu": float(loss), "fd_step_rel": 1e-6, "rows": rows,
                  "max_rel_scalar": max(r["rel"] for r in rows[: len(ci) + 1]), "seconds": time.perf_counter() - t0}
 
     if dist_.rank == 0:
