@@ -270,6 +270,25 @@ int potts_forward_ckpt(potts_context *ctx, const potts_mapping *map, const float
 int potts_backward(potts_tape *tape, float *d_grad_u, double *grad_ci, double *grad_lambda);
 void potts_tape_destroy(potts_tape *tape);
 
+/* ---------------------------------------------------------------------------
+ * Step-by-step split solve (no counterpart in the reference), for column
+ * sharding over several GPUs: the caller exchanges halo columns between the
+ * steps.  FP32 state, laid out with the mapping's own stride (component i of
+ * xi / v / vb starts at the returned pointer + i * plane_w, voxel (n, row, col)
+ * at the mapping's offset), so that a column's lines are the same span range
+ * in the state as in the mapping.  Create runs the nearest-label init; each
+ * call enqueues on the context's stream.
+ * ------------------------------------------------------------------------- */
+typedef struct potts_stepper potts_stepper;
+
+int potts_stepper_create(potts_context *ctx, const potts_mapping *map, const float *d_u, int K, const float *ci,
+                         float lambda, float tau1, float tau2, potts_stepper **out);
+int potts_stepper_dual(potts_stepper *stepper);            /* Xi <- Pi_K(Xi + tau2 grad+ Vbar) */
+int potts_stepper_primal(potts_stepper *stepper, int it);  /* V, Vbar of iteration it (0-based) */
+int potts_stepper_state(potts_stepper *stepper, float **xi, float **v, float **vb, int64_t *plane_w);
+int potts_stepper_finish(potts_stepper *stepper, float *d_res, uint8_t *d_labels, float *d_V);
+void potts_stepper_destroy(potts_stepper *stepper);
+
 /* Mask constructor of layout_cylinder::mapping_storage (include/layout_cylinder.h:152-195):
  * fills start_row[cols] and base[cols+1], returns the span (base[cols]). */
 uint64_t potts_cylinder_mapping(uint32_t rows, uint32_t cols, double xc, double yc, double r, uint32_t nstride,

@@ -103,6 +103,13 @@ SIGNATURES = {
                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_P)]),
     "potts_backward": (_I, [_P, _P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "potts_tape_destroy": (None, [_P]),
+    "potts_stepper_create": (_I, [_P, _MP, _P, _I, _FP, _F, _F, _F, ctypes.POINTER(_P)]),
+    "potts_stepper_dual": (_I, [_P]),
+    "potts_stepper_primal": (_I, [_P, _I]),
+    "potts_stepper_state": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),
+                                 ctypes.POINTER(ctypes.c_int64)]),
+    "potts_stepper_finish": (_I, [_P, _P, _P, _P]),
+    "potts_stepper_destroy": (None, [_P]),
 }
 STATIC_MAX_COLS = 16384
 

@@ -930,6 +930,7 @@ int context_init(int device, void *stream, bool use_stream, potts_context **out)
 
 #include "adjoint.cuh"
 #include "batch.cuh"
+#include "stepper.cuh"
 
 }  // namespace
 
@@ -1372,5 +1373,74 @@ int potts_backward(potts_tape *t, float *d_grad_u, double *grad_ci, double *grad
 }
 
 void potts_tape_destroy(potts_tape *t) { tape_free(t); }
+
+int potts_stepper_create(potts_context *ctx, const potts_mapping *map, const float *d_u, int K, const float *ci,
+                         float lambda, float tau1, float tau2, potts_stepper **out)
+{
+    if (!out) return fail(POTTS_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (!ctx) return fail(POTTS_EINVAL, "context is NULL");
+    potts_options o;
+    potts_default_options(&o);
+    POTTS_TRY(check_params(K, ci, lambda, tau1, tau2, 0, o));
+    if (!d_u) return fail(POTTS_EINVAL, "u is NULL");
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    auto *st = new potts_stepper();
+    st->ctx = ctx;
+    int rc = copy_mapping(map, st->mc);
+    if (rc == POTTS_OK) {
+        st->K = K;
+        st->tau1 = tau1;
+        st->tau2 = tau2;
+        st->lambda = lambda;
+        for (int i = 0; i < K; ++i) st->c[i] = ci[i];
+        st->d_u = d_u;
+        const potts_mapping &m = st->mc.m;
+        st->g.n_lines = st->mc.n_lines;
+        st->g.nstride_w = (int)m.nstride;  // the mapping's layout
+        st->g.plane_w = st->mc.n_lines * (int64_t)m.nstride;
+        st->g.nstride_in = (int)m.nstride;
+        st->g.ns = (int)m.n_images;
+        st->g.slab_start = 0;
+        rc = ensure(ctx, st->lines, sizeof(int4) * (size_t)std::max<int64_t>(st->mc.n_lines, 1));
+        if (rc == POTTS_OK && st->mc.n_lines > 0 &&
+            cudaMemcpy(st->lines.p, st->mc.lines.data(), sizeof(int4) * st->mc.n_lines, cudaMemcpyHostToDevice) !=
+                cudaSuccess)
+            rc = fail(POTTS_ECUDA, "copying the line table failed");
+        st->g.lines = static_cast<const int4 *>(st->lines.p);
+        if (rc == POTTS_OK)
+            rc = ensure(ctx, st->state, sizeof(float) * 5 * (size_t)(K - 1) * (size_t)std::max<int64_t>(st->g.plane_w, 1));
+    }
+    if (rc == POTTS_OK) rc = stepper_dispatch(st, 0, 0, nullptr, nullptr, nullptr);
+    if (rc != POTTS_OK) {
+        const std::string msg = g_last_error;
+        stepper_free(st);
+        g_last_error = msg;
+        return rc;
+    }
+    *out = st;
+    return POTTS_OK;
+}
+
+int potts_stepper_dual(potts_stepper *s) { return stepper_dispatch(s, 1, 0, nullptr, nullptr, nullptr); }
+
+int potts_stepper_primal(potts_stepper *s, int it) { return stepper_dispatch(s, 2, it, nullptr, nullptr, nullptr); }
+
+int potts_stepper_state(potts_stepper *s, float **xi, float **v, float **vb, int64_t *plane_w)
+{
+    if (!s) return fail(POTTS_EINVAL, "stepper is NULL");
+    if (xi) *xi = stepper_xi(s);
+    if (v) *v = stepper_v(s);
+    if (vb) *vb = stepper_vb(s);
+    if (plane_w) *plane_w = s->g.plane_w;
+    return POTTS_OK;
+}
+
+int potts_stepper_finish(potts_stepper *s, float *d_res, uint8_t *d_labels, float *d_V)
+{
+    return stepper_dispatch(s, 3, 0, d_res, d_labels, d_V);
+}
+
+void potts_stepper_destroy(potts_stepper *s) { stepper_free(s); }
 
 }  // extern "C"

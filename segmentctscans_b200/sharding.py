@@ -107,14 +107,12 @@ def make_shard(m: CylinderMapping, world: int, rank: int,
 
 @dataclass
 class HaloExchange:
-    """The two exchanges of an iteration, written against send/recv callables so that the same
-    protocol runs over NCCL (CUDA tensors), gloo (CPU tensors) or plain copies between shards
-    held by one process.
+    """The two exchanges of an iteration, written against an exchange callable so that the same
+    protocol runs over NCCL (CUDA tensors) or gloo (CPU tensors).
 
-    post(kind, plane_pairs): for kind "vbar" every rank sends the Vbar planes of its first owned
-    column to rank - 1 and receives those of its right halo column from rank + 1; for kind "xi"
-    it sends the Xi planes of its last owned column to rank + 1 and receives its left halo
-    column's from rank - 1."""
+    vbar(planes): every rank sends the Vbar planes of its first owned column to rank - 1 and
+    receives those of its right halo column from rank + 1.  xi(planes): it sends the Xi planes
+    of its last owned column to rank + 1 and receives its left halo column's from rank - 1."""
     shard: ColumnShard
     exchange: Callable[[list, list], None]   # (sends [(peer, array)], recvs [(peer, array)]) -> waits
 
@@ -160,3 +158,115 @@ def torch_exchange(sends, recvs) -> None:
             req.wait()
     for planes, b, e, buf in fills:
         planes[:, b:e].copy_(buf)
+
+
+class _CudaArray:
+    """__cuda_array_interface__ over device memory owned by the library (no copy)."""
+
+    def __init__(self, ptr: int, shape, strides):
+        self.__cuda_array_interface__ = {"data": (ptr, False), "shape": shape, "strides": strides,
+                                         "typestr": "<f4", "version": 2}
+
+
+def _device_view(ptr: int, planes: int, plane_w: int, span: int, dev):
+    import torch
+
+    return torch.as_tensor(_CudaArray(ptr, (planes, span), (4 * plane_w, 4)), device=dev)
+
+
+class Stepper:
+    """One local volume stepped on the GPU (potts_stepper_*).  xi [3(K-1), span], v and vb
+    [K-1, span] are torch views of the library's device buffers (valid until close())."""
+
+    def __init__(self, ctx, mapping: CylinderMapping, u_ptr: int, ci, lam: float, tau1: float, tau2: float):
+        import ctypes
+
+        import torch
+
+        from . import _native
+        from ._native import check
+
+        c = np.ascontiguousarray(np.asarray(ci, np.float32))
+        self.K = int(c.size)
+        self._lib = _native.host_lib()
+        self._check = check
+        self._mapping = mapping
+        h = ctypes.c_void_p()
+        check(self._lib.potts_stepper_create(ctx.handle, ctypes.byref(mapping.as_c()), ctypes.c_void_p(int(u_ptr)),
+                                             self.K, c.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(lam),
+                                             float(tau1), float(tau2), ctypes.byref(h)))
+        self._h = h
+        ptrs = [ctypes.c_void_p() for _ in range(3)]
+        pw = ctypes.c_int64()
+        check(self._lib.potts_stepper_state(h, *(ctypes.byref(p) for p in ptrs), ctypes.byref(pw)))
+        dev = torch.device("cuda", ctx.device)
+        span = mapping.span
+        self.xi = _device_view(int(ptrs[0].value), 3 * (self.K - 1), int(pw.value), span, dev)
+        self.v = _device_view(int(ptrs[1].value), self.K - 1, int(pw.value), span, dev)
+        self.vb = _device_view(int(ptrs[2].value), self.K - 1, int(pw.value), span, dev)
+
+    def dual(self) -> None:
+        self._check(self._lib.potts_stepper_dual(self._h))
+
+    def primal(self, it: int) -> None:
+        self._check(self._lib.potts_stepper_primal(self._h, int(it)))
+
+    def finish(self, res_ptr: int = 0, labels_ptr: int = 0, V_ptr: int = 0) -> None:
+        import ctypes
+
+        self._check(self._lib.potts_stepper_finish(self._h, ctypes.c_void_p(res_ptr), ctypes.c_void_p(labels_ptr),
+                                                   ctypes.c_void_p(V_ptr)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.potts_stepper_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def exchange_in_process(shards: list[ColumnShard], planes: list, kind: str) -> None:
+    """The exchange of one iteration between shards held by one process (device copies): kind
+    "vbar" fills every right halo column from the right neighbour's first owned column, "xi"
+    every left halo column from the left neighbour's last owned column."""
+    for r, s in enumerate(shards):
+        if kind == "vbar" and s.right_halo:
+            n = shards[r + 1]
+            b, e = s.col_span(s.c_hi)
+            nb, ne = n.col_span(n.c_lo)
+            planes[r][:, b:e].copy_(planes[r + 1][:, nb:ne])
+        if kind == "xi" and s.left_halo:
+            n = shards[r - 1]
+            b, e = s.col_span(s.c_lo - 1)
+            nb, ne = n.col_span(n.c_hi - 1)
+            planes[r][:, b:e].copy_(planes[r - 1][:, nb:ne])
+
+
+def solve_sharded(ctx, m: CylinderMapping, u, ci, lam: float, tau1: float, tau2: float, iters: int, rank: int,
+                  world: int):
+    """This rank's part of a column-sharded solve over torch.distributed (NCCL between GPUs).
+    u: the global u on this rank's device (a torch tensor over the mapping's span).  Returns
+    the shard and its local (labels uint8 [span], V [K-1, span]) device tensors, exact for the
+    owned columns.  The context should run on torch's current stream, which orders the
+    exchanges and the steps."""
+    import torch
+
+    shard = make_shard(m, world, rank)
+    u_loc = u[shard.span_begin:shard.span_begin + shard.mapping.span].contiguous()
+    st = Stepper(ctx, shard.mapping, u_loc.data_ptr(), ci, lam, tau1, tau2)
+    ex = HaloExchange(shard, torch_exchange)
+    for it in range(iters):
+        ex.vbar(st.vb)
+        st.dual()
+        ex.xi(st.xi)
+        st.primal(it)
+    labels = torch.zeros(shard.mapping.span, dtype=torch.uint8, device=u.device)
+    V = torch.zeros((st.K - 1, shard.mapping.span), dtype=torch.float32, device=u.device)
+    st.finish(labels_ptr=labels.data_ptr(), V_ptr=V.data_ptr())
+    ctx.synchronize()
+    st.close()
+    return shard, labels, V
