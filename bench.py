@@ -73,7 +73,7 @@ def parse_args():
                    help="state storage of the timed solves")
     p.add_argument("--no-storage-compare", action="store_true",
                    help="skip the FP32-plain / BF16 / FP16 comparison solves")
-    p.add_argument("--workload", choices=["config1", "config2", "config3", "config4", "config0", "mid", "mid4"],
+    p.add_argument("--workload", choices=["config1", "config2", "config3", "config4", "config0", "mid", "mid4", "tv"],
                    default="config1",
                    help="config1: 768x768x1024 r=370 (the benchmark); config0: 128^3 r=60; "
                         "mid: 384x384x256 r=180 (profiling size, state > L2)")
@@ -766,6 +766,115 @@ def run_adjoint(args, dist_: Dist) -> None:
     dist_.close()
 
 
+def run_tv(args, dist_: Dist) -> None:
+    """TV-L2 denoising (chambolle(), the next row after the Potts solve) on the 768^2 x 1024 core:
+    lambda = 0.06, tau = 0.99/6, 150 iterations as totalvarmin.cpp:60,140 calls it."""
+    import numpy as np
+    import torch
+
+    from segmentctscans_b200 import potts
+    from segmentctscans_b200.phantom import config1_phantom
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    dev = torch.device("cuda", dist_.local)
+    torch.cuda.set_device(dev)
+    dist_.init("nccl")
+    iters = 150 if args.iters == 1000 else args.iters
+    lam, tau = 0.06, 0.99 / 6.0
+    ph = config1_phantom(seed=dist_.rank, device=dev)
+    m, u = ph.mapping, ph.u
+    stream = torch.cuda.current_stream(dev)
+    ctx = potts.make_context(dev.index, stream=stream.cuda_stream)
+    g = torch.empty_like(u)
+
+    def step():
+        g.copy_(u)
+        return potts.tv_denoise(ctx, m, g.data_ptr(), lam, tau, iters)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    dist_.barrier()
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    stats = [step() for _ in range(args.steps)]
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    dist_.barrier()
+    clk = clocks.stop()
+    t_max = dist_.reduce(e0.elapsed_time(e1) / 1000.0, "max")
+    vox = m.data_size
+    value = dist_.reduce(float(vox) * iters * args.steps, "sum") / t_max / 1e9
+    launch_s = sum(s.loop_ms for s in stats) / 1000.0 / max(sum(s.loop_launches for s in stats), 1)
+    bpv = 48  # div: xi (3) in, v out; grad: v, g, xi (3) in, xi (3) out; FP32
+    achieved = bpv / 2 * vox / launch_s / 1e9
+    peaks = measured_peaks()
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None,
+                "kernel": "potts::tv_div_kernel + tv_grad_kernel (average launch)", "bytes_per_voxel_iter": bpv,
+                "avg_launch_ms": round(launch_s * 1000, 4),
+                "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)"}
+    e2e = None
+    if not args.no_e2e:
+        hu = torch.empty(m.span, dtype=torch.float32, pin_memory=True)
+        hu.copy_(u.cpu())
+        hout = torch.empty(m.span, dtype=torch.float32, pin_memory=True)
+
+        def e2e_step():
+            g.copy_(hu, non_blocking=True)
+            potts.tv_denoise(ctx, m, g.data_ptr(), lam, tau, iters, stats=False)
+            hout.copy_(g, non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize(dev)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = time.perf_counter()
+        f0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        f1.record(stream)
+        torch.cuda.synchronize(dev)
+        te = dist_.reduce(max(f0.elapsed_time(f1) / 1000.0, time.perf_counter() - w0), "max")
+        e2e = {"value": dist_.reduce(float(vox) * iters * args.steps, "sum") / te / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": 4 * m.span, "d2h_bytes_per_step": 4 * m.span}
+    cpu = None
+    if dist_.rank == 0 and dist_.world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle
+
+        sph = cpu_sample_phantom()
+        threads = os.cpu_count() or 1
+        oracle.set_threads(threads)
+        su = sph.u.numpy().copy()
+        t0 = time.perf_counter()
+        oracle.tv(sph.mapping, su, lam, tau, 1, "f64")
+        t1 = time.perf_counter() - t0
+        it_cpu = max(1, min(150, int(args.cpu_seconds / max(t1, 1e-3))))
+        t0 = time.perf_counter()
+        oracle.tv(sph.mapping, su, lam, tau, it_cpu, "f64")
+        tc = time.perf_counter() - t0
+        cpu = {"value": sph.mapping.data_size * it_cpu / tc / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"FP64 TV oracle, OpenMP {threads} threads: 768x768 cross-section, 16 slices, "
+                         f"{it_cpu} iterations, {tc:.1f} s"}
+    if dist_.rank == 0:
+        out = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist_.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1000 * t_max / args.steps, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"tv_{m.rows}x{m.cols}x{m.n_images}_r370", "in_mask_voxels": vox,
+                       "lambda": lam, "tau": tau, "iters": iters,
+                       "parallelism": f"replica x{dist_.world}" if dist_.world > 1 else "single",
+                       "l2": "inputs larger than L2"},
+            "roofline": roofline, "e2e": e2e, "gpu_launches": sum(s.total_launches for s in stats), "clocks": clk,
+            "cpu_baseline": cpu, "quality": {"final_sqrt_max_dxi2": stats[-1].dq_last},
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    dist_.close()
+
+
 def main():
     args = parse_args()
     d = Dist()
@@ -777,6 +886,9 @@ def main():
         return
     if args.workload == "config4":
         run_adjoint(args, d)
+        return
+    if args.workload == "tv":
+        run_tv(args, d)
         return
     run_ours(args, d)
 

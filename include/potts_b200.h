@@ -289,6 +289,15 @@ int potts_stepper_state(potts_stepper *stepper, float **xi, float **v, float **v
 int potts_stepper_finish(potts_stepper *stepper, float *d_res, uint8_t *d_labels, float *d_V);
 void potts_stepper_destroy(potts_stepper *stepper);
 
+/* TV-L2 (ROF) denoising of a field in place: chambolle() of
+ * totalvarmin/chambolle.cpp:220-276 (Chambolle's projection algorithm, xi and
+ * v zero at the start, `iters` iterations of the div and grad kernels, then
+ * g <- g - lambda div xi).  The reference's caller (totalvarmin.cpp:140) uses
+ * tau = 0.99 / 6 and 150 iterations.  stats (optional): solve_ms, loop_ms,
+ * launches, dq_trace / dq_last of the per-iteration max |dxi|^2. */
+int potts_tv_denoise(potts_context *ctx, const potts_mapping *map, float *d_g, float lambda, float tau, int iters,
+                     potts_stats *stats);
+
 /* Mask constructor of layout_cylinder::mapping_storage (include/layout_cylinder.h:152-195):
  * fills start_row[cols] and base[cols+1], returns the span (base[cols]). */
 uint64_t potts_cylinder_mapping(uint32_t rows, uint32_t cols, double xc, double yc, double r, uint32_t nstride,

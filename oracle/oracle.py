@@ -200,3 +200,20 @@ def energies(m, K: int, xi, V, u, ci, lam, precision: str = "f64") -> np.ndarray
     f(ctypes.byref(oc), K, _ptr(xi, ct), _ptr(V, ct), _ptr(u, ctypes.c_float), _ptr(c, ctypes.c_float), float(lam),
       _ptr(out, ctypes.c_double))
     return out
+
+
+def tv(m, g: np.ndarray, lam: float, tau: float, iters: int, precision: str = "f64"):
+    """TV-L2 denoising by Chambolle's projection algorithm (totalvarmin/chambolle.cpp:220-276) on the
+    CPU: returns (the denoised field, float32 over the span; the per-iteration max |dxi|^2)."""
+    _, ct = _real(precision)
+    out = np.ascontiguousarray(g, dtype=np.float32).copy()
+    dq = np.zeros(max(iters, 1), np.float32)
+    f = getattr(lib(), f"oracle_tv_{precision}")
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.POINTER(OCyl), ctypes.POINTER(ctypes.c_float), ctypes.c_float, ctypes.c_float,
+                  ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    oc = ocyl(m)
+    if f(ctypes.byref(oc), _ptr(out, ctypes.c_float), float(lam), float(tau), int(iters),
+         _ptr(dq, ctypes.c_float)) != 0:
+        raise RuntimeError("oracle_tv failed")
+    return out, dq[:iters]

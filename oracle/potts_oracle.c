@@ -600,3 +600,99 @@ void NAME(oracle_energies)(const ocyl *m, int K, const REAL *xi, const REAL *V, 
     ostate st = {m, K, (int64_t)m->base[m->cols], (REAL *)xi, (REAL *)V, NULL, 0, 0};
     energies(&st, u, c, (REAL)lam, 0, (int)m->n_images, out);
 }
+
+/* ---------------------------------------------------------------------------
+ * TV-L2 (ROF) denoising by Chambolle's projection algorithm,
+ * totalvarmin/chambolle.cpp:220-276, on the cylinder.  xi (3 planes) and v
+ * start at zero; each iteration
+ *   v  = div xi                                   (div_kernel, :33-87)
+ *   G  = grad+ v - (grad+ g) / lambda             (grad_kernel, :89-166)
+ *   xi = (xi + tau G) / (1 + tau |G|),  dq = max |xi_new - xi|^2
+ * and after the last one g <- g - lambda div xi   (update_kernel, :168-218).
+ * The differences use the same neighbour tests as the Potts kernels; the
+ * multiply-adds are fused where the reference's clang build contracts them
+ * (sum of squares, 1 + tau sqrt, xi + tau G, g - lambda d).  g is float and
+ * updated in place; dq_trace (optional) receives the per-iteration dq.
+ * ------------------------------------------------------------------------- */
+static void tv_div(const ocyl *m, REAL *const xi[3], REAL *out, int64_t col, int64_t row, int64_t n, int64_t o)
+{
+    const int64_t nn = m->n_images;
+    REAL d = 0;
+    if (0 < n) d -= xi[0][offset(m, n - 1, row, col)];
+    if (nn - 1 > n) d += xi[0][o];
+    if (row_begin(m, col) < row) d -= xi[1][offset(m, n, row - 1, col)];
+    if (row_end(m, col) - 1 > row) d += xi[1][o];
+    if ((int64_t)m->col_begin < col && row_in(m, (uint32_t)(col - 1), row)) d -= xi[2][offset(m, n, row, (uint32_t)(col - 1))];
+    if ((int64_t)m->col_end - 1 > col && row_in(m, (uint32_t)(col + 1), row)) d += xi[2][o];
+    *out = d;
+}
+
+int NAME(oracle_tv)(const ocyl *m, float *g, float lam_f, float tau_f, int iters, float *dq_trace)
+{
+    if (!m || !g || iters < 0) return -1;
+    const int64_t span = (int64_t)m->base[m->cols];
+    const size_t ns = (size_t)(span > 0 ? span : 1);
+    REAL *buf = (REAL *)calloc(ns * 5, sizeof(REAL));
+    if (!buf) return -1;
+    REAL *xi[3] = {buf, buf + ns, buf + 2 * ns};
+    REAL *v = buf + 3 * ns, *gr = buf + 4 * ns;
+    const REAL lam = (REAL)lam_f, tau = (REAL)tau_f;
+    for (int64_t i = 0; i < span; ++i) gr[i] = (REAL)g[i];
+    const int64_t nn = m->n_images;
+    for (int it = 0; it < iters; ++it) {
+#pragma omp parallel for schedule(dynamic, 4)
+        for (int64_t col = m->col_begin; col < m->col_end; ++col)
+            for (int64_t row = row_begin(m, col); row < row_end(m, col); ++row)
+                for (int64_t n = 0; n < nn; ++n) {
+                    const int64_t o = offset(m, n, row, col);
+                    tv_div(m, xi, &v[o], col, row, n, o);
+                }
+        REAL dq_max = 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(max : dq_max)
+        for (int64_t col = m->col_begin; col < m->col_end; ++col)
+            for (int64_t row = row_begin(m, col); row < row_end(m, col); ++row)
+                for (int64_t n = 0; n < nn; ++n) {
+                    const int64_t o = offset(m, n, row, col);
+                    REAL g1 = 0, g2 = 0, g3 = 0;
+                    if (nn - 1 > n) {
+                        const int64_t p = offset(m, n + 1, row, col);
+                        g1 = (v[p] - v[o]) - (gr[p] - gr[o]) / lam;
+                    }
+                    if (row_end(m, col) - 1 > row) {
+                        const int64_t p = offset(m, n, row + 1, col);
+                        g2 = (v[p] - v[o]) - (gr[p] - gr[o]) / lam;
+                    }
+                    if ((int64_t)m->col_end - 1 > col && row_in(m, (uint32_t)(col + 1), row)) {
+                        const int64_t p = offset(m, n, row, (uint32_t)(col + 1));
+                        g3 = (v[p] - v[o]) - (gr[p] - gr[o]) / lam;
+                    }
+                    REAL s = g1 * g1;
+                    s = FMA(g2, g2, s);
+                    s = FMA(g3, g3, s);
+                    const REAL denom = FMA(tau, SQRT(s), (REAL)1);
+                    const REAL q1 = FMA(tau, g1, xi[0][o]) / denom;
+                    const REAL q2 = FMA(tau, g2, xi[1][o]) / denom;
+                    const REAL q3 = FMA(tau, g3, xi[2][o]) / denom;
+                    const REAL e1 = xi[0][o] - q1, e2 = xi[1][o] - q2, e3 = xi[2][o] - q3;
+                    REAL dq = e1 * e1;
+                    dq = FMA(e2, e2, dq);
+                    dq = FMA(e3, e3, dq);
+                    if (dq > dq_max) dq_max = dq;
+                    xi[0][o] = q1;
+                    xi[1][o] = q2;
+                    xi[2][o] = q3;
+                }
+        if (dq_trace) dq_trace[it] = (float)dq_max;
+    }
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t col = m->col_begin; col < m->col_end; ++col)
+        for (int64_t row = row_begin(m, col); row < row_end(m, col); ++row)
+            for (int64_t n = 0; n < nn; ++n) {
+                const int64_t o = offset(m, n, row, col);
+                REAL d;
+                tv_div(m, xi, &d, col, row, n, o);
+                g[o] = (float)FMA(-lam, d, gr[o]);
+            }
+    free(buf);
+    return 0;
+}

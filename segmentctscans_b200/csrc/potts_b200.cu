@@ -16,6 +16,7 @@
 #include "kernels_plain.cuh"
 #include "kernels_adjoint.cuh"
 #include "kernels_tiled.cuh"
+#include "kernels_tv.cuh"
 #include "voxel.cuh"
 
 // Sets the message potts_last_error() returns on this thread; used by the
@@ -932,6 +933,68 @@ int context_init(int device, void *stream, bool use_stream, potts_context **out)
 #include "batch.cuh"
 #include "stepper.cuh"
 
+// TV-L2 denoising (chambolle(), totalvarmin/chambolle.cpp:220-276) of d_g in
+// place; xi and v live in the context's state buffer, laid out like g.
+int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, potts_stats *stats)
+{
+    const MappingCopy &mc = ctx->mapping;
+    Geometry g{};
+    g.lines = static_cast<const int4 *>(ctx->lines.p);
+    g.n_lines = mc.n_lines;
+    g.nstride_w = (int)mc.m.nstride;
+    g.plane_w = mc.n_lines * (int64_t)mc.m.nstride;
+    g.nstride_in = (int)mc.m.nstride;
+    g.ns = (int)mc.m.n_images;
+    g.slab_start = 0;
+    cudaStream_t s = ctx->stream;
+    POTTS_TRY(ensure(ctx, ctx->state, sizeof(float) * 4 * (size_t)std::max<int64_t>(g.plane_w, 1)));
+    POTTS_TRY(ensure(ctx, ctx->dq, sizeof(float) * (size_t)std::max(iters, 1)));
+    float *xi = static_cast<float *>(ctx->state.p), *v = xi + 3 * g.plane_w;
+    float *dq = static_cast<float *>(ctx->dq.p);
+    ctx->seg_used = 0;
+    ctx->seg_open = false;
+    ctx->loop_launches = ctx->total_launches = 0;
+    POTTS_CUDA(cudaEventRecord(ctx->ev0, s));
+    POTTS_CUDA(cudaMemsetAsync(ctx->state.p, 0, sizeof(float) * 4 * (size_t)std::max<int64_t>(g.plane_w, 1), s));
+    POTTS_CUDA(cudaMemsetAsync(dq, 0, sizeof(float) * (size_t)std::max(iters, 1), s));
+    const unsigned nb = plain_blocks(g, 0, g.ns);
+    if (g.n_lines > 0) {
+        POTTS_TRY(seg_begin(ctx));
+        for (int it = 0; it < iters; ++it) {
+            potts::tv_div_kernel<<<nb, potts::kPlainThreads, 0, s>>>(g, xi, v);
+            potts::tv_grad_kernel<<<nb, potts::kPlainThreads, 0, s>>>(g, d_g, xi, v, lam, tau, dq + it);
+            ctx->loop_launches += 2;
+            ctx->total_launches += 2;
+        }
+        POTTS_TRY(seg_end(ctx));
+        potts::tv_update_kernel<<<nb, potts::kPlainThreads, 0, s>>>(g, d_g, xi, lam);
+        ctx->total_launches += 1;
+        POTTS_CUDA(cudaGetLastError());
+    }
+    POTTS_CUDA(cudaEventRecord(ctx->ev1, s));
+    if (stats) {
+        POTTS_CUDA(cudaStreamSynchronize(s));
+        float ms = 0.0f;
+        POTTS_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        stats->n_slabs = 1;
+        stats->slab_w = g.ns;
+        stats->iters = iters;
+        stats->solve_ms = ms;
+        POTTS_TRY(seg_total_ms(ctx, &stats->loop_ms));
+        stats->loop_launches = ctx->loop_launches;
+        stats->total_launches = ctx->total_launches;
+        stats->state_bytes = sizeof(float) * 4 * (uint64_t)std::max<int64_t>(g.plane_w, 1);
+        stats->dq_last = 0.0f;
+        if (iters > 0) {
+            std::vector<float> tr((size_t)iters);
+            POTTS_CUDA(cudaMemcpy(tr.data(), dq, sizeof(float) * iters, cudaMemcpyDeviceToHost));
+            stats->dq_last = std::sqrt(tr.back());
+            if (stats->dq_trace) std::memcpy(stats->dq_trace, tr.data(), sizeof(float) * iters);
+        }
+    }
+    return POTTS_OK;
+}
+
 }  // namespace
 
 __attribute__((visibility("hidden"))) void potts_set_last_error(const std::string &msg) { g_last_error = msg; }
@@ -1442,5 +1505,18 @@ int potts_stepper_finish(potts_stepper *s, float *d_res, uint8_t *d_labels, floa
 }
 
 void potts_stepper_destroy(potts_stepper *s) { stepper_free(s); }
+
+int potts_tv_denoise(potts_context *ctx, const potts_mapping *map, float *d_g, float lambda, float tau, int iters,
+                     potts_stats *stats)
+{
+    if (!ctx) return fail(POTTS_EINVAL, "context is NULL");
+    if (!d_g) return fail(POTTS_EINVAL, "g is NULL");
+    if (!std::isfinite(lambda) || lambda == 0.0f || !std::isfinite(tau))
+        return fail(POTTS_EINVAL, "lambda must be finite and non-zero, tau finite");
+    if (iters < 0) return fail(POTTS_EINVAL, "iters must be >= 0");
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    POTTS_TRY(upload_lines(ctx, map));
+    return tv_run(ctx, d_g, lambda, tau, iters, stats);
+}
 
 }  // extern "C"

@@ -433,3 +433,31 @@ def loss_and_grad(mapping: CylinderMapping, u: np.ndarray, truth: np.ndarray, ci
     finally:
         if own:
             ctx.close()
+
+
+# --------------------------------------------------------------------------- TV-L2 denoising
+def tv_denoise(ctx: CudaContext, mapping: CylinderMapping, g_ptr: int, lam: float, tau: float, iters: int, *,
+               stats: bool = True) -> Optional[SolveStats]:
+    """chambolle() (totalvarmin/chambolle.cpp:220-276): TV-L2 denoising of the device field at g_ptr
+    (the mapping's span, float32) in place."""
+    st, dq, en = _make_stats(iters, 0, stats)
+    check(_native.host_lib().potts_tv_denoise(ctx.handle, ctypes.byref(mapping.as_c()), ctypes.c_void_p(int(g_ptr)),
+                                              float(lam), float(tau), int(iters),
+                                              ctypes.byref(st) if stats else None))
+    return _stats_out(st, dq, en) if stats else None
+
+
+def tv_denoise_host(mapping: CylinderMapping, g: np.ndarray, lam: float, tau: float, iters: int, *,
+                    ctx: Optional[CudaContext] = None) -> tuple[np.ndarray, SolveStats]:
+    """TV-L2 denoising of a host field (float32, the mapping's span); returns (result, stats)."""
+    own = ctx is None
+    ctx = ctx or make_context(0)
+    try:
+        fld = upload(ctx, mapping, np.ascontiguousarray(g, np.float32))
+        st = tv_denoise(ctx, mapping, fld.data_ptr(), lam, tau, iters)
+        out = download(ctx, fld)
+        fld.free()
+        return out, st
+    finally:
+        if own:
+            ctx.close()

@@ -227,3 +227,22 @@ def test_bf16_store_is_reproducible_and_keyed_by_global_slice(oracle_mod):
                          want_state=False)
     assert np.array_equal(mv(x.res), mv(y.res)) and np.array_equal(mv(x.labels), mv(y.labels))
     assert np.array_equal(mv(s.labels), mv(x.labels))
+
+
+# --------------------------------------------------------------------------- TV-L2 (ROF) denoising
+def test_tv_oracle_properties(oracle_mod):
+    """Constant fields are fixed points; the in-mask sum is preserved (div of a field whose
+    missing-neighbour terms are zero sums to zero); FP32 mode tracks FP64."""
+    m, u, _ = random_volume(16, 14, 15, 6.4, 3, seed=8)
+    mv = m.mask_values
+    c, dq = oracle_mod.tv(m, np.full(m.span, 0.37, np.float32), 0.1, 0.99 / 6, 20, "f64")
+    assert np.array_equal(mv(c), np.full_like(mv(c), 0.37)) and not np.any(dq)
+    a, dqa = oracle_mod.tv(m, u, 0.1, 0.99 / 6, 40, "f64")
+    b, _ = oracle_mod.tv(m, u, 0.1, 0.99 / 6, 40, "f32")
+    assert abs(mv(a).astype(np.float64).sum() - mv(u).astype(np.float64).sum()) <= 1e-4 * mv(u).size
+    assert np.linalg.norm(mv(a) - mv(b)) <= 1e-5 * np.linalg.norm(mv(a))
+    assert dqa[-1] < dqa[0]
+    # smoothing lowers the total variation along n
+    tv_in = np.abs(np.diff(mv(u), axis=-1)).sum()
+    tv_out = np.abs(np.diff(mv(a), axis=-1)).sum()
+    assert tv_out < tv_in
