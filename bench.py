@@ -788,9 +788,11 @@ def run_tv(args, dist_: Dist) -> None:
     ctx = potts.make_context(dev.index, stream=stream.cuda_stream)
     g = torch.empty_like(u)
 
+    variant = 0 if args.variant == "fused" else 1
+
     def step():
         g.copy_(u)
-        return potts.tv_denoise(ctx, m, g.data_ptr(), lam, tau, iters)
+        return potts.tv_denoise(ctx, m, g.data_ptr(), lam, tau, iters, variant=variant)
 
     for _ in range(args.warmup):
         step()
@@ -809,12 +811,15 @@ def run_tv(args, dist_: Dist) -> None:
     vox = m.data_size
     value = dist_.reduce(float(vox) * iters * args.steps, "sum") / t_max / 1e9
     launch_s = sum(s.loop_ms for s in stats) / 1000.0 / max(sum(s.loop_launches for s in stats), 1)
-    bpv = 48  # div: xi (3) in, v out; grad: v, g, xi (3) in, xi (3) out; FP32
-    achieved = bpv / 2 * vox / launch_s / 1e9
+    # fused: xi (3) and g in, xi (3) out; split: div reads xi (3), writes v; grad reads v, g, xi (3),
+    # writes xi (3) -- per launch the average of the two
+    bpv = 28 if variant == 0 else 48
+    achieved = (bpv if variant == 0 else bpv / 2) * vox / launch_s / 1e9
     peaks = measured_peaks()
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None,
-                "kernel": "potts::tv_div_kernel + tv_grad_kernel (average launch)", "bytes_per_voxel_iter": bpv,
+                "kernel": "potts::tv_fused_kernel" if variant == 0 else "potts::tv_div_kernel + tv_grad_kernel (average launch)",
+                "bytes_per_voxel_iter": bpv,
                 "avg_launch_ms": round(launch_s * 1000, 4),
                 "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)"}
     e2e = None
@@ -825,7 +830,7 @@ def run_tv(args, dist_: Dist) -> None:
 
         def e2e_step():
             g.copy_(hu, non_blocking=True)
-            potts.tv_denoise(ctx, m, g.data_ptr(), lam, tau, iters, stats=False)
+            potts.tv_denoise(ctx, m, g.data_ptr(), lam, tau, iters, variant=variant, stats=False)
             hout.copy_(g, non_blocking=True)
 
         e2e_step()
@@ -864,7 +869,7 @@ def run_tv(args, dist_: Dist) -> None:
             "warmup": args.warmup, "ms_per_step": round(1000 * t_max / args.steps, 2), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"tv_{m.rows}x{m.cols}x{m.n_images}_r370", "in_mask_voxels": vox,
-                       "lambda": lam, "tau": tau, "iters": iters,
+                       "lambda": lam, "tau": tau, "iters": iters, "variant": args.variant,
                        "parallelism": f"replica x{dist_.world}" if dist_.world > 1 else "single",
                        "l2": "inputs larger than L2"},
             "roofline": roofline, "e2e": e2e, "gpu_launches": sum(s.total_launches for s in stats), "clocks": clk,

@@ -291,12 +291,15 @@ void potts_stepper_destroy(potts_stepper *stepper);
 
 /* TV-L2 (ROF) denoising of a field in place: chambolle() of
  * totalvarmin/chambolle.cpp:220-276 (Chambolle's projection algorithm, xi and
- * v zero at the start, `iters` iterations of the div and grad kernels, then
+ * v zero at the start, `iters` iterations of the div and grad steps, then
  * g <- g - lambda div xi).  The reference's caller (totalvarmin.cpp:140) uses
- * tau = 0.99 / 6 and 150 iterations.  stats (optional): solve_ms, loop_ms,
- * launches, dq_trace / dq_last of the per-iteration max |dxi|^2. */
+ * tau = 0.99 / 6 and 150 iterations.  variant: POTTS_VARIANT_FUSED (one launch
+ * per iteration, v rebuilt on chip, xi ping-pong) or POTTS_VARIANT_PLAIN (the
+ * reference's div and grad launches); both give the same bits.  stats
+ * (optional): solve_ms, loop_ms, launches, dq_trace / dq_last of the
+ * per-iteration max |dxi|^2. */
 int potts_tv_denoise(potts_context *ctx, const potts_mapping *map, float *d_g, float lambda, float tau, int iters,
-                     potts_stats *stats);
+                     int variant, potts_stats *stats);
 
 /* Mask constructor of layout_cylinder::mapping_storage (include/layout_cylinder.h:152-195):
  * fills start_row[cols] and base[cols+1], returns the span (base[cols]). */

@@ -110,7 +110,7 @@ SIGNATURES = {
                                  ctypes.POINTER(ctypes.c_int64)]),
     "potts_stepper_finish": (_I, [_P, _P, _P, _P]),
     "potts_stepper_destroy": (None, [_P]),
-    "potts_tv_denoise": (_I, [_P, _MP, _P, _F, _F, _I, _SP]),
+    "potts_tv_denoise": (_I, [_P, _MP, _P, _F, _F, _I, _I, _SP]),
 }
 STATIC_MAX_COLS = 16384
 

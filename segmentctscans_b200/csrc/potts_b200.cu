@@ -934,8 +934,9 @@ int context_init(int device, void *stream, bool use_stream, potts_context **out)
 #include "stepper.cuh"
 
 // TV-L2 denoising (chambolle(), totalvarmin/chambolle.cpp:220-276) of d_g in
-// place; xi and v live in the context's state buffer, laid out like g.
-int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, potts_stats *stats)
+// place; xi (two halves of 3 planes for the fused form) and v live in the
+// context's state buffer, laid out like g.
+int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int variant, potts_stats *stats)
 {
     const MappingCopy &mc = ctx->mapping;
     Geometry g{};
@@ -947,24 +948,33 @@ int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, pott
     g.ns = (int)mc.m.n_images;
     g.slab_start = 0;
     cudaStream_t s = ctx->stream;
-    POTTS_TRY(ensure(ctx, ctx->state, sizeof(float) * 4 * (size_t)std::max<int64_t>(g.plane_w, 1)));
+    const size_t planes = variant == POTTS_VARIANT_PLAIN ? 4 : 6;
+    POTTS_TRY(ensure(ctx, ctx->state, sizeof(float) * planes * (size_t)std::max<int64_t>(g.plane_w, 1)));
     POTTS_TRY(ensure(ctx, ctx->dq, sizeof(float) * (size_t)std::max(iters, 1)));
     float *xi = static_cast<float *>(ctx->state.p), *v = xi + 3 * g.plane_w;
+    float *xi_b = xi + 3 * g.plane_w;  // fused form: the second half
     float *dq = static_cast<float *>(ctx->dq.p);
     ctx->seg_used = 0;
     ctx->seg_open = false;
     ctx->loop_launches = ctx->total_launches = 0;
     POTTS_CUDA(cudaEventRecord(ctx->ev0, s));
-    POTTS_CUDA(cudaMemsetAsync(ctx->state.p, 0, sizeof(float) * 4 * (size_t)std::max<int64_t>(g.plane_w, 1), s));
+    POTTS_CUDA(cudaMemsetAsync(ctx->state.p, 0, sizeof(float) * planes * (size_t)std::max<int64_t>(g.plane_w, 1), s));
     POTTS_CUDA(cudaMemsetAsync(dq, 0, sizeof(float) * (size_t)std::max(iters, 1), s));
     const unsigned nb = plain_blocks(g, 0, g.ns);
     if (g.n_lines > 0) {
         POTTS_TRY(seg_begin(ctx));
         for (int it = 0; it < iters; ++it) {
-            potts::tv_div_kernel<<<nb, potts::kPlainThreads, 0, s>>>(g, xi, v);
-            potts::tv_grad_kernel<<<nb, potts::kPlainThreads, 0, s>>>(g, d_g, xi, v, lam, tau, dq + it);
-            ctx->loop_launches += 2;
-            ctx->total_launches += 2;
+            if (variant == POTTS_VARIANT_PLAIN) {
+                potts::tv_div_kernel<<<nb, potts::kPlainThreads, 0, s>>>(g, xi, v);
+                potts::tv_grad_kernel<<<nb, potts::kPlainThreads, 0, s>>>(g, d_g, xi, v, lam, tau, dq + it);
+                ctx->loop_launches += 2;
+                ctx->total_launches += 2;
+            } else {
+                potts::tv_fused_kernel<<<nb, potts::kPlainThreads, 0, s>>>(g, d_g, xi, xi_b, lam, tau, dq + it);
+                std::swap(xi, xi_b);
+                ctx->loop_launches += 1;
+                ctx->total_launches += 1;
+            }
         }
         POTTS_TRY(seg_end(ctx));
         potts::tv_update_kernel<<<nb, potts::kPlainThreads, 0, s>>>(g, d_g, xi, lam);
@@ -983,7 +993,7 @@ int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, pott
         POTTS_TRY(seg_total_ms(ctx, &stats->loop_ms));
         stats->loop_launches = ctx->loop_launches;
         stats->total_launches = ctx->total_launches;
-        stats->state_bytes = sizeof(float) * 4 * (uint64_t)std::max<int64_t>(g.plane_w, 1);
+        stats->state_bytes = sizeof(float) * planes * (uint64_t)std::max<int64_t>(g.plane_w, 1);
         stats->dq_last = 0.0f;
         if (iters > 0) {
             std::vector<float> tr((size_t)iters);
@@ -1507,16 +1517,17 @@ int potts_stepper_finish(potts_stepper *s, float *d_res, uint8_t *d_labels, floa
 void potts_stepper_destroy(potts_stepper *s) { stepper_free(s); }
 
 int potts_tv_denoise(potts_context *ctx, const potts_mapping *map, float *d_g, float lambda, float tau, int iters,
-                     potts_stats *stats)
+                     int variant, potts_stats *stats)
 {
     if (!ctx) return fail(POTTS_EINVAL, "context is NULL");
     if (!d_g) return fail(POTTS_EINVAL, "g is NULL");
     if (!std::isfinite(lambda) || lambda == 0.0f || !std::isfinite(tau))
         return fail(POTTS_EINVAL, "lambda must be finite and non-zero, tau finite");
     if (iters < 0) return fail(POTTS_EINVAL, "iters must be >= 0");
+    if (variant != POTTS_VARIANT_FUSED && variant != POTTS_VARIANT_PLAIN) return fail(POTTS_EINVAL, "unknown variant");
     POTTS_CUDA(cudaSetDevice(ctx->device));
     POTTS_TRY(upload_lines(ctx, map));
-    return tv_run(ctx, d_g, lambda, tau, iters, stats);
+    return tv_run(ctx, d_g, lambda, tau, iters, variant, stats);
 }
 
 }  // extern "C"

@@ -437,24 +437,24 @@ def loss_and_grad(mapping: CylinderMapping, u: np.ndarray, truth: np.ndarray, ci
 
 # --------------------------------------------------------------------------- TV-L2 denoising
 def tv_denoise(ctx: CudaContext, mapping: CylinderMapping, g_ptr: int, lam: float, tau: float, iters: int, *,
-               stats: bool = True) -> Optional[SolveStats]:
+               variant: int = 0, stats: bool = True) -> Optional[SolveStats]:
     """chambolle() (totalvarmin/chambolle.cpp:220-276): TV-L2 denoising of the device field at g_ptr
-    (the mapping's span, float32) in place."""
+    (the mapping's span, float32) in place; variant 0 = fused, 1 = the reference's two launches."""
     st, dq, en = _make_stats(iters, 0, stats)
     check(_native.host_lib().potts_tv_denoise(ctx.handle, ctypes.byref(mapping.as_c()), ctypes.c_void_p(int(g_ptr)),
-                                              float(lam), float(tau), int(iters),
+                                              float(lam), float(tau), int(iters), int(variant),
                                               ctypes.byref(st) if stats else None))
     return _stats_out(st, dq, en) if stats else None
 
 
 def tv_denoise_host(mapping: CylinderMapping, g: np.ndarray, lam: float, tau: float, iters: int, *,
-                    ctx: Optional[CudaContext] = None) -> tuple[np.ndarray, SolveStats]:
+                    variant: int = 0, ctx: Optional[CudaContext] = None) -> tuple[np.ndarray, SolveStats]:
     """TV-L2 denoising of a host field (float32, the mapping's span); returns (result, stats)."""
     own = ctx is None
     ctx = ctx or make_context(0)
     try:
         fld = upload(ctx, mapping, np.ascontiguousarray(g, np.float32))
-        st = tv_denoise(ctx, mapping, fld.data_ptr(), lam, tau, iters)
+        st = tv_denoise(ctx, mapping, fld.data_ptr(), lam, tau, iters, variant=variant)
         out = download(ctx, fld)
         fld.free()
         return out, st

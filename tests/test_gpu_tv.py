@@ -20,16 +20,17 @@ TAU_TV = 0.99 / 6.0  # totalvarmin/totalvarmin.cpp:140
     (5, 3, 40, 1.2, 12),      # columns of one row
     (12, 10, 10, 4.3, 0),     # zero iterations
 ])
-def test_tv_bitwise_equal_to_fp32_oracle(cuda_device, oracle_mod, geom):
+@pytest.mark.parametrize("variant", [0, 1], ids=["fused", "plain"])
+def test_tv_bitwise_equal_to_fp32_oracle(cuda_device, oracle_mod, geom, variant):
     n, rows, cols, r, iters = geom
     m, u, _ = random_volume(n, rows, cols, r, 3, seed=n + cols)
-    out, st = potts.tv_denoise_host(m, u, 0.1, TAU_TV, iters)
+    out, st = potts.tv_denoise_host(m, u, 0.1, TAU_TV, iters, variant=variant)
     ref, dq = oracle_mod.tv(m, u, 0.1, TAU_TV, iters, "f32")
     mv = m.mask_values
     assert np.array_equal(mv(out), mv(ref))
     if iters:
         np.testing.assert_array_equal(st.dq_trace, dq)
-        assert st.loop_launches == 2 * iters
+        assert st.loop_launches == (2 if variant else 1) * iters
 
 
 def test_tv_against_fp64_oracle_on_phantom(cuda_device, oracle_mod):
