@@ -73,7 +73,7 @@ def parse_args():
                    help="state storage of the timed solves")
     p.add_argument("--no-storage-compare", action="store_true",
                    help="skip the FP32-plain / BF16 / FP16 comparison solves")
-    p.add_argument("--workload", choices=["config1", "config2", "config3", "config4", "config0", "mid", "mid4", "tv"],
+    p.add_argument("--workload", choices=["config1", "config2", "config3", "config4", "config0", "mid", "mid4", "tv", "tvmid"],
                    default="config1",
                    help="config1: 768x768x1024 r=370 (the benchmark); config0: 128^3 r=60; "
                         "mid: 384x384x256 r=180 (profiling size, state > L2)")
@@ -782,7 +782,12 @@ def run_tv(args, dist_: Dist) -> None:
     dist_.init("nccl")
     iters = 150 if args.iters == 1000 else args.iters
     lam, tau = 0.06, 0.99 / 6.0
-    ph = config1_phantom(seed=dist_.rank, device=dev)
+    if args.workload == "tvmid":  # the profiling-size volume
+        from segmentctscans_b200.phantom import make_phantom
+
+        ph = make_phantom(256, 384, 384, 180.0, seed=dist_.rank, radius_range=(6.0, 30.0), noise=7e-3, device=dev)
+    else:
+        ph = config1_phantom(seed=dist_.rank, device=dev)
     m, u = ph.mapping, ph.u
     stream = torch.cuda.current_stream(dev)
     ctx = potts.make_context(dev.index, stream=stream.cuda_stream)
@@ -868,7 +873,7 @@ def run_tv(args, dist_: Dist) -> None:
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist_.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1000 * t_max / args.steps, 2), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"tv_{m.rows}x{m.cols}x{m.n_images}_r370", "in_mask_voxels": vox,
+            "config": {"workload": f"tv_{m.rows}x{m.cols}x{m.n_images}", "in_mask_voxels": vox,
                        "lambda": lam, "tau": tau, "iters": iters, "variant": args.variant,
                        "parallelism": f"replica x{dist_.world}" if dist_.world > 1 else "single",
                        "l2": "inputs larger than L2"},
@@ -892,7 +897,7 @@ def main():
     if args.workload == "config4":
         run_adjoint(args, d)
         return
-    if args.workload == "tv":
+    if args.workload in ("tv", "tvmid"):
         run_tv(args, d)
         return
     run_ours(args, d)

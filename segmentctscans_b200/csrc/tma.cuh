@@ -91,11 +91,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return false;
 }
 
-__device__ __forceinline__ void mbar_inval(uint64_t *bar)
-{
-    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
-}
-
 // Single-thread form (for the producer lane).
 __device__ __forceinline__ bool mbar_wait_thread(uint64_t *bar, uint32_t parity, volatile int *abort)
 {
