@@ -68,7 +68,8 @@ def parse_args():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--iters", type=int, default=1000)
     p.add_argument("--gap-every", type=int, default=50)
-    p.add_argument("--variant", choices=["fused", "plain"], default="fused")
+    p.add_argument("--variant", choices=["fused", "plain", "voxel"], default="fused",
+                   help="voxel: TV workloads only, the per-voxel fused TV kernel")
     p.add_argument("--storage", choices=["f32", "bf16", "f16"], default="f32",
                    help="state storage of the timed solves")
     p.add_argument("--no-storage-compare", action="store_true",
@@ -88,7 +89,10 @@ def parse_args():
     p.add_argument("--tile-vpt", type=int, default=0, help="fused slices per thread (0 = library default)")
     p.add_argument("--prefetch", type=int, default=0,
                    help="fused: planes of L2 prefetch ahead of the load ring (0 = library default, -1 = none)")
-    return p.parse_args()
+    args = p.parse_args()
+    if args.variant == "voxel" and args.workload not in ("tv", "tvmid"):
+        p.error("--variant voxel applies to the TV workloads only")
+    return args
 
 
 def tau_baseline() -> float:
@@ -793,7 +797,7 @@ def run_tv(args, dist_: Dist) -> None:
     ctx = potts.make_context(dev.index, stream=stream.cuda_stream)
     g = torch.empty_like(u)
 
-    variant = 0 if args.variant == "fused" else 1
+    variant = {"fused": 0, "plain": 1, "voxel": 2}[args.variant]
 
     def step():
         g.copy_(u)
@@ -818,12 +822,13 @@ def run_tv(args, dist_: Dist) -> None:
     launch_s = sum(s.loop_ms for s in stats) / 1000.0 / max(sum(s.loop_launches for s in stats), 1)
     # fused: xi (3) and g in, xi (3) out; split: div reads xi (3), writes v; grad reads v, g, xi (3),
     # writes xi (3) -- per launch the average of the two
-    bpv = 28 if variant == 0 else 48
-    achieved = (bpv if variant == 0 else bpv / 2) * vox / launch_s / 1e9
+    bpv = 48 if variant == 1 else 28
+    achieved = (bpv / 2 if variant == 1 else bpv) * vox / launch_s / 1e9
     peaks = measured_peaks()
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None,
-                "kernel": "potts::tv_fused_kernel" if variant == 0 else "potts::tv_div_kernel + tv_grad_kernel (average launch)",
+                "kernel": {0: "potts::tv_tiled_kernel<8,128>", 1: "potts::tv_div_kernel + tv_grad_kernel (average launch)",
+                           2: "potts::tv_fused_kernel"}[variant],
                 "bytes_per_voxel_iter": bpv,
                 "avg_launch_ms": round(launch_s * 1000, 4),
                 "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)"}

@@ -294,8 +294,10 @@ void potts_stepper_destroy(potts_stepper *stepper);
  * v zero at the start, `iters` iterations of the div and grad steps, then
  * g <- g - lambda div xi).  The reference's caller (totalvarmin.cpp:140) uses
  * tau = 0.99 / 6 and 150 iterations.  variant: POTTS_VARIANT_FUSED (one launch
- * per iteration, v rebuilt on chip, xi ping-pong) or POTTS_VARIANT_PLAIN (the
- * reference's div and grad launches); both give the same bits.  stats
+ * per iteration over 8 x 128 tiles marching along the columns, xi and v staged
+ * in shared memory, xi ping-pong), POTTS_VARIANT_PLAIN (the reference's div and
+ * grad launches) or 2 (one launch per iteration, v rebuilt per voxel from
+ * global memory); all give the same bits.  stats
  * (optional): solve_ms, loop_ms, launches, dq_trace / dq_last of the
  * per-iteration max |dxi|^2. */
 int potts_tv_denoise(potts_context *ctx, const potts_mapping *map, float *d_g, float lambda, float tau, int iters,

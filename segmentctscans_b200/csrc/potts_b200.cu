@@ -936,6 +936,28 @@ int context_init(int device, void *stream, bool use_stream, potts_context **out)
 // TV-L2 denoising (chambolle(), totalvarmin/chambolle.cpp:220-276) of d_g in
 // place; xi (two halves of 3 planes for the fused form) and v live in the
 // context's state buffer, laid out like g.
+// Work items and shared-memory size of the tiled TV kernel for TR x TN tiles.
+template <int TR, int TN>
+int tv_tiled_setup(potts_context *ctx, int ns)
+{
+    POTTS_TRY(plan_tiles(ctx, ns, TileChoice{TR, TN, 1, 64}));
+    POTTS_CUDA(cudaFuncSetAttribute(potts::tv_tiled_kernel<TR, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(sizeof(float) * potts::TvTile<TR, TN>::SMEM_FLOATS)));
+    return POTTS_OK;
+}
+
+template <int TR, int TN>
+void tv_tiled_launch(potts_context *ctx, const Geometry &g, const float *d_g, const float *xi, float *xi_out,
+                     float lam, float tau, float *dq)
+{
+    if (ctx->n_work == 0) return;
+    const MappingCopy &mc = ctx->mapping;
+    potts::tv_tiled_kernel<TR, TN><<<ctx->n_work, potts::kTvThreads,
+                                     sizeof(float) * potts::TvTile<TR, TN>::SMEM_FLOATS, ctx->stream>>>(
+        g, static_cast<const int4 *>(ctx->cols.p), (int)mc.m.col_begin, (int)mc.m.col_end,
+        static_cast<const int4 *>(ctx->work.p), d_g, xi, xi_out, lam, tau, dq);
+}
+
 int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int variant, potts_stats *stats)
 {
     const MappingCopy &mc = ctx->mapping;
@@ -948,7 +970,7 @@ int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int 
     g.ns = (int)mc.m.n_images;
     g.slab_start = 0;
     cudaStream_t s = ctx->stream;
-    const size_t planes = variant == POTTS_VARIANT_PLAIN ? 4 : 6;
+    const size_t planes = variant == POTTS_VARIANT_PLAIN ? 4 : 6;  // fused forms: xi ping-pong
     POTTS_TRY(ensure(ctx, ctx->state, sizeof(float) * planes * (size_t)std::max<int64_t>(g.plane_w, 1)));
     POTTS_TRY(ensure(ctx, ctx->dq, sizeof(float) * (size_t)std::max(iters, 1)));
     float *xi = static_cast<float *>(ctx->state.p), *v = xi + 3 * g.plane_w;
@@ -961,10 +983,22 @@ int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int 
     POTTS_CUDA(cudaMemsetAsync(ctx->state.p, 0, sizeof(float) * planes * (size_t)std::max<int64_t>(g.plane_w, 1), s));
     POTTS_CUDA(cudaMemsetAsync(dq, 0, sizeof(float) * (size_t)std::max(iters, 1), s));
     const unsigned nb = plain_blocks(g, 0, g.ns);
+    // tiled form: the Potts kernel's column table and work items for 8 x 128 tiles
+    constexpr int kTvRows = 8, kTvSlices = 128;
+    // the tiled kernel copies 16-byte words of rows: g and every line must start on one, else the
+    // per-voxel fused kernel runs
+    const bool words = mc.m.nstride % 4 == 0 && reinterpret_cast<uintptr_t>(d_g) % 16 == 0;
+    const bool tiled = words && variant == POTTS_VARIANT_FUSED;
+    if (tiled && g.n_lines > 0 && iters > 0) POTTS_TRY((tv_tiled_setup<kTvRows, kTvSlices>(ctx, g.ns)));
     if (g.n_lines > 0) {
         POTTS_TRY(seg_begin(ctx));
         for (int it = 0; it < iters; ++it) {
-            if (variant == POTTS_VARIANT_PLAIN) {
+            if (tiled) {
+                tv_tiled_launch<kTvRows, kTvSlices>(ctx, g, d_g, xi, xi_b, lam, tau, dq + it);
+                std::swap(xi, xi_b);
+                ctx->loop_launches += 1;
+                ctx->total_launches += 1;
+            } else if (variant == POTTS_VARIANT_PLAIN) {
                 potts::tv_div_kernel<<<nb, potts::kPlainThreads, 0, s>>>(g, xi, v);
                 potts::tv_grad_kernel<<<nb, potts::kPlainThreads, 0, s>>>(g, d_g, xi, v, lam, tau, dq + it);
                 ctx->loop_launches += 2;
@@ -1524,7 +1558,7 @@ int potts_tv_denoise(potts_context *ctx, const potts_mapping *map, float *d_g, f
     if (!std::isfinite(lambda) || lambda == 0.0f || !std::isfinite(tau))
         return fail(POTTS_EINVAL, "lambda must be finite and non-zero, tau finite");
     if (iters < 0) return fail(POTTS_EINVAL, "iters must be >= 0");
-    if (variant != POTTS_VARIANT_FUSED && variant != POTTS_VARIANT_PLAIN) return fail(POTTS_EINVAL, "unknown variant");
+    if (variant < 0 || variant > 2) return fail(POTTS_EINVAL, "unknown variant");
     POTTS_CUDA(cudaSetDevice(ctx->device));
     POTTS_TRY(upload_lines(ctx, map));
     return tv_run(ctx, d_g, lambda, tau, iters, variant, stats);
