@@ -191,157 +191,199 @@ __device__ __forceinline__ void tv_cp_commit() { asm volatile("cp.async.commit_g
 // wait until at most one group (the newest) of this thread's copies is in flight
 __device__ __forceinline__ void tv_cp_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
-// Issue the copies of one column plane (table entry ci) into the xi box sx and the g box sg.
-// Global rows start on 16-byte words: the line stride is a multiple of 32 floats, the planes
-// are multiples of it and the base pointers are 16-byte aligned (checked by the host).
-template <int TR, int TN>
-__device__ __forceinline__ void tv_issue_plane(const Geometry &g, int4 ci, int r0, int n0,
-                                               const float *__restrict__ xi_in, const float *__restrict__ gin,
-                                               float *sx, float *sg)
-{
-    using T = TvTile<TR, TN>;
-    constexpr int CH = TN / 4;      // 16-byte chunks per row
-    constexpr int XO = CH + 2;      // xi row: chunks, then slice n0-1, then slice n0+TN
-    constexpr int GO = CH + 1;      // g row: chunks, then slice n0+TN
-    for (int i = threadIdx.x; i < 3 * T::XR * XO; i += blockDim.x) {
-        const int line = i / XO, k = i % XO;  // line = comp * XR + rr
-        const int comp = line / T::XR, rr = line % T::XR;
-        const int row = r0 - 1 + rr;
-        const bool rin = tv_row_in(ci, row);
-        const int64_t gl = comp * g.plane_w + (int64_t)(ci.x + row - ci.y) * g.nstride_w;
-        float *dst = sx + comp * T::XC + rr * T::XS;
-        if (k < CH) {
-            const int n = n0 + 4 * k;
-            const int bytes = rin ? 4 * max(0, min(4, g.ns - n)) : 0;
-            tv_cp_async16(dst + 4 + 4 * k, bytes ? xi_in + gl + n : xi_in, bytes);
-        } else {
-            const int n = k == CH ? n0 - 1 : n0 + TN;
-            const bool in = rin && n >= 0 && n < g.ns;
-            tv_cp_async4(dst + (k == CH ? 3 : TN + 4), in ? xi_in + gl + n : xi_in, in);
-        }
-    }
-    for (int i = threadIdx.x; i < T::VR * GO; i += blockDim.x) {
-        const int rr = i / GO, k = i % GO;
-        const int row = r0 + rr;
-        const bool rin = tv_row_in(ci, row);
-        const int64_t gl = (int64_t)(ci.x + row - ci.y) * g.nstride_w;
-        float *dst = sg + rr * T::GS;
-        if (k < CH) {
-            const int n = n0 + 4 * k;
-            const int bytes = rin ? 4 * max(0, min(4, g.ns - n)) : 0;
-            tv_cp_async16(dst + 4 * k, bytes ? gin + gl + n : gin, bytes);
-        } else {
-            const int n = n0 + TN;
-            const bool in = rin && n < g.ns;
-            tv_cp_async4(dst + TN, in ? gin + gl + n : gin, in);
-        }
-    }
-}
-
-// v = div xi at (plane with table entry ci, its xi box sx; the previous plane's xi box sxp and
-// entry cp) for the v box (rows r0 .. r0+TR, slices n0 .. n0+TN).
-template <int TR, int TN>
-__device__ __forceinline__ void tv_plane_div(const Geometry &g, int4 ci, int4 cp, int4 cn, int r0, int n0,
-                                             const float *sx, const float *sxp, float *sv)
-{
-    using T = TvTile<TR, TN>;
-    constexpr int VN = TN + 1;
-    const float *s0 = sx, *s1 = sx + T::XC, *s2p = sxp + 2 * T::XC, *s2 = sx + 2 * T::XC;
-    for (int i = threadIdx.x; i < T::VR * VN; i += blockDim.x) {
-        const int rr = i / VN, nn = i % VN;
-        const int row = r0 + rr, n = n0 + nn;
-        float d = 0.0f;
-        if (tv_row_in(ci, row) && n < g.ns) {
-            const int b = (rr + 1) * T::XS + (nn + 4);  // (row, n) in the xi box
-            if (n > 0) d -= s0[b - 1];
-            if (n + 1 < g.ns) d += s0[b];
-            if (row > ci.y) d -= s1[b - T::XS];
-            if (row + 1 < ci.z) d += s1[b];
-            if (tv_row_in(cp, row)) d -= s2p[b];
-            if (tv_row_in(cn, row)) d += s2[b];
-        }
-        sv[rr * T::GS + nn] = d;
-    }
-}
-
 }  // namespace potts
 
 namespace potts {
 
 constexpr int kTvThreads = 256;
 
+// Thread assignments (8 x 128 tiles, 256 threads; fixed for the whole column march, so
+// that index arithmetic is done once per block):
+//  - update: thread t owns slice nn = t % 128 and rows 4h .. 4h+3 (h = t / 128), walking
+//    down the rows with the v and g values of the row below kept in registers;
+//  - divergence: the same slice, v rows 5h .. 5h+4 (of nine), xi_1 of the row above kept in
+//    registers; thread t < 9 also computes v at slice n0+128 of row t;
+//  - copies: 16-byte chunk t % 32 of the xi box lines t/32 + 8j (j < 4; 30 lines =
+//    3 components x 10 rows) and of the g box lines t/32 + 8j (j < 2; 9 rows); thread t < 60
+//    copies the halo slice of xi line t/2 (n0-1 for even t, n0+128 for odd t), threads
+//    64 .. 72 the slice n0+128 of g row t-64.
 template <int TR, int TN>
-__global__ void __launch_bounds__(kTvThreads)
+__global__ void __launch_bounds__(kTvThreads, 3)
     tv_tiled_kernel(Geometry g, const int4 *__restrict__ cols, int col_begin, int col_end,
                     const int4 *__restrict__ work, const float *__restrict__ gin, const float *__restrict__ xi_in,
                     float *__restrict__ xi_out, float lam, float tau, float *dq)
 {
+    static_assert(TR == 8 && TN == 128 && kTvThreads == 256, "thread assignments are for 8 x 128 tiles");
     using T = TvTile<TR, TN>;
     extern __shared__ __align__(16) float tv_smem[];
-    // ring slots (0..2 for xi and g, 0..1 for v), selected arithmetically to stay in registers
     auto sx = [&](int sl) { return tv_smem + sl * T::XI_PLANE; };
     auto sg = [&](int sl) { return tv_smem + 3 * T::XI_PLANE + sl * T::V_PLANE; };
     auto sv = [&](int sl) { return tv_smem + 3 * T::XI_PLANE + (3 + sl) * T::V_PLANE; };
+    const int t = threadIdx.x;
     const int4 wk = work[blockIdx.x];
     const int r0 = wk.x, n0 = wk.y, ca = wk.z, cb = wk.w;
+    const int64_t nsw = g.nstride_w;
     auto col_at = [&](int c) { return (c >= col_begin && c < col_end) ? cols[c] : make_int4(0, 0, 0, 0); };
 
+    // ---- copy assignments
+    const int ck = t & 31, cl = t >> 5;
+    const int cbytes = 4 * max(0, min(4, g.ns - (n0 + 4 * ck)));
+    int64_t xoff[4];
+    int xdst[4], xrow[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int line = cl + 8 * j, comp = line / 10, rr = line % 10;
+        xrow[j] = line < 30 ? r0 - 1 + rr : INT32_MIN;  // INT32_MIN: no line, never in a column
+        xoff[j] = comp * g.plane_w + (int64_t)(r0 - 1 + rr) * nsw + n0 + 4 * ck;
+        xdst[j] = comp * T::XC + rr * T::XS + 4 + 4 * ck;
+    }
+    const int grow1 = cl == 0 ? r0 + 8 : INT32_MIN;  // the ninth g row, copied by warp 0
+    // halo slices: kind 1 = xi, 2 = g
+    int s_kind = 0, s_row = INT32_MIN, s_dst = 0;
+    int64_t s_off = 0;
+    if (t < 60) {
+        const int line = t >> 1, comp = line / 10, rr = line % 10, n = (t & 1) ? n0 + TN : n0 - 1;
+        s_kind = 1;
+        s_row = (n >= 0 && n < g.ns) ? r0 - 1 + rr : INT32_MIN;
+        s_off = comp * g.plane_w + (int64_t)(r0 - 1 + rr) * nsw + n;
+        s_dst = comp * T::XC + rr * T::XS + ((t & 1) ? TN + 4 : 3);
+    } else if (t >= 64 && t < 64 + T::VR) {
+        const int rr = t - 64, n = n0 + TN;
+        s_kind = 2;
+        s_row = n < g.ns ? r0 + rr : INT32_MIN;
+        s_off = (int64_t)(r0 + rr) * nsw + n;
+        s_dst = rr * T::GS + TN;
+    }
+    auto issue = [&](int c, int slot) {
+        const int4 ci = col_at(c);
+        const int64_t shift = (int64_t)(ci.x - ci.y) * nsw;  // line of row r: ci.x + r - ci.y
+        float *X = sx(slot), *G = sg(slot);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (xrow[j] == INT32_MIN) continue;
+            const int b = tv_row_in(ci, xrow[j]) ? cbytes : 0;
+            tv_cp_async16(X + xdst[j], b ? xi_in + xoff[j] + shift : xi_in, b);
+        }
+        {
+            const int b = tv_row_in(ci, r0 + cl) ? cbytes : 0;
+            tv_cp_async16(G + cl * T::GS + 4 * ck, b ? gin + (int64_t)(r0 + cl) * nsw + n0 + 4 * ck + shift : gin, b);
+        }
+        if (grow1 != INT32_MIN) {
+            const int b = tv_row_in(ci, grow1) ? cbytes : 0;
+            tv_cp_async16(G + 8 * T::GS + 4 * ck, b ? gin + (int64_t)grow1 * nsw + n0 + 4 * ck + shift : gin, b);
+        }
+        if (s_kind) {
+            const bool in = tv_row_in(ci, s_row);
+            const float *src = s_kind == 1 ? xi_in : gin;
+            tv_cp_async4((s_kind == 1 ? X : G) + s_dst, in ? src + s_off + shift : src, in);
+        }
+    };
+
+    // ---- divergence and update assignments
+    const int nn = t & (TN - 1), h = t >> 7;
+    const int n = n0 + nn;
+    const bool nin = n < g.ns, nbk = n > 0, nfw = n + 1 < g.ns;
+    // v = div xi of the plane with entry ci (xi box X), previous plane cp (xi box Xp), next cn
+    auto divergence = [&](int4 ci, int4 cp, int4 cn, const float *X, const float *Xp, float *V) {
+        const float *s0 = X, *s1 = X + T::XC, *s2 = X + 2 * T::XC, *s2p = Xp + 2 * T::XC;
+        float up = s1[(5 * h) * T::XS + nn + 4];  // xi_1 of the row above the first
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+            const int rr = 5 * h + m;
+            if (rr >= T::VR) break;
+            const int row = r0 + rr, b = (rr + 1) * T::XS + nn + 4;
+            const float a0m = s0[b - 1], a0 = s0[b], a1 = s1[b], a2p = s2p[b], a2 = s2[b];
+            float d = 0.0f;
+            if (tv_row_in(ci, row) && nin) {
+                if (nbk) d -= a0m;
+                if (nfw) d += a0;
+                if (row > ci.y) d -= up;
+                if (row + 1 < ci.z) d += a1;
+                if (tv_row_in(cp, row)) d -= a2p;
+                if (tv_row_in(cn, row)) d += a2;
+            }
+            V[rr * T::GS + nn] = d;
+            up = a1;
+        }
+        if (t < T::VR) {  // slice n0+TN of row t
+            const int rr = t, row = r0 + rr, ne = n0 + TN, b = (rr + 1) * T::XS + TN + 4;
+            float d = 0.0f;
+            if (tv_row_in(ci, row) && ne < g.ns) {
+                d -= s0[b - 1];
+                if (ne + 1 < g.ns) d += s0[b];
+                if (row > ci.y) d -= s1[b - T::XS];
+                if (row + 1 < ci.z) d += s1[b];
+                if (tv_row_in(cp, row)) d -= s2p[b];
+                if (tv_row_in(cn, row)) d += s2[b];
+            }
+            V[rr * T::GS + TN] = d;
+        }
+    };
+
     // planes ca-1, ca, ca+1 into slots 0, 1, 2 (plane c sits in slot (c - ca + 1) mod 3)
+#pragma unroll 1
     for (int k = 0; k < 3; ++k) {
-        if (ca - 1 + k <= cb) tv_issue_plane<TR, TN>(g, col_at(ca - 1 + k), r0, n0, xi_in, gin, sx(k), sg(k));
+        if (ca - 1 + k <= cb) issue(ca - 1 + k, k);
         tv_cp_commit();
     }
     tv_cp_wait_one();  // planes ca-1 and ca have landed (this thread's copies)
     __syncthreads();   // ... and every thread's
-    tv_plane_div<TR, TN>(g, col_at(ca), col_at(ca - 1), col_at(ca + 1), r0, n0, sx(1), sx(0), sv(0));
+    divergence(col_at(ca), col_at(ca - 1), col_at(ca + 1), sx(1), sx(0), sv(0));
     __syncthreads();
     float dmax = 0.0f;
     int sp = 0, sc = 1, sn = 2;  // slots of planes c-1, c, c+1
     int vc = 0;                  // v slot of plane c
+    const int64_t rowoff = (int64_t)(r0 + 4 * h) * nsw + n;
+#pragma unroll 1
     for (int c = ca; c < cb; ++c) {
         // plane c+2 into the slot of plane c-1, free since the last barrier
-        if (c + 2 <= cb) tv_issue_plane<TR, TN>(g, col_at(c + 2), r0, n0, xi_in, gin, sx(sp), sg(sp));
+        if (c + 2 <= cb) issue(c + 2, sp);
         tv_cp_commit();
         tv_cp_wait_one();  // plane c+1 has landed
         __syncthreads();
         const int4 ci = col_at(c), cn = col_at(c + 1);
-        tv_plane_div<TR, TN>(g, cn, ci, col_at(c + 2), r0, n0, sx(sn), sx(sc), sv(vc ^ 1));
+        divergence(cn, ci, col_at(c + 2), sx(sn), sx(sc), sv(vc ^ 1));
         __syncthreads();
-        const float *v0p = sv(vc), *v1p = sv(vc ^ 1), *g0p = sg(sc), *g1p = sg(sn);
+        const float *Vc = sv(vc), *Vn = sv(vc ^ 1), *Gc = sg(sc), *Gn = sg(sn);
         const float *x0 = sx(sc), *x1 = x0 + T::XC, *x2 = x0 + 2 * T::XC;
-        for (int i = threadIdx.x; i < TR * TN; i += blockDim.x) {
-            const int rr = i / TN, nn = i % TN;
-            const int row = r0 + rr, n = n0 + nn;
-            if (!tv_row_in(ci, row) || n >= g.ns) continue;
-            const int a = rr * T::GS + nn;                  // (row, n) in the v and g boxes
-            const int b = (rr + 1) * T::XS + (nn + 4);      // (row, n) in the xi box
-            const float v0 = v0p[a], gg = g0p[a];
-            float g1 = 0.0f, g2 = 0.0f, g3 = 0.0f;
-            if (n + 1 < g.ns) g1 = (v0p[a + 1] - v0) - __fdiv_rn(g0p[a + 1] - gg, lam);
-            if (row + 1 < ci.z) g2 = (v0p[a + T::GS] - v0) - __fdiv_rn(g0p[a + T::GS] - gg, lam);
-            if (tv_row_in(cn, row)) g3 = (v1p[a] - v0) - __fdiv_rn(g1p[a] - gg, lam);
-            float s = g1 * g1;
-            s = fmaf(g2, g2, s);
-            s = fmaf(g3, g3, s);
-            const float denom = fmaf(tau, __fsqrt_rn(s), 1.0f);
-            const float q1 = __fdiv_rn(fmaf(tau, g1, x0[b]), denom);
-            const float q2 = __fdiv_rn(fmaf(tau, g2, x1[b]), denom);
-            const float q3 = __fdiv_rn(fmaf(tau, g3, x2[b]), denom);
-            const float e1 = x0[b] - q1, e2 = x1[b] - q2, e3 = x2[b] - q3;
-            float d = e1 * e1;
-            d = fmaf(e2, e2, d);
-            d = fmaf(e3, e3, d);
-            dmax = fmaxf(dmax, d);
-            const int64_t o = (int64_t)(ci.x + row - ci.y) * g.nstride_w + n;
-            xi_out[o] = q1;
-            xi_out[g.plane_w + o] = q2;
-            xi_out[2 * g.plane_w + o] = q3;
+        const int64_t o0 = (int64_t)(ci.x - ci.y) * nsw + rowoff;
+        float v0 = Vc[(4 * h) * T::GS + nn], gg = Gc[(4 * h) * T::GS + nn];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const int rr = 4 * h + m, row = r0 + rr;
+            const int a = rr * T::GS + nn, b = (rr + 1) * T::XS + nn + 4;
+            const float vr = Vc[a + 1], gr = Gc[a + 1], vd = Vc[a + T::GS], gd = Gc[a + T::GS];
+            if (tv_row_in(ci, row) && nin) {
+                float g1 = 0.0f, g2 = 0.0f, g3 = 0.0f;
+                if (nfw) g1 = (vr - v0) - __fdiv_rn(gr - gg, lam);
+                if (row + 1 < ci.z) g2 = (vd - v0) - __fdiv_rn(gd - gg, lam);
+                if (tv_row_in(cn, row)) g3 = (Vn[a] - v0) - __fdiv_rn(Gn[a] - gg, lam);
+                float s = g1 * g1;
+                s = fmaf(g2, g2, s);
+                s = fmaf(g3, g3, s);
+                const float denom = fmaf(tau, __fsqrt_rn(s), 1.0f);
+                const float xa = x0[b], xb = x1[b], xc = x2[b];
+                const float q1 = __fdiv_rn(fmaf(tau, g1, xa), denom);
+                const float q2 = __fdiv_rn(fmaf(tau, g2, xb), denom);
+                const float q3 = __fdiv_rn(fmaf(tau, g3, xc), denom);
+                const float e1 = xa - q1, e2 = xb - q2, e3 = xc - q3;
+                float d = e1 * e1;
+                d = fmaf(e2, e2, d);
+                d = fmaf(e3, e3, d);
+                dmax = fmaxf(dmax, d);
+                const int64_t o = o0 + m * nsw;
+                xi_out[o] = q1;
+                xi_out[g.plane_w + o] = q2;
+                xi_out[2 * g.plane_w + o] = q3;
+            }
+            v0 = vd;
+            gg = gd;
         }
         __syncthreads();
-        const int t = sp;
+        const int tmp = sp;
         sp = sc;
         sc = sn;
-        sn = t;
+        sn = tmp;
         vc ^= 1;
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");  // nothing may be in flight at exit
