@@ -820,9 +820,10 @@ def run_tv(args, dist_: Dist) -> None:
     vox = m.data_size
     value = dist_.reduce(float(vox) * iters * args.steps, "sum") / t_max / 1e9
     launch_s = sum(s.loop_ms for s in stats) / 1000.0 / max(sum(s.loop_launches for s in stats), 1)
-    # fused: xi (3) and g in, xi (3) out; split: div reads xi (3), writes v; grad reads v, g, xi (3),
-    # writes xi (3) -- per launch the average of the two
-    bpv = 48 if variant == 1 else 28
+    # tiled: xi (3) and the differences of g (3) in, xi (3) out; per-voxel fused: xi (3) and g in,
+    # xi (3) out; split: div reads xi (3), writes v; grad reads v, g, xi (3), writes xi (3) -- per
+    # launch the average of the two
+    bpv = {0: 36, 1: 48, 2: 28}[variant]
     achieved = (bpv / 2 if variant == 1 else bpv) * vox / launch_s / 1e9
     peaks = measured_peaks()
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",

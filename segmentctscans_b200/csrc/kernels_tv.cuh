@@ -8,10 +8,13 @@
 // with -fmad=false).
 #pragma once
 
+#include <cuda.h>
+
 #include <cstdint>
 
 #include "geometry.cuh"
 #include "kernels_plain.cuh"
+#include "tma.cuh"
 
 namespace potts {
 
@@ -143,6 +146,27 @@ __global__ void __launch_bounds__(kPlainThreads) tv_update_kernel(Geometry g, fl
     gio[o] = fmaf(-lam, tv_div_at(g, xi, o, p.n, li), gio[o]);
 }
 
+// The lambda-scaled forward differences of g that grad_kernel (:89-166) computes in every
+// iteration, computed once per solve with the same operations: D_n = (g(x+e_n) - g(x)) /
+// lambda, D_r and D_c likewise (zero where the neighbour does not exist), three planes laid
+// out like g.  g does not change during the iterations, so an iteration that reads D gets
+// the same bits as one that recomputes it.
+__global__ void __launch_bounds__(kPlainThreads) tv_gdiff_kernel(Geometry g, const float *__restrict__ gin,
+                                                                 float *__restrict__ D, float lam)
+{
+    const PlainIndex p = plain_index(g, 0, g.ns);
+    if (!p.valid) return;
+    const LineInfo li = load_line(g, p.line);
+    const int64_t o = p.line * g.nstride_w + p.n;
+    float d1 = 0.0f, d2 = 0.0f, d3 = 0.0f;
+    if (p.n + 1 < g.ns) d1 = __fdiv_rn(gin[o + 1] - gin[o], lam);
+    if (li.flags & kHasNextRow) d2 = __fdiv_rn(gin[o + g.nstride_w] - gin[o], lam);
+    if (li.next_col >= 0) d3 = __fdiv_rn(gin[(int64_t)li.next_col * g.nstride_w + p.n] - gin[o], lam);
+    D[o] = d1;
+    D[g.plane_w + o] = d2;
+    D[2 * g.plane_w + o] = d3;
+}
+
 }  // namespace potts
 
 namespace potts {
@@ -150,46 +174,33 @@ namespace potts {
 // Tiled fused iteration.  A block owns a tile of TR rows x TN slices and marches
 // over the columns [ca, cb) of its work item (x = first row, y = first slice,
 // z/w = column range, the work items of the Potts kernel).  Shared memory holds
-// a ring of three column planes of xi (rows r0-1 .. r0+TR, slices n0-1 ..
-// n0+TN) and of g (rows r0 .. r0+TR, slices n0 .. n0+TN), filled by cp.async
-// two planes ahead of the plane being updated, and two planes of v = div xi
-// (the g box), so that each xi, g value is read from DRAM once per plane and v
-// is computed once per voxel.  The operations per voxel are those of
-// tv_div_at and tv_grad_kernel, in the same order.  Rows of the boxes are
-// padded so that slice n0 starts a 16-byte word: xi rows hold slice n at
-// n - n0 + 4 (stride TN + 8), g and v rows at n - n0 (stride TN + 4); the
-// slices n0 .. n0+TN-1 of a row come in 16-byte copies, the halo slices
-// singly.
+// a ring of three column planes of xi (rows r0-1 .. r0+TR, slices n0-4 ..
+// n0+TN+3, the three components), each one TMA box loaded two planes ahead of
+// the plane being updated, and two planes of v = div xi (rows r0 .. r0+TR,
+// slices n0 .. n0+TN), so that each xi value is read from DRAM once per plane
+// and v is computed once per voxel.  The lambda-scaled differences of g come
+// from tv_gdiff_kernel's planes.  The operations per voxel are those of
+// tv_div_at and tv_grad_kernel, in the same order.  The xi box starts at slice
+// n0-4 so that its first word is 16-byte aligned: slice n sits at n - n0 + 4 of
+// a row (stride TN + 8); v rows hold slice n at n - n0 (stride TN + 4).  Box
+// rows outside the plane's column come from other columns or are zero-filled;
+// they are never read.
 template <int TR, int TN>
 struct TvTile {
-    static_assert(TN % 4 == 0, "16-byte row chunks");
+    static_assert(TN % 4 == 0, "16-byte aligned box start");
     static constexpr int XR = TR + 2, XS = TN + 8;  // xi box: rows r0-1 .., row stride
-    static constexpr int VR = TR + 1, GS = TN + 4;  // v and g boxes: rows r0 .., row stride
+    static constexpr int VR = TR + 1, GS = TN + 4;  // v box: rows r0 .., row stride
     static constexpr int XC = XR * XS;              // one xi component
     static constexpr int XI_PLANE = 3 * XC;
+    static constexpr int XI_SLOT = (XI_PLANE + 31) / 32 * 32;  // 128-byte aligned slots
     static constexpr int V_PLANE = VR * GS;
-    static constexpr int SMEM_FLOATS = 3 * XI_PLANE + 3 * V_PLANE + 2 * V_PLANE;
+    static constexpr uint32_t BOX_BYTES = 4u * XI_PLANE;
+    static constexpr int OFF_BAR = 4 * (3 * XI_SLOT + 2 * V_PLANE);  // bytes: 3 mbarriers, abort flag
+    static constexpr int SMEM_BYTES = OFF_BAR + 3 * 8 + 8 + 128;     // + alignment slack
 };
 
 // column table entry: x = first line, y/z = row range of the column (the Potts kernel's table)
 __device__ __forceinline__ bool tv_row_in(int4 ci, int row) { return row >= ci.y && row < ci.z; }
-
-// asynchronous copies global -> shared: 4 bytes (zero when !valid), and 16 bytes of which the
-// first `bytes` are read and the rest zero-filled
-__device__ __forceinline__ void tv_cp_async4(float *dst, const float *src, bool valid)
-{
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0)
-                 : "memory");
-}
-__device__ __forceinline__ void tv_cp_async16(float *dst, const float *src, int bytes)
-{
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void tv_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-// wait until at most one group (the newest) of this thread's copies is in flight
-__device__ __forceinline__ void tv_cp_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 }  // namespace potts
 
@@ -200,86 +211,58 @@ constexpr int kTvThreads = 256;
 // Thread assignments (8 x 128 tiles, 256 threads; fixed for the whole column march, so
 // that index arithmetic is done once per block):
 //  - update: thread t owns slice nn = t % 128 and rows 4h .. 4h+3 (h = t / 128), walking
-//    down the rows with the v and g values of the row below kept in registers;
+//    down the rows with the v value of the row below kept in a register;
 //  - divergence: the same slice, v rows 5h .. 5h+4 (of nine), xi_1 of the row above kept in
-//    registers; thread t < 9 also computes v at slice n0+128 of row t;
-//  - copies: 16-byte chunk t % 32 of the xi box lines t/32 + 8j (j < 4; 30 lines =
-//    3 components x 10 rows) and of the g box lines t/32 + 8j (j < 2; 9 rows); thread t < 60
-//    copies the halo slice of xi line t/2 (n0-1 for even t, n0+128 for odd t), threads
-//    64 .. 72 the slice n0+128 of g row t-64.
+//    a register; thread t < 9 also computes v at slice n0+128 of row t;
+//  - thread 0 issues the TMA loads.
+// Every wait on a load is bounded; a block whose wait gives up sets *err, drains its loads in
+// flight (bounded) and stops.
 template <int TR, int TN>
 __global__ void __launch_bounds__(kTvThreads, 3)
     tv_tiled_kernel(Geometry g, const int4 *__restrict__ cols, int col_begin, int col_end,
-                    const int4 *__restrict__ work, const float *__restrict__ gin, const float *__restrict__ xi_in,
-                    float *__restrict__ xi_out, float lam, float tau, float *dq)
+                    const int4 *__restrict__ work, const __grid_constant__ CUtensorMap xi_map,
+                    const float *__restrict__ D, float *__restrict__ xi_out, float tau, float *dq, int *err)
 {
     static_assert(TR == 8 && TN == 128 && kTvThreads == 256, "thread assignments are for 8 x 128 tiles");
     using T = TvTile<TR, TN>;
-    extern __shared__ __align__(16) float tv_smem[];
-    auto sx = [&](int sl) { return tv_smem + sl * T::XI_PLANE; };
-    auto sg = [&](int sl) { return tv_smem + 3 * T::XI_PLANE + sl * T::V_PLANE; };
-    auto sv = [&](int sl) { return tv_smem + 3 * T::XI_PLANE + (3 + sl) * T::V_PLANE; };
+    extern __shared__ __align__(128) uint8_t tv_raw[];
+    // align to 128 bytes by pointer arithmetic on the shared array itself
+    uint8_t *const base = tv_raw + ((128u - (smem_addr(tv_raw) & 127u)) & 127u);
+    float *const smf = reinterpret_cast<float *>(base);
+    uint64_t *const bar = reinterpret_cast<uint64_t *>(base + T::OFF_BAR);
+    volatile int *const abort = reinterpret_cast<volatile int *>(base + T::OFF_BAR + 3 * 8);
+    auto sx = [&](int sl) { return smf + sl * T::XI_SLOT; };
+    auto sv = [&](int sl) { return smf + 3 * T::XI_SLOT + sl * T::V_PLANE; };
     const int t = threadIdx.x;
     const int4 wk = work[blockIdx.x];
     const int r0 = wk.x, n0 = wk.y, ca = wk.z, cb = wk.w;
     const int64_t nsw = g.nstride_w;
     auto col_at = [&](int c) { return (c >= col_begin && c < col_end) ? cols[c] : make_int4(0, 0, 0, 0); };
 
-    // ---- copy assignments
-    const int ck = t & 31, cl = t >> 5;
-    const int cbytes = 4 * max(0, min(4, g.ns - (n0 + 4 * ck)));
-    int64_t xoff[4];
-    int xdst[4], xrow[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int line = cl + 8 * j, comp = line / 10, rr = line % 10;
-        xrow[j] = line < 30 ? r0 - 1 + rr : INT32_MIN;  // INT32_MIN: no line, never in a column
-        xoff[j] = comp * g.plane_w + (int64_t)(r0 - 1 + rr) * nsw + n0 + 4 * ck;
-        xdst[j] = comp * T::XC + rr * T::XS + 4 + 4 * ck;
+    if (t == 0) {
+        for (int k = 0; k < 3; ++k) mbar_init(bar + k, 1);
+        *abort = 0;
+        mbar_fence_init();
+        tma_prefetch_desc(&xi_map);
     }
-    const int grow1 = cl == 0 ? r0 + 8 : INT32_MIN;  // the ninth g row, copied by warp 0
-    // halo slices: kind 1 = xi, 2 = g
-    int s_kind = 0, s_row = INT32_MIN, s_dst = 0;
-    int64_t s_off = 0;
-    if (t < 60) {
-        const int line = t >> 1, comp = line / 10, rr = line % 10, n = (t & 1) ? n0 + TN : n0 - 1;
-        s_kind = 1;
-        s_row = (n >= 0 && n < g.ns) ? r0 - 1 + rr : INT32_MIN;
-        s_off = comp * g.plane_w + (int64_t)(r0 - 1 + rr) * nsw + n;
-        s_dst = comp * T::XC + rr * T::XS + ((t & 1) ? TN + 4 : 3);
-    } else if (t >= 64 && t < 64 + T::VR) {
-        const int rr = t - 64, n = n0 + TN;
-        s_kind = 2;
-        s_row = n < g.ns ? r0 + rr : INT32_MIN;
-        s_off = (int64_t)(r0 + rr) * nsw + n;
-        s_dst = rr * T::GS + TN;
-    }
+    __syncthreads();
+    uint32_t phase = 0, pending = 0;  // per slot: parity of the next wait, load in flight (thread 0's view)
+    // plane c's xi box (rows r0-1 .., slices n0-4 ..) into ring slot `slot`; thread 0 only
     auto issue = [&](int c, int slot) {
         const int4 ci = col_at(c);
-        const int64_t shift = (int64_t)(ci.x - ci.y) * nsw;  // line of row r: ci.x + r - ci.y
-        float *X = sx(slot), *G = sg(slot);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            if (xrow[j] == INT32_MIN) continue;
-            const int b = tv_row_in(ci, xrow[j]) ? cbytes : 0;
-            tv_cp_async16(X + xdst[j], b ? xi_in + xoff[j] + shift : xi_in, b);
+        mbar_arrive_expect_tx(bar + slot, T::BOX_BYTES);
+        tma_load_3d(sx(slot), &xi_map, bar + slot, n0 - 4, ci.x - ci.y + r0 - 1, 0);
+        pending |= 1u << slot;
+    };
+    auto wait_slot = [&](int slot) {  // warp-uniform
+        const bool ok = mbar_wait_warp(bar + slot, (phase >> slot) & 1u, abort);
+        if (ok) {
+            phase ^= 1u << slot;
+            pending &= ~(1u << slot);
         }
-        {
-            const int b = tv_row_in(ci, r0 + cl) ? cbytes : 0;
-            tv_cp_async16(G + cl * T::GS + 4 * ck, b ? gin + (int64_t)(r0 + cl) * nsw + n0 + 4 * ck + shift : gin, b);
-        }
-        if (grow1 != INT32_MIN) {
-            const int b = tv_row_in(ci, grow1) ? cbytes : 0;
-            tv_cp_async16(G + 8 * T::GS + 4 * ck, b ? gin + (int64_t)grow1 * nsw + n0 + 4 * ck + shift : gin, b);
-        }
-        if (s_kind) {
-            const bool in = tv_row_in(ci, s_row);
-            const float *src = s_kind == 1 ? xi_in : gin;
-            tv_cp_async4((s_kind == 1 ? X : G) + s_dst, in ? src + s_off + shift : src, in);
-        }
+        return ok;
     };
 
-    // ---- divergence and update assignments
     const int nn = t & (TN - 1), h = t >> 7;
     const int n = n0 + nn;
     const bool nin = n < g.ns, nbk = n > 0, nfw = n + 1 < g.ns;
@@ -321,43 +304,51 @@ __global__ void __launch_bounds__(kTvThreads, 3)
     };
 
     // planes ca-1, ca, ca+1 into slots 0, 1, 2 (plane c sits in slot (c - ca + 1) mod 3)
-#pragma unroll 1
-    for (int k = 0; k < 3; ++k) {
-        if (ca - 1 + k <= cb) issue(ca - 1 + k, k);
-        tv_cp_commit();
-    }
-    tv_cp_wait_one();  // planes ca-1 and ca have landed (this thread's copies)
-    __syncthreads();   // ... and every thread's
-    divergence(col_at(ca), col_at(ca - 1), col_at(ca + 1), sx(1), sx(0), sv(0));
+    if (t == 0)
+        for (int k = 0; k < 3; ++k)
+            if (ca - 1 + k <= cb) issue(ca - 1 + k, k);
+    wait_slot(0);
+    wait_slot(1);
+    __syncthreads();
+    if (!*abort) divergence(col_at(ca), col_at(ca - 1), col_at(ca + 1), sx(1), sx(0), sv(0));
     __syncthreads();
     float dmax = 0.0f;
     int sp = 0, sc = 1, sn = 2;  // slots of planes c-1, c, c+1
     int vc = 0;                  // v slot of plane c
     const int64_t rowoff = (int64_t)(r0 + 4 * h) * nsw + n;
 #pragma unroll 1
-    for (int c = ca; c < cb; ++c) {
-        // plane c+2 into the slot of plane c-1, free since the last barrier
-        if (c + 2 <= cb) issue(c + 2, sp);
-        tv_cp_commit();
-        tv_cp_wait_one();  // plane c+1 has landed
-        __syncthreads();
+    for (int c = ca; c < cb && !*abort; ++c) {
         const int4 ci = col_at(c), cn = col_at(c + 1);
+        const int64_t o0 = (int64_t)(ci.x - ci.y) * nsw + rowoff;
+        // this plane's differences of g, in flight during the wait and the divergence
+        float dg[4][3];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const bool in = tv_row_in(ci, r0 + 4 * h + m) && nin;
+            const int64_t o = o0 + m * nsw;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) dg[m][k] = in ? __ldg(D + k * g.plane_w + o) : 0.0f;
+        }
+        // plane c+2 into the slot of plane c-1, free since the last barrier
+        if (t == 0 && c + 2 <= cb) issue(c + 2, sp);
+        wait_slot(sn);  // plane c+1
+        __syncthreads();
+        if (*abort) break;
         divergence(cn, ci, col_at(c + 2), sx(sn), sx(sc), sv(vc ^ 1));
         __syncthreads();
-        const float *Vc = sv(vc), *Vn = sv(vc ^ 1), *Gc = sg(sc), *Gn = sg(sn);
+        const float *Vc = sv(vc), *Vn = sv(vc ^ 1);
         const float *x0 = sx(sc), *x1 = x0 + T::XC, *x2 = x0 + 2 * T::XC;
-        const int64_t o0 = (int64_t)(ci.x - ci.y) * nsw + rowoff;
-        float v0 = Vc[(4 * h) * T::GS + nn], gg = Gc[(4 * h) * T::GS + nn];
+        float v0 = Vc[(4 * h) * T::GS + nn];
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
             const int rr = 4 * h + m, row = r0 + rr;
             const int a = rr * T::GS + nn, b = (rr + 1) * T::XS + nn + 4;
-            const float vr = Vc[a + 1], gr = Gc[a + 1], vd = Vc[a + T::GS], gd = Gc[a + T::GS];
+            const float vr = Vc[a + 1], vd = Vc[a + T::GS];
             if (tv_row_in(ci, row) && nin) {
                 float g1 = 0.0f, g2 = 0.0f, g3 = 0.0f;
-                if (nfw) g1 = (vr - v0) - __fdiv_rn(gr - gg, lam);
-                if (row + 1 < ci.z) g2 = (vd - v0) - __fdiv_rn(gd - gg, lam);
-                if (tv_row_in(cn, row)) g3 = (Vn[a] - v0) - __fdiv_rn(Gn[a] - gg, lam);
+                if (nfw) g1 = (vr - v0) - dg[m][0];
+                if (row + 1 < ci.z) g2 = (vd - v0) - dg[m][1];
+                if (tv_row_in(cn, row)) g3 = (Vn[a] - v0) - dg[m][2];
                 float s = g1 * g1;
                 s = fmaf(g2, g2, s);
                 s = fmaf(g3, g3, s);
@@ -377,7 +368,6 @@ __global__ void __launch_bounds__(kTvThreads, 3)
                 xi_out[2 * g.plane_w + o] = q3;
             }
             v0 = vd;
-            gg = gd;
         }
         __syncthreads();
         const int tmp = sp;
@@ -386,7 +376,12 @@ __global__ void __launch_bounds__(kTvThreads, 3)
         sn = tmp;
         vc ^= 1;
     }
-    asm volatile("cp.async.wait_all;\n" ::: "memory");  // nothing may be in flight at exit
+    if (t == 0 && *abort) {
+        // loads still in flight must land before the block's shared memory goes away
+        for (int k = 0; k < 3; ++k)
+            if ((pending >> k) & 1u) mbar_wait_bounded(bar + k, (phase >> k) & 1u, kDrainTries);
+        atomicExch(err, 1);
+    }
     if (dq) block_max_to(dmax, dq);
 }
 

@@ -937,25 +937,32 @@ int context_init(int device, void *stream, bool use_stream, potts_context **out)
 // place; xi (two halves of 3 planes for the fused form) and v live in the
 // context's state buffer, laid out like g.
 // Work items and shared-memory size of the tiled TV kernel for TR x TN tiles.
+// Work items, shared-memory size and the tensor maps of the two xi buffers (3 planes each,
+// boxes of XS slices x XR lines x 3 components) of the tiled TV kernel for TR x TN tiles.
 template <int TR, int TN>
-int tv_tiled_setup(potts_context *ctx, int ns)
+int tv_tiled_setup(potts_context *ctx, const Geometry &g, const float *xi_a, const float *xi_b, CUtensorMap *maps)
 {
-    POTTS_TRY(plan_tiles(ctx, ns, TileChoice{TR, TN, 1, 64}));
+    using T = potts::TvTile<TR, TN>;
+    POTTS_TRY(plan_tiles(ctx, g.ns, TileChoice{TR, TN, 1, 64}));
     POTTS_CUDA(cudaFuncSetAttribute(potts::tv_tiled_kernel<TR, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(sizeof(float) * potts::TvTile<TR, TN>::SMEM_FLOATS)));
+                                    T::SMEM_BYTES));
+    const uint64_t dims[3] = {(uint64_t)g.nstride_w, (uint64_t)g.n_lines, 3};
+    const uint64_t strides[2] = {sizeof(float) * (uint64_t)g.nstride_w, sizeof(float) * (uint64_t)g.plane_w};
+    const uint32_t box[3] = {(uint32_t)T::XS, (uint32_t)T::XR, 3};
+    POTTS_TRY(encode_map(&maps[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, xi_a, 3, dims, strides, box));
+    POTTS_TRY(encode_map(&maps[1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, xi_b, 3, dims, strides, box));
     return POTTS_OK;
 }
 
 template <int TR, int TN>
-void tv_tiled_launch(potts_context *ctx, const Geometry &g, const float *d_g, const float *xi, float *xi_out,
-                     float lam, float tau, float *dq)
+void tv_tiled_launch(potts_context *ctx, const Geometry &g, const CUtensorMap &xi_map, const float *D, float *xi_out,
+                     float tau, float *dq)
 {
     if (ctx->n_work == 0) return;
     const MappingCopy &mc = ctx->mapping;
-    potts::tv_tiled_kernel<TR, TN><<<ctx->n_work, potts::kTvThreads,
-                                     sizeof(float) * potts::TvTile<TR, TN>::SMEM_FLOATS, ctx->stream>>>(
+    potts::tv_tiled_kernel<TR, TN><<<ctx->n_work, potts::kTvThreads, potts::TvTile<TR, TN>::SMEM_BYTES, ctx->stream>>>(
         g, static_cast<const int4 *>(ctx->cols.p), (int)mc.m.col_begin, (int)mc.m.col_end,
-        static_cast<const int4 *>(ctx->work.p), d_g, xi, xi_out, lam, tau, dq);
+        static_cast<const int4 *>(ctx->work.p), xi_map, D, xi_out, tau, dq, (int *)ctx->err.p);
 }
 
 int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int variant, potts_stats *stats)
@@ -970,11 +977,16 @@ int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int 
     g.ns = (int)mc.m.n_images;
     g.slab_start = 0;
     cudaStream_t s = ctx->stream;
-    const size_t planes = variant == POTTS_VARIANT_PLAIN ? 4 : 6;  // fused forms: xi ping-pong
+    // the tiled kernel's TMA boxes need 16-byte line strides, else the per-voxel fused kernel runs
+    const bool tiled = variant == POTTS_VARIANT_FUSED && mc.m.nstride % 4 == 0;
+    // split: xi, v; fused forms: xi ping-pong; tiled: and the three difference planes of g
+    const size_t planes = variant == POTTS_VARIANT_PLAIN ? 4 : tiled ? 9 : 6;
     POTTS_TRY(ensure(ctx, ctx->state, sizeof(float) * planes * (size_t)std::max<int64_t>(g.plane_w, 1)));
     POTTS_TRY(ensure(ctx, ctx->dq, sizeof(float) * (size_t)std::max(iters, 1)));
+    POTTS_TRY(ensure(ctx, ctx->err, sizeof(int)));
     float *xi = static_cast<float *>(ctx->state.p), *v = xi + 3 * g.plane_w;
-    float *xi_b = xi + 3 * g.plane_w;  // fused form: the second half
+    float *xi_b = xi + 3 * g.plane_w;  // fused forms: the second half
+    float *dgp = xi + 6 * g.plane_w;    // tiled form: differences of g
     float *dq = static_cast<float *>(ctx->dq.p);
     ctx->seg_used = 0;
     ctx->seg_open = false;
@@ -982,20 +994,24 @@ int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int 
     POTTS_CUDA(cudaEventRecord(ctx->ev0, s));
     POTTS_CUDA(cudaMemsetAsync(ctx->state.p, 0, sizeof(float) * planes * (size_t)std::max<int64_t>(g.plane_w, 1), s));
     POTTS_CUDA(cudaMemsetAsync(dq, 0, sizeof(float) * (size_t)std::max(iters, 1), s));
+    POTTS_CUDA(cudaMemsetAsync(ctx->err.p, 0, sizeof(int), s));
     const unsigned nb = plain_blocks(g, 0, g.ns);
     // tiled form: the Potts kernel's column table and work items for 8 x 128 tiles
     constexpr int kTvRows = 8, kTvSlices = 128;
-    // the tiled kernel copies 16-byte words of rows: g and every line must start on one, else the
-    // per-voxel fused kernel runs
-    const bool words = mc.m.nstride % 4 == 0 && reinterpret_cast<uintptr_t>(d_g) % 16 == 0;
-    const bool tiled = words && variant == POTTS_VARIANT_FUSED;
-    if (tiled && g.n_lines > 0 && iters > 0) POTTS_TRY((tv_tiled_setup<kTvRows, kTvSlices>(ctx, g.ns)));
+    CUtensorMap xi_maps[2];  // of xi and xi_b
+    int map_in = 0;          // the map of the buffer the next launch reads
+    if (tiled && g.n_lines > 0 && iters > 0) {
+        POTTS_TRY((tv_tiled_setup<kTvRows, kTvSlices>(ctx, g, xi, xi_b, xi_maps)));
+        potts::tv_gdiff_kernel<<<nb, potts::kPlainThreads, 0, s>>>(g, d_g, dgp, lam);
+        ctx->total_launches += 1;
+    }
     if (g.n_lines > 0) {
         POTTS_TRY(seg_begin(ctx));
         for (int it = 0; it < iters; ++it) {
             if (tiled) {
-                tv_tiled_launch<kTvRows, kTvSlices>(ctx, g, d_g, xi, xi_b, lam, tau, dq + it);
+                tv_tiled_launch<kTvRows, kTvSlices>(ctx, g, xi_maps[map_in], dgp, xi_b, tau, dq + it);
                 std::swap(xi, xi_b);
+                map_in ^= 1;
                 ctx->loop_launches += 1;
                 ctx->total_launches += 1;
             } else if (variant == POTTS_VARIANT_PLAIN) {
@@ -1017,7 +1033,7 @@ int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int 
     }
     POTTS_CUDA(cudaEventRecord(ctx->ev1, s));
     if (stats) {
-        POTTS_CUDA(cudaStreamSynchronize(s));
+        POTTS_TRY(check_device_error(ctx));
         float ms = 0.0f;
         POTTS_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
         stats->n_slabs = 1;

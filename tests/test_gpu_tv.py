@@ -55,7 +55,8 @@ def test_tv_errors(cuda_device):
 
 
 def test_tv_unaligned_field_pointer(cuda_device, oracle_mod):
-    """A field that does not start on a 16-byte word takes the per-voxel kernel: same bits."""
+    """A field that does not start on a 16-byte word (the tiled kernel reads g only through its
+    difference planes): same bits."""
     import torch
 
     m, u, _ = random_volume(21, 14, 15, 6.2, 3, seed=9)
