@@ -221,7 +221,8 @@ template <int TR, int TN>
 __global__ void __launch_bounds__(kTvThreads, 3)
     tv_tiled_kernel(Geometry g, const int4 *__restrict__ cols, int col_begin, int col_end,
                     const int4 *__restrict__ work, const __grid_constant__ CUtensorMap xi_map,
-                    const float *__restrict__ D, float *__restrict__ xi_out, float tau, float *dq, int *err)
+                    const __grid_constant__ CUtensorMap d_map, const float *__restrict__ D, float *__restrict__ xi_out,
+                    float tau, float *dq, int *err)
 {
     static_assert(TR == 8 && TN == 128 && kTvThreads == 256, "thread assignments are for 8 x 128 tiles");
     using T = TvTile<TR, TN>;
@@ -244,15 +245,18 @@ __global__ void __launch_bounds__(kTvThreads, 3)
         *abort = 0;
         mbar_fence_init();
         tma_prefetch_desc(&xi_map);
+        tma_prefetch_desc(&d_map);
     }
     __syncthreads();
     uint32_t phase = 0, pending = 0;  // per slot: parity of the next wait, load in flight (thread 0's view)
-    // plane c's xi box (rows r0-1 .., slices n0-4 ..) into ring slot `slot`; thread 0 only
+    // plane c's xi box (rows r0-1 .., slices n0-4 ..) into ring slot `slot`, and its box of the
+    // differences of g (rows r0 .., slices n0 ..) into L2; thread 0 only
     auto issue = [&](int c, int slot) {
         const int4 ci = col_at(c);
         mbar_arrive_expect_tx(bar + slot, T::BOX_BYTES);
         tma_load_3d(sx(slot), &xi_map, bar + slot, n0 - 4, ci.x - ci.y + r0 - 1, 0);
         pending |= 1u << slot;
+        if (c >= ca) tma_prefetch_l2_3d(&d_map, n0, ci.x - ci.y + r0, 0);
     };
     auto wait_slot = [&](int slot) {  // warp-uniform
         const bool ok = mbar_wait_warp(bar + slot, (phase >> slot) & 1u, abort);
@@ -317,7 +321,7 @@ __global__ void __launch_bounds__(kTvThreads, 3)
     int vc = 0;                  // v slot of plane c
     const int64_t rowoff = (int64_t)(r0 + 4 * h) * nsw + n;
 #pragma unroll 1
-    for (int c = ca; c < cb && !*abort; ++c) {
+    for (int c = ca; c < cb; ++c) {
         const int4 ci = col_at(c), cn = col_at(c + 1);
         const int64_t o0 = (int64_t)(ci.x - ci.y) * nsw + rowoff;
         // this plane's differences of g, in flight during the wait and the divergence
@@ -329,11 +333,12 @@ __global__ void __launch_bounds__(kTvThreads, 3)
 #pragma unroll
             for (int k = 0; k < 3; ++k) dg[m][k] = in ? __ldg(D + k * g.plane_w + o) : 0.0f;
         }
-        // plane c+2 into the slot of plane c-1, free since the last barrier
-        if (t == 0 && c + 2 <= cb) issue(c + 2, sp);
         wait_slot(sn);  // plane c+1
+        // past this barrier every thread is done with iteration c-1: the slot of plane c-1 and
+        // the v slot of plane c-1 are free
         __syncthreads();
         if (*abort) break;
+        if (t == 0 && c + 2 <= cb) issue(c + 2, sp);
         divergence(cn, ci, col_at(c + 2), sx(sn), sx(sc), sv(vc ^ 1));
         __syncthreads();
         const float *Vc = sv(vc), *Vn = sv(vc ^ 1);
@@ -369,7 +374,6 @@ __global__ void __launch_bounds__(kTvThreads, 3)
             }
             v0 = vd;
         }
-        __syncthreads();
         const int tmp = sp;
         sp = sc;
         sc = sn;

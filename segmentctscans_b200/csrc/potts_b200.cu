@@ -940,7 +940,8 @@ int context_init(int device, void *stream, bool use_stream, potts_context **out)
 // Work items, shared-memory size and the tensor maps of the two xi buffers (3 planes each,
 // boxes of XS slices x XR lines x 3 components) of the tiled TV kernel for TR x TN tiles.
 template <int TR, int TN>
-int tv_tiled_setup(potts_context *ctx, const Geometry &g, const float *xi_a, const float *xi_b, CUtensorMap *maps)
+int tv_tiled_setup(potts_context *ctx, const Geometry &g, const float *xi_a, const float *xi_b, const float *D,
+                   CUtensorMap *maps)
 {
     using T = potts::TvTile<TR, TN>;
     POTTS_TRY(plan_tiles(ctx, g.ns, TileChoice{TR, TN, 1, 64}));
@@ -951,18 +952,20 @@ int tv_tiled_setup(potts_context *ctx, const Geometry &g, const float *xi_a, con
     const uint32_t box[3] = {(uint32_t)T::XS, (uint32_t)T::XR, 3};
     POTTS_TRY(encode_map(&maps[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, xi_a, 3, dims, strides, box));
     POTTS_TRY(encode_map(&maps[1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, xi_b, 3, dims, strides, box));
+    const uint32_t dbox[3] = {(uint32_t)TN, (uint32_t)TR, 3};  // differences of g: L2 prefetch boxes
+    POTTS_TRY(encode_map(&maps[2], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, D, 3, dims, strides, dbox));
     return POTTS_OK;
 }
 
 template <int TR, int TN>
-void tv_tiled_launch(potts_context *ctx, const Geometry &g, const CUtensorMap &xi_map, const float *D, float *xi_out,
-                     float tau, float *dq)
+void tv_tiled_launch(potts_context *ctx, const Geometry &g, const CUtensorMap &xi_map, const CUtensorMap &d_map,
+                     const float *D, float *xi_out, float tau, float *dq)
 {
     if (ctx->n_work == 0) return;
     const MappingCopy &mc = ctx->mapping;
     potts::tv_tiled_kernel<TR, TN><<<ctx->n_work, potts::kTvThreads, potts::TvTile<TR, TN>::SMEM_BYTES, ctx->stream>>>(
         g, static_cast<const int4 *>(ctx->cols.p), (int)mc.m.col_begin, (int)mc.m.col_end,
-        static_cast<const int4 *>(ctx->work.p), xi_map, D, xi_out, tau, dq, (int *)ctx->err.p);
+        static_cast<const int4 *>(ctx->work.p), xi_map, d_map, D, xi_out, tau, dq, (int *)ctx->err.p);
 }
 
 int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int variant, potts_stats *stats)
@@ -998,10 +1001,10 @@ int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int 
     const unsigned nb = plain_blocks(g, 0, g.ns);
     // tiled form: the Potts kernel's column table and work items for 8 x 128 tiles
     constexpr int kTvRows = 8, kTvSlices = 128;
-    CUtensorMap xi_maps[2];  // of xi and xi_b
+    CUtensorMap xi_maps[3];  // of xi, xi_b and the differences of g
     int map_in = 0;          // the map of the buffer the next launch reads
     if (tiled && g.n_lines > 0 && iters > 0) {
-        POTTS_TRY((tv_tiled_setup<kTvRows, kTvSlices>(ctx, g, xi, xi_b, xi_maps)));
+        POTTS_TRY((tv_tiled_setup<kTvRows, kTvSlices>(ctx, g, xi, xi_b, dgp, xi_maps)));
         potts::tv_gdiff_kernel<<<nb, potts::kPlainThreads, 0, s>>>(g, d_g, dgp, lam);
         ctx->total_launches += 1;
     }
@@ -1009,7 +1012,7 @@ int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int 
         POTTS_TRY(seg_begin(ctx));
         for (int it = 0; it < iters; ++it) {
             if (tiled) {
-                tv_tiled_launch<kTvRows, kTvSlices>(ctx, g, xi_maps[map_in], dgp, xi_b, tau, dq + it);
+                tv_tiled_launch<kTvRows, kTvSlices>(ctx, g, xi_maps[map_in], xi_maps[2], dgp, xi_b, tau, dq + it);
                 std::swap(xi, xi_b);
                 map_in ^= 1;
                 ctx->loop_launches += 1;
