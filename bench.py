@@ -867,13 +867,17 @@ def run_tv(args, dist_: Dist) -> None:
         t0 = time.perf_counter()
         oracle.tv(sph.mapping, su, lam, tau, 1, "f64")
         t1 = time.perf_counter() - t0
+        # solves of up to 150 iterations (the reference's count), repeated to fill the budget
         it_cpu = max(1, min(150, int(args.cpu_seconds / max(t1, 1e-3))))
-        t0 = time.perf_counter()
-        oracle.tv(sph.mapping, su, lam, tau, it_cpu, "f64")
+        reps, t0 = 0, time.perf_counter()
+        while reps == 0 or time.perf_counter() - t0 < args.cpu_seconds:
+            oracle.tv(sph.mapping, su, lam, tau, it_cpu, "f64")
+            reps += 1
         tc = time.perf_counter() - t0
-        cpu = {"value": sph.mapping.data_size * it_cpu / tc / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+        cpu = {"value": sph.mapping.data_size * it_cpu * reps / tc / 1e9, "unit": UNIT, "cores": threads,
+               "kind": "port",
                "sample": f"FP64 TV oracle, OpenMP {threads} threads: 768x768 cross-section, 16 slices, "
-                         f"{it_cpu} iterations, {tc:.1f} s"}
+                         f"{reps} solves of {it_cpu} iterations, {tc:.1f} s"}
     if dist_.rank == 0:
         out = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist_.world, "steps": args.steps,

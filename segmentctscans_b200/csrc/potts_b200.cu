@@ -995,7 +995,8 @@ int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int 
     ctx->seg_open = false;
     ctx->loop_launches = ctx->total_launches = 0;
     POTTS_CUDA(cudaEventRecord(ctx->ev0, s));
-    POTTS_CUDA(cudaMemsetAsync(ctx->state.p, 0, sizeof(float) * planes * (size_t)std::max<int64_t>(g.plane_w, 1), s));
+    // xi starts at zero; every other plane is written at the voxels it is read at before it is read
+    POTTS_CUDA(cudaMemsetAsync(ctx->state.p, 0, sizeof(float) * 3 * (size_t)std::max<int64_t>(g.plane_w, 1), s));
     POTTS_CUDA(cudaMemsetAsync(dq, 0, sizeof(float) * (size_t)std::max(iters, 1), s));
     POTTS_CUDA(cudaMemsetAsync(ctx->err.p, 0, sizeof(int), s));
     const unsigned nb = plain_blocks(g, 0, g.ns);
