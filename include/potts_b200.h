@@ -303,6 +303,58 @@ void potts_stepper_destroy(potts_stepper *stepper);
 int potts_tv_denoise(potts_context *ctx, const potts_mapping *map, float *d_g, float lambda, float tau, int iters,
                      int variant, potts_stats *stats);
 
+/* ---- Label-finding inputs: the GPU steps before the Potts solve --------------
+ * Fields are device arrays laid out like `map` (the mapping's span of floats);
+ * only in-mask voxels are read or written.  Results that the reference returns
+ * as host values or vectors are written to host memory, and the call returns
+ * after the stream has finished them. */
+
+/* min_max() (include/min_max.h:7, min_max/min_max.cpp:18-81): min and max over
+ * the in-mask voxels; FLT_MAX / -FLT_MAX for an empty mapping. */
+int potts_min_max(potts_context *ctx, const potts_mapping *map, const float *d_field, float *out_min, float *out_max);
+/* The same over the strictly positive values only: grad_min_max_kernel
+ * (uv-hist/uv-hist-kernel.cpp:29-68), the v range of uv_hist. */
+int potts_min_max_positive(potts_context *ctx, const potts_mapping *map, const float *d_field, float *out_min,
+                           float *out_max);
+/* grad_magn() (include/grad_magn.h:5-6, grad-magn/grad_magn.cpp:17-79): d_v =
+ * 0.5 |central-difference gradient of d_u| at every in-mask voxel, -1 where a
+ * neighbour along n, row or column is outside the mask.  Enqueued on the
+ * context's stream; d_u and d_v must differ. */
+int potts_grad_magn(potts_context *ctx, const potts_mapping *map, const float *d_u, float *d_v);
+/* calc_hist(ctx, in, range_start, range_end, nbins, delta) (include/calc_hist.h:12-13,
+ * calc_hist/calc_hist.cpp:23-80,93-138): counts of nbins (1..65535) bins over
+ * [range_start, range_end]; bin = round(nbins t - 0.5) clamped, t the position
+ * in the range.  jitter > 0 adds a uniform value in [-jitter/2, jitter/2) to
+ * every voxel and counts only voxels with range_start - jitter/2 <= x and
+ * x + jitter/2 <= range_end, as the reference does; the reference draws the
+ * jitter from a randomly seeded stream, here it is a function of (seed, voxel),
+ * so a seed reproduces a histogram.  out_counts: nbins counts (host);
+ * out_density (optional, host): counts / (in-mask voxels x bin width), the
+ * reference's return value. */
+int potts_calc_hist(potts_context *ctx, const potts_mapping *map, const float *d_field, float range_start,
+                    float range_end, uint32_t nbins, float jitter, uint64_t seed, uint32_t *out_counts,
+                    double *out_density);
+/* calc_hist(ctx, in, nbins, delta) (include/calc_hist.h:9-10, calc_hist.cpp:82-91): the
+ * same over [min, max] of the field, which are returned. */
+int potts_calc_hist_auto(potts_context *ctx, const potts_mapping *map, const float *d_field, uint32_t nbins,
+                         float jitter, uint64_t seed, uint32_t *out_counts, double *out_density, float *out_min,
+                         float *out_max);
+/* Layout of the 2-D histogram (uv-hist/uv-hist-kernel.cpp:112-118): row stride
+ * (nbins rounded up to 32) and span ((nbins - 1) * stride + nbins counts). */
+uint32_t potts_uv_hist_stride(uint32_t nbins);
+uint64_t potts_uv_hist_span(uint32_t nbins);
+/* uv_hist(ctx, u, v, u_start, u_end, v_start, v_end, nbins) (uv-hist/uv-hist.h:33-41,
+ * uv-hist-kernel.cpp:100-197): counts of the pairs (u, v) in nbins x nbins bins,
+ * row ybin (v) x column xbin (u), at ybin * stride + xbin of out_hist (host,
+ * potts_uv_hist_span(nbins) counts). */
+int potts_uv_hist(potts_context *ctx, const potts_mapping *map, const float *d_u, const float *d_v, float u_start,
+                  float u_end, float v_start, float v_end, uint32_t nbins, uint32_t *out_hist);
+/* uv_hist(ctx, u, v, nbins) (uv-hist/uv-hist.h:26-31, uv-hist-kernel.cpp:70-98): the
+ * same over u in [min u, max u] and v in [min, max] of its strictly positive
+ * values; out_ranges = {u_start, u_end, v_start, v_end}. */
+int potts_uv_hist_auto(potts_context *ctx, const potts_mapping *map, const float *d_u, const float *d_v,
+                       uint32_t nbins, uint32_t *out_hist, float *out_ranges);
+
 /* Mask constructor of layout_cylinder::mapping_storage (include/layout_cylinder.h:152-195):
  * fills start_row[cols] and base[cols+1], returns the span (base[cols]). */
 uint64_t potts_cylinder_mapping(uint32_t rows, uint32_t cols, double xc, double yc, double r, uint32_t nstride,

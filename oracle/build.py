@@ -1,7 +1,7 @@
 """Build recipe for the CPU oracle (test infrastructure only).
 
 Compiles ``potts_oracle.c`` twice (REAL=double -> ``*_f64`` symbols, REAL=float
--> ``*_f32`` symbols) plus ``cylinder_oracle.c`` into
+-> ``*_f32`` symbols) plus ``cylinder_oracle.c`` and ``label_oracle.c`` into
 ``oracle/_build/libpotts_oracle.so`` with gcc, OpenMP and ``-ffp-contract=off``
 (no multiply-add is fused unless the source calls fma/fmaf).
 """
@@ -16,7 +16,7 @@ HERE = Path(__file__).resolve().parent
 OUT_DIR = HERE / "_build"
 LIB_PATH = OUT_DIR / "libpotts_oracle.so"
 CFLAGS = ["-O2", "-fPIC", "-fopenmp", "-ffp-contract=off", "-fno-math-errno", "-std=c11", "-Wall", "-Wno-unused-variable"]
-SOURCES = [HERE / "potts_oracle.c", HERE / "cylinder_oracle.c"]
+SOURCES = [HERE / "potts_oracle.c", HERE / "cylinder_oracle.c", HERE / "label_oracle.c"]
 
 
 def up_to_date() -> bool:
@@ -42,9 +42,10 @@ def build_oracle(force: bool = False) -> Path:
         obj = OUT_DIR / f"potts_oracle_{sfx}.o"
         _run([cc, *CFLAGS, f"-DREAL={real}", f"-DSFX={sfx}", *extra, "-c", str(SOURCES[0]), "-o", str(obj)])
         objs.append(obj)
-    obj = OUT_DIR / "cylinder_oracle.o"
-    _run([cc, *CFLAGS, "-c", str(SOURCES[1]), "-o", str(obj)])
-    objs.append(obj)
+    for src in SOURCES[1:]:
+        obj = OUT_DIR / (src.stem + ".o")
+        _run([cc, *CFLAGS, "-c", str(src), "-o", str(obj)])
+        objs.append(obj)
     tmp = str(LIB_PATH) + ".tmp"
     _run([cc, "-shared", "-fopenmp", *map(str, objs), "-o", tmp, "-lm"])
     os.replace(tmp, LIB_PATH)

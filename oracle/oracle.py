@@ -2,7 +2,7 @@
 
 Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of bench.py
 use this module, as the checker.  The restated algorithm lives in
-``potts_oracle.c`` (FP64 and FP32 builds) and ``cylinder_oracle.c``; see their
+``potts_oracle.c`` (FP64 and FP32 builds), ``cylinder_oracle.c`` and ``label_oracle.c``; see their
 headers for the reference lines each function follows.  Parity unpinned: the
 reference has no tests or golden vectors for this path and cannot be built
 here.
@@ -217,3 +217,72 @@ def tv(m, g: np.ndarray, lam: float, tau: float, iters: int, precision: str = "f
          _ptr(dq, ctypes.c_float)) != 0:
         raise RuntimeError("oracle_tv failed")
     return out, dq[:iters]
+
+
+# ---- label-finding inputs (label_oracle.c) ----------------------------------
+
+def _fptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _uptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+
+
+def min_max(m, f: np.ndarray, positive: bool = False):
+    """min_max (min_max/min_max.cpp:18-54) or, positive, the min/max of the strictly positive values
+    (uv-hist-kernel.cpp:29-68) over the in-mask voxels."""
+    f = np.ascontiguousarray(f, dtype=np.float32)
+    out = np.zeros(2, np.float32)
+    fn = lib().oracle_min_max
+    fn.argtypes = [ctypes.POINTER(OCyl), ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    oc = ocyl(m)
+    fn(ctypes.byref(oc), _fptr(f), int(bool(positive)), _fptr(out))
+    return float(out[0]), float(out[1])
+
+
+def grad_magn(m, u: np.ndarray) -> np.ndarray:
+    """grad_magn (grad-magn/grad_magn.cpp:17-58): the span, in-mask voxels written, others 0."""
+    u = np.ascontiguousarray(u, dtype=np.float32)
+    v = np.zeros_like(u)
+    fn = lib().oracle_grad_magn
+    fn.argtypes = [ctypes.POINTER(OCyl), ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
+    oc = ocyl(m)
+    fn(ctypes.byref(oc), _fptr(u), _fptr(v))
+    return v
+
+
+def calc_hist(m, f: np.ndarray, range_start: float, range_end: float, nbins: int, jitter: float = 0.0,
+              seed: int = 0) -> np.ndarray:
+    """calc_hist counts (calc_hist/calc_hist.cpp:23-80), jitter from (seed, voxel)."""
+    f = np.ascontiguousarray(f, dtype=np.float32)
+    counts = np.zeros(nbins, np.uint32)
+    fn = lib().oracle_calc_hist
+    fn.argtypes = [ctypes.POINTER(OCyl), ctypes.POINTER(ctypes.c_float), ctypes.c_float, ctypes.c_float,
+                   ctypes.c_uint32, ctypes.c_float, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint32)]
+    oc = ocyl(m)
+    fn(ctypes.byref(oc), _fptr(f), float(range_start), float(range_end), int(nbins), float(jitter),
+       int(seed) & (2**64 - 1), _uptr(counts))
+    return counts
+
+
+def uv_stride(nbins: int) -> int:
+    return (nbins + 31) // 32 * 32
+
+
+def uv_hist(m, u: np.ndarray, v: np.ndarray, u_start: float, u_end: float, v_start: float, v_end: float,
+            nbins: int) -> np.ndarray:
+    """uv_hist counts (uv-hist/uv-hist-kernel.cpp:100-197): (nbins - 1) * stride + nbins values,
+    row ybin (v), column xbin (u)."""
+    u = np.ascontiguousarray(u, dtype=np.float32)
+    v = np.ascontiguousarray(v, dtype=np.float32)
+    stride = uv_stride(nbins)
+    hist = np.zeros((nbins - 1) * stride + nbins, np.uint32)
+    fn = lib().oracle_uv_hist
+    fn.argtypes = [ctypes.POINTER(OCyl), ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                   ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_uint32, ctypes.c_uint32,
+                   ctypes.POINTER(ctypes.c_uint32)]
+    oc = ocyl(m)
+    fn(ctypes.byref(oc), _fptr(u), _fptr(v), float(u_start), float(u_end), float(v_start), float(v_end), int(nbins),
+       stride, _uptr(hist))
+    return hist

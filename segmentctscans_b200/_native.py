@@ -111,6 +111,15 @@ SIGNATURES = {
     "potts_stepper_finish": (_I, [_P, _P, _P, _P]),
     "potts_stepper_destroy": (None, [_P]),
     "potts_tv_denoise": (_I, [_P, _MP, _P, _F, _F, _I, _I, _SP]),
+    "potts_min_max": (_I, [_P, _MP, _P, _FP, _FP]),
+    "potts_min_max_positive": (_I, [_P, _MP, _P, _FP, _FP]),
+    "potts_grad_magn": (_I, [_P, _MP, _P, _P]),
+    "potts_calc_hist": (_I, [_P, _MP, _P, _F, _F, _U32, _F, _U64, _P, _P]),
+    "potts_calc_hist_auto": (_I, [_P, _MP, _P, _U32, _F, _U64, _P, _P, _FP, _FP]),
+    "potts_uv_hist_stride": (_U32, [_U32]),
+    "potts_uv_hist_span": (_U64, [_U32]),
+    "potts_uv_hist": (_I, [_P, _MP, _P, _P, _F, _F, _F, _F, _U32, _P]),
+    "potts_uv_hist_auto": (_I, [_P, _MP, _P, _P, _U32, _P, _FP]),
 }
 STATIC_MAX_COLS = 16384
 

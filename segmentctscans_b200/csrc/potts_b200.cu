@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -16,6 +17,7 @@
 #include "kernels_plain.cuh"
 #include "kernels_adjoint.cuh"
 #include "kernels_tiled.cuh"
+#include "kernels_hist.cuh"
 #include "kernels_tv.cuh"
 #include "voxel.cuh"
 
@@ -195,6 +197,7 @@ struct potts_context {
     MappingCopy mapping;  // last mapping whose line table is on the device
     bool mapping_valid = false;
     DevBuf lines, state, dq, energy, partial, host_u, host_res, host_labels, ustage, err;
+    DevBuf hist;  // min/max partials and histogram counters of the label-finding inputs
     float *pinned_dq = nullptr;
     // tiled-kernel tables: per column (depends on the mapping) and the work
     // items of the last (slab extent, tile shape) planned
@@ -272,7 +275,7 @@ int ensure(potts_context *ctx, DevBuf &b, size_t bytes)
 size_t cached_bytes(const potts_context *ctx)
 {
     return ctx->state.bytes + ctx->partial.bytes + ctx->host_u.bytes + ctx->host_res.bytes + ctx->host_labels.bytes +
-           ctx->ustage.bytes;
+           ctx->ustage.bytes + ctx->hist.bytes;
 }
 
 int upload_lines(potts_context *ctx, const potts_mapping *map)
@@ -931,12 +934,9 @@ int context_init(int device, void *stream, bool use_stream, potts_context **out)
 
 #include "adjoint.cuh"
 #include "batch.cuh"
+#include "label_inputs.cuh"
 #include "stepper.cuh"
 
-// TV-L2 denoising (chambolle(), totalvarmin/chambolle.cpp:220-276) of d_g in
-// place; xi (two halves of 3 planes for the fused form) and v live in the
-// context's state buffer, laid out like g.
-// Work items and shared-memory size of the tiled TV kernel for TR x TN tiles.
 // Work items, shared-memory size and the tensor maps of the two xi buffers (3 planes each,
 // boxes of XS slices x XR lines x 3 components) of the tiled TV kernel for TR x TN tiles.
 template <int TR, int TN>
@@ -968,6 +968,9 @@ void tv_tiled_launch(potts_context *ctx, const Geometry &g, const CUtensorMap &x
         static_cast<const int4 *>(ctx->work.p), xi_map, d_map, D, xi_out, tau, dq, (int *)ctx->err.p);
 }
 
+// TV-L2 denoising (chambolle(), totalvarmin/chambolle.cpp:220-276) of d_g in
+// place; xi (two halves of 3 planes for the fused forms), v (split form) and the
+// differences of g (tiled form) live in the context's state buffer, laid out like g.
 int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int variant, potts_stats *stats)
 {
     const MappingCopy &mc = ctx->mapping;
@@ -1110,7 +1113,8 @@ void potts_context_destroy(potts_context *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (DevBuf *b : {&ctx->lines, &ctx->state, &ctx->dq, &ctx->energy, &ctx->partial, &ctx->host_u,
-                      &ctx->host_res, &ctx->host_labels, &ctx->ustage, &ctx->err, &ctx->cols, &ctx->work, &ctx->vols})
+                      &ctx->host_res, &ctx->host_labels, &ctx->ustage, &ctx->err, &ctx->cols, &ctx->work, &ctx->vols,
+                      &ctx->hist})
         if (b->p) cudaFree(b->p);
     if (ctx->pinned_dq) cudaFreeHost(ctx->pinned_dq);
     for (cudaEvent_t e : ctx->seg_ev) cudaEventDestroy(e);
@@ -1582,6 +1586,89 @@ int potts_tv_denoise(potts_context *ctx, const potts_mapping *map, float *d_g, f
     POTTS_CUDA(cudaSetDevice(ctx->device));
     POTTS_TRY(upload_lines(ctx, map));
     return tv_run(ctx, d_g, lambda, tau, iters, variant, stats);
+}
+
+int potts_min_max(potts_context *ctx, const potts_mapping *map, const float *d_field, float *out_min, float *out_max)
+{
+    if (!ctx || !map || !d_field || !out_min || !out_max) return fail(POTTS_EINVAL, "NULL argument");
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    POTTS_TRY(upload_lines(ctx, map));
+    return minmax_run(ctx, d_field, false, out_min, out_max);
+}
+
+int potts_min_max_positive(potts_context *ctx, const potts_mapping *map, const float *d_field, float *out_min,
+                           float *out_max)
+{
+    if (!ctx || !map || !d_field || !out_min || !out_max) return fail(POTTS_EINVAL, "NULL argument");
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    POTTS_TRY(upload_lines(ctx, map));
+    return minmax_run(ctx, d_field, true, out_min, out_max);
+}
+
+int potts_grad_magn(potts_context *ctx, const potts_mapping *map, const float *d_u, float *d_v)
+{
+    if (!ctx || !map || !d_u || !d_v) return fail(POTTS_EINVAL, "NULL argument");
+    if (d_u == d_v) return fail(POTTS_EINVAL, "u and v must be different fields");
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    POTTS_TRY(upload_lines(ctx, map));
+    return grad_magn_run(ctx, d_u, d_v);
+}
+
+int potts_calc_hist(potts_context *ctx, const potts_mapping *map, const float *d_field, float range_start,
+                    float range_end, uint32_t nbins, float jitter, uint64_t seed, uint32_t *out_counts,
+                    double *out_density)
+{
+    if (!ctx || !map || !d_field || !out_counts) return fail(POTTS_EINVAL, "NULL argument");
+    POTTS_TRY(check_nbins(nbins));
+    if (!std::isfinite(jitter) || jitter < 0.0f) return fail(POTTS_EINVAL, "jitter must be finite and >= 0");
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    POTTS_TRY(upload_lines(ctx, map));
+    POTTS_TRY(hist1d_run(ctx, d_field, range_start, range_end, (int)nbins, jitter, seed, out_counts));
+    if (out_density) {
+        // calc_hist.cpp:129-135: counts / (in-mask voxels x bin width), in double
+        const double bin_width = ((double)range_end - (double)range_start) / nbins;
+        const double voxels = (double)ctx->mapping.n_lines * (double)ctx->mapping.m.n_images;
+        const double scale = 1.0 / (voxels * bin_width);
+        for (uint32_t i = 0; i < nbins; ++i) out_density[i] = out_counts[i] * scale;
+    }
+    return POTTS_OK;
+}
+
+int potts_calc_hist_auto(potts_context *ctx, const potts_mapping *map, const float *d_field, uint32_t nbins,
+                         float jitter, uint64_t seed, uint32_t *out_counts, double *out_density, float *out_min,
+                         float *out_max)
+{
+    if (!ctx || !map || !d_field || !out_counts || !out_min || !out_max) return fail(POTTS_EINVAL, "NULL argument");
+    POTTS_TRY(check_nbins(nbins));
+    POTTS_TRY(potts_min_max(ctx, map, d_field, out_min, out_max));
+    return potts_calc_hist(ctx, map, d_field, *out_min, *out_max, nbins, jitter, seed, out_counts, out_density);
+}
+
+uint32_t potts_uv_hist_stride(uint32_t nbins) { return nbins ? uv_stride((int)nbins) : 0u; }
+
+uint64_t potts_uv_hist_span(uint32_t nbins) { return nbins ? uv_span((int)nbins) : 0u; }
+
+int potts_uv_hist(potts_context *ctx, const potts_mapping *map, const float *d_u, const float *d_v, float u_start,
+                  float u_end, float v_start, float v_end, uint32_t nbins, uint32_t *out_hist)
+{
+    if (!ctx || !map || !d_u || !d_v || !out_hist) return fail(POTTS_EINVAL, "NULL argument");
+    POTTS_TRY(check_nbins(nbins));
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    POTTS_TRY(upload_lines(ctx, map));
+    const potts::UvRange r{u_start, u_end, v_start, v_end, (int)nbins, (int)uv_stride((int)nbins)};
+    return uv_hist_run(ctx, d_u, d_v, r, out_hist);
+}
+
+int potts_uv_hist_auto(potts_context *ctx, const potts_mapping *map, const float *d_u, const float *d_v,
+                       uint32_t nbins, uint32_t *out_hist, float *out_ranges)
+{
+    if (!ctx || !map || !d_u || !d_v || !out_hist || !out_ranges) return fail(POTTS_EINVAL, "NULL argument");
+    POTTS_TRY(check_nbins(nbins));
+    // uv-hist-kernel.cpp:70-98: v over its strictly positive values, u over all
+    POTTS_TRY(potts_min_max_positive(ctx, map, d_v, &out_ranges[2], &out_ranges[3]));
+    POTTS_TRY(potts_min_max(ctx, map, d_u, &out_ranges[0], &out_ranges[1]));
+    return potts_uv_hist(ctx, map, d_u, d_v, out_ranges[0], out_ranges[1], out_ranges[2], out_ranges[3], nbins,
+                         out_hist);
 }
 
 }  // extern "C"

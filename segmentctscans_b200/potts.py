@@ -461,3 +461,77 @@ def tv_denoise_host(mapping: CylinderMapping, g: np.ndarray, lam: float, tau: fl
     finally:
         if own:
             ctx.close()
+
+
+# ---- label-finding inputs -----------------------------------------------------
+
+def min_max(ctx: CudaContext, mapping: CylinderMapping, f_ptr: int, *, positive: bool = False) -> tuple[float, float]:
+    """min_max() (min_max/min_max.cpp:56-81) of the device field at f_ptr over the in-mask voxels;
+    positive=True: over its strictly positive values (uv-hist-kernel.cpp:70-92)."""
+    lo, hi = ctypes.c_float(), ctypes.c_float()
+    fn = _native.host_lib().potts_min_max_positive if positive else _native.host_lib().potts_min_max
+    check(fn(ctx.handle, ctypes.byref(mapping.as_c()), ctypes.c_void_p(int(f_ptr)), ctypes.byref(lo),
+             ctypes.byref(hi)))
+    return lo.value, hi.value
+
+
+def grad_magn(ctx: CudaContext, mapping: CylinderMapping, u_ptr: int, v_ptr: int) -> None:
+    """grad_magn() (grad-magn/grad_magn.cpp:17-79): v = 0.5 |central-difference gradient of u|, -1 at
+    the mask boundary; enqueued on the context's stream."""
+    check(_native.host_lib().potts_grad_magn(ctx.handle, ctypes.byref(mapping.as_c()), ctypes.c_void_p(int(u_ptr)),
+                                             ctypes.c_void_p(int(v_ptr))))
+
+
+def calc_hist(ctx: CudaContext, mapping: CylinderMapping, f_ptr: int, range_start: float, range_end: float,
+              nbins: int, *, jitter: float = 0.0, seed: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """calc_hist(ctx, in, range_start, range_end, nbins, delta) (calc_hist/calc_hist.cpp:93-138):
+    (counts uint32, density float64 = counts / (in-mask voxels x bin width))."""
+    counts = np.zeros(int(nbins), np.uint32)
+    dens = np.zeros(int(nbins), np.float64)
+    check(_native.host_lib().potts_calc_hist(ctx.handle, ctypes.byref(mapping.as_c()), ctypes.c_void_p(int(f_ptr)),
+                                             float(range_start), float(range_end), int(nbins), float(jitter),
+                                             int(seed) & (2**64 - 1), counts.ctypes.data, dens.ctypes.data))
+    return counts, dens
+
+
+def calc_hist_auto(ctx: CudaContext, mapping: CylinderMapping, f_ptr: int, nbins: int, *, jitter: float = 0.0,
+                   seed: int = 0) -> tuple[np.ndarray, np.ndarray, float, float]:
+    """calc_hist(ctx, in, nbins, delta) (calc_hist.cpp:82-91): the histogram over [min, max] of the
+    field; returns (counts, density, min, max)."""
+    counts = np.zeros(int(nbins), np.uint32)
+    dens = np.zeros(int(nbins), np.float64)
+    lo, hi = ctypes.c_float(), ctypes.c_float()
+    check(_native.host_lib().potts_calc_hist_auto(ctx.handle, ctypes.byref(mapping.as_c()),
+                                                  ctypes.c_void_p(int(f_ptr)), int(nbins), float(jitter),
+                                                  int(seed) & (2**64 - 1), counts.ctypes.data, dens.ctypes.data,
+                                                  ctypes.byref(lo), ctypes.byref(hi)))
+    return counts, dens, lo.value, hi.value
+
+
+def uv_hist_matrix(hist: np.ndarray, nbins: int) -> np.ndarray:
+    """The nbins x nbins view (row ybin, column xbin) of a 2-D histogram's span."""
+    stride = int(_native.host_lib().potts_uv_hist_stride(int(nbins)))
+    return np.lib.stride_tricks.as_strided(hist, shape=(nbins, nbins), strides=(4 * stride, 4), writeable=False)
+
+
+def uv_hist(ctx: CudaContext, mapping: CylinderMapping, u_ptr: int, v_ptr: int, u_start: float, u_end: float,
+            v_start: float, v_end: float, nbins: int) -> np.ndarray:
+    """uv_hist(ctx, u, v, u_start, u_end, v_start, v_end, nbins) (uv-hist-kernel.cpp:100-197): the
+    counts span ((nbins - 1) * stride + nbins, row ybin of v, column xbin of u)."""
+    hist = np.zeros(int(_native.host_lib().potts_uv_hist_span(int(nbins))), np.uint32)
+    check(_native.host_lib().potts_uv_hist(ctx.handle, ctypes.byref(mapping.as_c()), ctypes.c_void_p(int(u_ptr)),
+                                           ctypes.c_void_p(int(v_ptr)), float(u_start), float(u_end), float(v_start),
+                                           float(v_end), int(nbins), hist.ctypes.data))
+    return hist
+
+
+def uv_hist_auto(ctx: CudaContext, mapping: CylinderMapping, u_ptr: int, v_ptr: int,
+                 nbins: int) -> tuple[np.ndarray, tuple[float, float, float, float]]:
+    """uv_hist(ctx, u, v, nbins) (uv-hist-kernel.cpp:70-98): ranges from u's min/max and the min/max of
+    v's strictly positive values; returns (counts span, (u_start, u_end, v_start, v_end))."""
+    hist = np.zeros(int(_native.host_lib().potts_uv_hist_span(int(nbins))), np.uint32)
+    rng = np.zeros(4, np.float32)
+    check(_native.host_lib().potts_uv_hist_auto(ctx.handle, ctypes.byref(mapping.as_c()), ctypes.c_void_p(int(u_ptr)),
+                                                ctypes.c_void_p(int(v_ptr)), int(nbins), hist.ctypes.data,
+                                                rng.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+    return hist, tuple(float(x) for x in rng)

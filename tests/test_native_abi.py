@@ -109,3 +109,10 @@ def test_context_without_gpu_fails_loudly(native_lib):
     st = native_lib.potts_context_create(0, ctypes.byref(h))
     assert st == _native.POTTS_ENODEV and not h.value
     assert b"device" in native_lib.potts_last_error()
+
+
+def test_uv_hist_layout(native_lib):
+    """uv-hist-kernel.cpp:112-118: rows padded to 32 counts (128 bytes), span (nbins-1) stride + nbins."""
+    assert native_lib.potts_uv_hist_stride(512) == 512 and native_lib.potts_uv_hist_stride(7) == 32
+    assert native_lib.potts_uv_hist_span(512) == 511 * 512 + 512
+    assert native_lib.potts_uv_hist_span(7) == 6 * 32 + 7 and native_lib.potts_uv_hist_span(1) == 1
