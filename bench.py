@@ -74,7 +74,8 @@ def parse_args():
                    help="state storage of the timed solves")
     p.add_argument("--no-storage-compare", action="store_true",
                    help="skip the FP32-plain / BF16 / FP16 comparison solves")
-    p.add_argument("--workload", choices=["config1", "config2", "config3", "config4", "config0", "mid", "mid4", "tv", "tvmid"],
+    p.add_argument("--workload", choices=["config1", "config2", "config3", "config4", "config0", "mid", "mid4", "tv", "tvmid",
+                            "fieldio", "fieldiomid"],
                    default="config1",
                    help="config1: 768x768x1024 r=370 (the benchmark); config0: 128^3 r=60; "
                         "mid: 384x384x256 r=180 (profiling size, state > L2)")
@@ -895,6 +896,140 @@ def run_tv(args, dist_: Dist) -> None:
     dist_.close()
 
 
+def run_fieldio(args, dist_: Dist) -> None:
+    """Field I/O around the solve on the 768^2 x 1024 core: the .bin archive of an FP32 field loaded
+    (Field<float>::load, the potts-model input) and saved (Field<float>::save, the transpose output),
+    a uint16 scan's find_intensity_range + convert_to_fp (transpose), and the --rawout VTK label box
+    (potts-model).  value = in-mask voxels per second through the five device kernels of one step;
+    e2e = the same step through the C ABI with host (pinned) bytes in and out."""
+    import numpy as np
+    import torch
+
+    from segmentctscans_b200 import potts
+    from segmentctscans_b200.phantom import config1_phantom, make_phantom
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    dev = torch.device("cuda", dist_.local)
+    torch.cuda.set_device(dev)
+    dist_.init("nccl")
+    if args.workload == "fieldiomid":
+        ph = make_phantom(256, 384, 384, 180.0, seed=dist_.rank, radius_range=(6.0, 30.0), noise=7e-3, device=dev)
+    else:
+        ph = config1_phantom(seed=dist_.rank, device=dev)
+    m, u = ph.mapping, ph.u
+    vox = m.data_size
+    stream = torch.cuda.current_stream(dev)
+    ctx = potts.make_context(dev.index, stream=stream.cuda_stream)
+    # a uint16 scan of the same phantom (the transpose input) and the output buffers
+    w16 = (u * 50000.0 + 1000.0).clamp_(0, 65535).to(torch.int32).to(torch.int16)
+    g = torch.empty_like(u)
+    un = torch.empty_like(u)
+    n_arch, _ = potts.archive_size(m, "f32")
+    s, rows, cols, _ = potts.raw_labels_dims(m)
+    box_bytes = s * rows * cols
+    h_arch = torch.empty(n_arch, dtype=torch.uint8, pin_memory=True)
+    h_vtk = torch.empty(box_bytes + 4096, dtype=torch.uint8, pin_memory=True)
+    a_np, v_np = h_arch.numpy(), h_vtk.numpy()
+    d_box = torch.empty(box_bytes, dtype=torch.uint8, device=dev)
+
+    def step(host: bool):
+        """One pass; returns the kernel times (ms) of the five kernels."""
+        _, t_save = potts.archive_save(ctx, m, "f32", u.data_ptr(), 0.0, 1.0, out=a_np)
+        _, t_load = potts.archive_load(ctx, a_np, "f32", g.data_ptr(), m.span)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e[0].record(stream)
+        lo, hi, _ = potts.find_intensity_range(ctx, m, w16.data_ptr(), 1e-4)
+        e[1].record(stream)
+        potts.convert_to_fp(ctx, m, "u16", w16.data_ptr(), float(lo), float(hi), un.data_ptr())
+        e[2].record(stream)
+        if host:
+            _, t_box = potts.vtk_labels(ctx, m, u.data_ptr(), out=v_np)
+        else:
+            potts.raw_labels(ctx, m, u.data_ptr(), d_box.data_ptr())
+            e[3].record(stream)
+        torch.cuda.synchronize(dev)
+        t_hist = e[0].elapsed_time(e[1])
+        t_conv = e[1].elapsed_time(e[2])
+        if not host:
+            t_box = e[2].elapsed_time(e[3])
+        return {"pack": t_save, "unpack": t_load, "u16_hist": t_hist, "convert_to_fp": t_conv, "raw_box": t_box}
+
+    for _ in range(args.warmup):
+        step(False)
+    # size-independent check at full size: the archive round trip reproduces every in-mask value
+    mv = g.view(m.n_lines, m.nstride)[:, : m.n_images]
+    assert torch.equal(mv.view(torch.int32), u.view(m.n_lines, m.nstride)[:, : m.n_images].view(torch.int32))
+    torch.cuda.synchronize(dev)
+    dist_.barrier()
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    times = [step(False) for _ in range(args.steps)]
+    torch.cuda.synchronize(dev)
+    dist_.barrier()
+    clk = clocks.stop()
+    avg = {k: sum(t[k] for t in times) / len(times) for k in times[0]}
+    t_step = sum(avg.values()) / 1000.0
+    t_max = dist_.reduce(t_step * args.steps, "max")
+    value = dist_.reduce(float(vox) * args.steps, "sum") / t_max / 1e9
+    # algorithmic bytes per launch
+    algo = {"unpack": 8 * vox, "pack": 8 * vox, "u16_hist": 2 * vox, "convert_to_fp": 6 * vox,
+            "raw_box": 4 * vox + box_bytes}
+    peaks = measured_peaks()
+    kernels = {k: {"avg_ms": round(avg[k], 4), "gbs": round(algo[k] / (avg[k] / 1000.0) / 1e9, 1),
+                   "frac": round(algo[k] / (avg[k] / 1000.0) / 1e9 / peaks["hbm_gbs"], 4),
+                   "bytes_per_launch": algo[k]} for k in avg}
+    roofline = {"bound": "hbm", "achieved": kernels["unpack"]["gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": kernels["unpack"]["frac"], "traffic": None, "kernel": "potts::archive_unpack_kernel<32>",
+                "bytes_per_voxel": 8, "avg_launch_ms": kernels["unpack"]["avg_ms"],
+                "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)"}
+    e2e = None
+    if not args.no_e2e:
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = time.perf_counter()
+        f0.record(stream)
+        for _ in range(args.steps):
+            step(True)
+        f1.record(stream)
+        torch.cuda.synchronize(dev)
+        te = dist_.reduce(max(f0.elapsed_time(f1) / 1000.0, time.perf_counter() - w0), "max")
+        e2e = {"value": dist_.reduce(float(vox) * args.steps, "sum") / te / 1e9, "unit": "Gvox/s",
+               "h2d_bytes_per_step": n_arch, "d2h_bytes_per_step": n_arch + box_bytes,
+               "note": "archive saved to and loaded from pinned host bytes, VTK file assembled in pinned host memory"}
+    cpu = None
+    if dist_.rank == 0 and dist_.world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle
+
+        sph = cpu_sample_phantom()
+        su = sph.u.numpy().copy()
+        data, _ = oracle.archive_encode(sph.mapping, su, "f32", 0.0, 1.0)
+        reps, t0 = 0, time.perf_counter()
+        while reps == 0 or time.perf_counter() - t0 < min(args.cpu_seconds, 15.0):
+            oracle.archive_decode(data, "f32")
+            oracle.archive_encode(sph.mapping, su, "f32", 0.0, 1.0)
+            reps += 1
+        tc = time.perf_counter() - t0
+        cpu = {"value": sph.mapping.data_size * reps / (tc / 2.0) / 1e9, "unit": "Gvox/s", "cores": 1, "kind": "port",
+               "sample": f"bit-serial C oracle, 1 thread: archive decode + encode of the 768x768 cross-section, "
+                         f"16 slices ({sph.mapping.data_size} voxels), {reps} rounds in {tc:.1f} s; value per pass"}
+    if dist_.rank == 0:
+        out = {
+            "metric": "field I/O Gvox/s (archive load + save, intensity range + convert_to_fp, raw label box)",
+            "value": round(value, 3), "unit": "Gvox/s", "n_gpus": dist_.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1000 * t_max / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": f"fieldio_{m.rows}x{m.cols}x{m.n_images}", "in_mask_voxels": vox,
+                       "archive_bytes": n_arch, "box_bytes": box_bytes,
+                       "parallelism": f"replica x{dist_.world}" if dist_.world > 1 else "single",
+                       "l2": "inputs larger than L2"},
+            "roofline": roofline, "kernels": kernels, "e2e": e2e, "gpu_launches": 5 * args.steps, "clocks": clk,
+            "cpu_baseline": cpu, "check": "archive round trip equal on every in-mask voxel",
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    dist_.close()
+
+
 def main():
     args = parse_args()
     d = Dist()
@@ -909,6 +1044,9 @@ def main():
         return
     if args.workload in ("tv", "tvmid"):
         run_tv(args, d)
+        return
+    if args.workload in ("fieldio", "fieldiomid"):
+        run_fieldio(args, d)
         return
     run_ours(args, d)
 

@@ -355,6 +355,93 @@ int potts_uv_hist(potts_context *ctx, const potts_mapping *map, const float *d_u
 int potts_uv_hist_auto(potts_context *ctx, const potts_mapping *map, const float *d_u, const float *d_v,
                        uint32_t nbins, uint32_t *out_hist, float *out_ranges);
 
+/* ---- Field archive (.bin files) and the steps either side of the solve ------
+ * The reference's tools exchange volumes as Field<T> archives: io::BinOArchive
+ * of Field<T>::save (include/field.h:92-119, include/layout_cylinder.h:233-257,
+ * include/io/writeprimitives.h, include/io/outbitstream.h).  One MSB-first bit
+ * stream without an archive header: the mapping in Exp-Golomb codes (extents,
+ * nstride, col_begin, col_end, the start_row and base tables as first value and
+ * signed differences), for FP32 fields the bit patterns of lo and hi, then the
+ * in-mask voxels column by column, row by row, n = 0 .. n_images-1, 32 bits
+ * (FP32) or 16 bits (uint16) each.  The header is coded on the host; the voxel
+ * payload is packed and unpacked on the GPU. */
+enum potts_element {
+    POTTS_ELEM_F32 = 0, /* Field<float>: 32-bit voxels, lo/hi in the header */
+    POTTS_ELEM_U16 = 1  /* Field<uint16_t>: 16-bit voxels */
+};
+
+typedef struct potts_archive_info {
+    uint32_t n_images, rows, cols, nstride, col_begin, col_end; /* the archive's mapping */
+    uint64_t span;        /* elements of the device field it loads into (base[cols]) */
+    float lo, hi;         /* Field<float>::lo()/hi() (include/field.h:79-80); 0 for uint16 */
+    uint64_t header_bits; /* bits before the first voxel */
+    uint64_t voxels;      /* in-mask voxels in the payload */
+    uint64_t total_bytes; /* bytes of the whole archive */
+} potts_archive_info;
+
+typedef struct potts_io_stats {
+    double kernel_ms; /* out: device time of the call's kernel (CUDA events around it) */
+    int launches;     /* out: kernels launched */
+} potts_io_stats;
+
+/* mapping_storage::load (include/layout_cylinder.h:259-312) and the lo/hi of
+ * Field<float>::load (include/field.h:121-131): parses the header of an archive
+ * of element type `elem`.  start_row (cols entries) and base (cols + 1) are
+ * optional; call once without them to learn cols.  POTTS_EINVAL when the bytes
+ * end inside the header or the mapping is not one this library accepts. */
+int potts_archive_read_header(const uint8_t *bytes, uint64_t n_bytes, int elem, potts_archive_info *info,
+                              uint32_t *start_row, uint32_t *base);
+/* Size in bytes of the archive of a field with this mapping (host only). */
+int potts_archive_size(const potts_mapping *map, int elem, uint64_t *total_bytes, uint64_t *header_bits);
+/* Field<T>::load (include/field.h:121-147) into device memory: the voxels of
+ * the archive at `bytes` (host) are written to d_field (float or uint16_t
+ * elements laid out by the archive's mapping, at least info.span elements =
+ * `capacity`); padding slices are not written.  Returns after the copy. */
+int potts_archive_load(potts_context *ctx, const uint8_t *bytes, uint64_t n_bytes, int elem, void *d_field,
+                       uint64_t capacity, potts_archive_info *info, potts_io_stats *stats);
+/* Field<T>::save (include/field.h:92-119) of a device field laid out by `map`
+ * into host memory `out` (capacity bytes); lo/hi are stored for FP32 fields.
+ * out = NULL only reports the size in *out_bytes. */
+int potts_archive_save(potts_context *ctx, const potts_mapping *map, int elem, const void *d_field, float lo,
+                       float hi, uint8_t *out, uint64_t capacity, uint64_t *out_bytes, potts_io_stats *stats);
+/* convert_to_fp(ctx, in, lo, hi) (transpose/convert_to_fp.h:8-10,
+ * transpose/convert_to_fp.cpp:11-79): d_out = 0 where v <= lo, 1 where v >= hi,
+ * else (v - lo) / (hi - lo) in FP32, for a float or uint16 field.  Enqueued on
+ * the context's stream; padding slices are not written. */
+int potts_convert_to_fp(potts_context *ctx, const potts_mapping *map, int elem, const void *d_in, float lo, float hi,
+                        float *d_out);
+/* find_intensity_range(ctx, field, tail_thr) (transpose/find_intensity_range.h,
+ * transpose/find_intensity_range.cpp:64-110): the 65536-bin histogram of a
+ * uint16 field, lo = the last bin whose cumulative count is at most
+ * tail_thr x total, hi = the first bin whose cumulative count reaches
+ * (1 - tail_thr) x total, both narrowed to uint16 as the reference does.
+ * out_hist (optional, host): the 65536 counts. */
+int potts_find_intensity_range(potts_context *ctx, const potts_mapping *map, const uint16_t *d_field,
+                               double tail_thr, uint16_t *out_lo, uint16_t *out_hi, uint64_t *out_hist);
+/* Extent of the raw label box of potts-model.cpp:186-202: slices x rows x
+ * cols, rows from the smallest first row to the largest end row of the columns
+ * that hold rows, cols = col_end - col_begin; row_begin is the box's first row. */
+int potts_raw_labels_dims(const potts_mapping *map, uint32_t *slices, uint32_t *rows, uint32_t *cols,
+                          uint32_t *row_begin);
+/* The raw label box (potts-model.cpp:203-217) in device memory: byte
+ * ((c * rows + r) * slices + n) = min(255, max(0, round(255 v))) of voxel
+ * (n, row_begin + r, col_begin + c) inside the mask, 255 outside.  Enqueued on
+ * the context's stream. */
+int potts_raw_labels(potts_context *ctx, const potts_mapping *map, const float *d_field, uint8_t *d_box);
+/* The --rawout VTK ImageData file of potts-model.cpp:184-243 (XML header, the
+ * box size as 4 little-endian bytes, the raw label box, XML footer) in host
+ * memory; out = NULL only reports the size.  Byte-identical to the reference's
+ * file for the same field. */
+int potts_vtk_labels(potts_context *ctx, const potts_mapping *map, const float *d_field, uint8_t *out,
+                     uint64_t capacity, uint64_t *out_bytes, potts_io_stats *stats);
+/* write_png(img, col, lambda) (potts-model.cpp:34-49): the lines of column
+ * `col` as an 8-bit grey PNG (rows down, slices across), grey =
+ * saturate(round-half-even(255 |v|^(1/2.2))), as cv::pow + convertTo compute
+ * it, here in FP64; written with stored deflate blocks.  out = NULL only
+ * reports the size. */
+int potts_png_slice(potts_context *ctx, const potts_mapping *map, const float *d_field, uint32_t col, uint8_t *out,
+                    uint64_t capacity, uint64_t *out_bytes);
+
 /* Mask constructor of layout_cylinder::mapping_storage (include/layout_cylinder.h:152-195):
  * fills start_row[cols] and base[cols+1], returns the span (base[cols]). */
 uint64_t potts_cylinder_mapping(uint32_t rows, uint32_t cols, double xc, double yc, double r, uint32_t nstride,

@@ -1,7 +1,8 @@
 """Build recipe for the CPU oracle (test infrastructure only).
 
 Compiles ``potts_oracle.c`` twice (REAL=double -> ``*_f64`` symbols, REAL=float
--> ``*_f32`` symbols) plus ``cylinder_oracle.c`` and ``label_oracle.c`` into
+-> ``*_f32`` symbols) plus ``cylinder_oracle.c``, ``label_oracle.c`` and
+``fieldio_oracle.c`` into
 ``oracle/_build/libpotts_oracle.so`` with gcc, OpenMP and ``-ffp-contract=off``
 (no multiply-add is fused unless the source calls fma/fmaf).
 """
@@ -16,7 +17,7 @@ HERE = Path(__file__).resolve().parent
 OUT_DIR = HERE / "_build"
 LIB_PATH = OUT_DIR / "libpotts_oracle.so"
 CFLAGS = ["-O2", "-fPIC", "-fopenmp", "-ffp-contract=off", "-fno-math-errno", "-std=c11", "-Wall", "-Wno-unused-variable"]
-SOURCES = [HERE / "potts_oracle.c", HERE / "cylinder_oracle.c", HERE / "label_oracle.c"]
+SOURCES = [HERE / "potts_oracle.c", HERE / "cylinder_oracle.c", HERE / "label_oracle.c", HERE / "fieldio_oracle.c"]
 
 
 def up_to_date() -> bool:

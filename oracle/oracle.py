@@ -2,7 +2,8 @@
 
 Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of bench.py
 use this module, as the checker.  The restated algorithm lives in
-``potts_oracle.c`` (FP64 and FP32 builds), ``cylinder_oracle.c`` and ``label_oracle.c``; see their
+``potts_oracle.c`` (FP64 and FP32 builds), ``cylinder_oracle.c``, ``label_oracle.c`` and
+``fieldio_oracle.c``; see their
 headers for the reference lines each function follows.  Parity unpinned: the
 reference has no tests or golden vectors for this path and cannot be built
 here.
@@ -286,3 +287,135 @@ def uv_hist(m, u: np.ndarray, v: np.ndarray, u_start: float, u_end: float, v_sta
     fn(ctypes.byref(oc), _fptr(u), _fptr(v), float(u_start), float(u_end), float(v_start), float(v_end), int(nbins),
        stride, _uptr(hist))
     return hist
+
+
+# ---- field archive, convert_to_fp, intensity range, writers (fieldio_oracle.c) ----------
+
+ELEM_BITS = {"f32": 32, "u16": 16}
+
+
+def archive_encode(m, field: np.ndarray, elem: str = "f32", lo: float = 0.0, hi: float = 0.0) -> tuple[bytes, int]:
+    """Field<T>::save (include/field.h:92-119): (archive bytes, header bits).  `field` is the span
+    (float32 or uint16)."""
+    bits = ELEM_BITS[elem]
+    raw = np.ascontiguousarray(field, dtype=np.float32 if bits == 32 else np.uint16)
+    fn = lib().oracle_archive_encode
+    fn.restype = ctypes.c_uint64
+    fn.argtypes = [ctypes.POINTER(OCyl), ctypes.c_int, ctypes.c_void_p, ctypes.c_float, ctypes.c_float,
+                   ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]
+    oc = ocyl(m)
+    hb = ctypes.c_uint64()
+    n = fn(ctypes.byref(oc), bits, raw.ctypes.data, float(lo), float(hi), None, ctypes.byref(hb))
+    out = np.zeros(int(n), np.uint8)
+    fn(ctypes.byref(oc), bits, raw.ctypes.data, float(lo), float(hi), out.ctypes.data, ctypes.byref(hb))
+    return out.tobytes(), int(hb.value)
+
+
+@dataclass
+class ArchiveContents:
+    mapping: object
+    lo: float
+    hi: float
+    header_bits: int
+    field: np.ndarray  # the span, float32 or uint16; padding slices 0
+
+
+def archive_decode(data: bytes, elem: str = "f32") -> ArchiveContents:
+    """Field<T>::load (include/field.h:121-147, include/layout_cylinder.h:259-312)."""
+    from segmentctscans_b200.layout import CylinderMapping
+
+    bits = ELEM_BITS[elem]
+    buf = np.frombuffer(data, np.uint8)
+    fn = lib().oracle_archive_decode
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(ctypes.c_uint32),
+                   ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_float),
+                   ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]
+    hdr = np.zeros(6, np.uint32)
+    hb = ctypes.c_uint64()
+    if fn(buf.ctypes.data, buf.size, bits, _uptr(hdr), None, None, None, None, ctypes.byref(hb)) != 0:
+        raise ValueError("archive header is malformed or truncated")
+    cols = int(hdr[2])
+    sr = np.zeros(cols, np.uint32)
+    bs = np.zeros(cols + 1, np.uint32)
+    lohi = np.zeros(2, np.float32)
+    if fn(buf.ctypes.data, buf.size, bits, _uptr(hdr), _uptr(sr), _uptr(bs), _fptr(lohi), None, None) != 0:
+        raise ValueError("archive header is malformed or truncated")
+    m = CylinderMapping(int(hdr[0]), int(hdr[1]), cols, int(hdr[3]), int(hdr[4]), int(hdr[5]), sr, bs)
+    field = np.zeros(m.span, np.float32 if bits == 32 else np.uint16)
+    if fn(buf.ctypes.data, buf.size, bits, _uptr(hdr), _uptr(sr), _uptr(bs), _fptr(lohi), field.ctypes.data,
+          ctypes.byref(hb)) != 0:
+        raise ValueError("archive ends inside the voxel payload")
+    return ArchiveContents(m, float(lohi[0]), float(lohi[1]), int(hb.value), field)
+
+
+def convert_to_fp(m, field: np.ndarray, lo: float, hi: float) -> np.ndarray:
+    """convert_to_fp_kernel (transpose/convert_to_fp.cpp:11-47) of a float32 or uint16 span; other
+    entries 0."""
+    bits = 16 if field.dtype == np.uint16 else 32
+    raw = np.ascontiguousarray(field, dtype=np.uint16 if bits == 16 else np.float32)
+    out = np.zeros(raw.size, np.float32)
+    fn = lib().oracle_convert_to_fp
+    fn.argtypes = [ctypes.POINTER(OCyl), ctypes.c_int, ctypes.c_void_p, ctypes.c_float, ctypes.c_float,
+                   ctypes.POINTER(ctypes.c_float)]
+    oc = ocyl(m)
+    fn(ctypes.byref(oc), bits, raw.ctypes.data, float(lo), float(hi), _fptr(out))
+    return out
+
+
+def intensity_range(m, field: np.ndarray, tail: float) -> tuple[int, int, np.ndarray]:
+    """find_intensity_range (transpose/find_intensity_range.cpp:22-110): (lo, hi, 65536 counts)."""
+    raw = np.ascontiguousarray(field, dtype=np.uint16)
+    hist = np.zeros(65536, np.uint64)
+    fh = lib().oracle_u16_hist
+    fh.argtypes = [ctypes.POINTER(OCyl), ctypes.c_void_p, ctypes.c_void_p]
+    oc = ocyl(m)
+    fh(ctypes.byref(oc), raw.ctypes.data, hist.ctypes.data)
+    lo, hi = ctypes.c_uint16(), ctypes.c_uint16()
+    fr = lib().oracle_intensity_range
+    fr.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(ctypes.c_uint16), ctypes.POINTER(ctypes.c_uint16)]
+    fr(hist.ctypes.data, float(tail), ctypes.byref(lo), ctypes.byref(hi))
+    return int(lo.value), int(hi.value), hist
+
+
+def raw_box(m, field: np.ndarray) -> tuple[np.ndarray, tuple[int, int, int, int]]:
+    """The --rawout label box (potts-model/potts-model.cpp:184-217): (bytes [cols, rows, slices],
+    (slices, rows, cols, row_begin))."""
+    f = np.ascontiguousarray(field, dtype=np.float32)
+    dims = np.zeros(4, np.uint32)
+    fn = lib().oracle_raw_box
+    fn.argtypes = [ctypes.POINTER(OCyl), ctypes.POINTER(ctypes.c_float), ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32)]
+    oc = ocyl(m)
+    fn(ctypes.byref(oc), _fptr(f), None, _uptr(dims))
+    out = np.zeros(int(dims[0]) * int(dims[1]) * int(dims[2]), np.uint8)
+    fn(ctypes.byref(oc), _fptr(f), out.ctypes.data, _uptr(dims))
+    return out.reshape(int(dims[2]), int(dims[1]), int(dims[0])), tuple(int(x) for x in dims)
+
+
+def vtk_file(m, field: np.ndarray) -> bytes:
+    """The whole --rawout file (potts-model.cpp:218-241) around the oracle's raw box."""
+    box, (s, r, c, _) = raw_box(m, field)
+    head = ("<?xml version=\"1.0\"?>\n"
+            "<VTKFile type=\"ImageData\" byte_order=\"LittleEndian\">\n"
+            f"  <ImageData WholeExtent=\"0 {s - 1} 0 {r - 1} 0 {c - 1}\">\n"
+            f"    <Piece Extent=\"0 {s - 1} 0 {r - 1} 0 {c - 1}\">\n"
+            "      <PointData Scalars=\"labels\">\n"
+            "        <DataArray type=\"UInt8\" Name=\"labels\" format=\"appended\" offset=\"0\"/>\n"
+            "      </PointData>\n"
+            "    </Piece>\n"
+            "  </ImageData>\n"
+            "  <AppendedData encoding=\"raw\">\n_")
+    return (head.encode() + np.uint32(box.size & 0xffffffff).tobytes() + box.tobytes()
+            + b"\n  </AppendedData>\n</VTKFile>\n")
+
+
+def png_gray(m, field: np.ndarray, col: int) -> np.ndarray:
+    """write_png's grey levels (potts-model/potts-model.cpp:34-49) of column col: [rows, n_images]."""
+    f = np.ascontiguousarray(field, dtype=np.float32)
+    rows = m.row_end(col) - m.row_begin(col)
+    pix = np.zeros((rows, m.n_images), np.uint8)
+    fn = lib().oracle_png_gray
+    fn.argtypes = [ctypes.POINTER(OCyl), ctypes.POINTER(ctypes.c_float), ctypes.c_uint32, ctypes.c_void_p]
+    oc = ocyl(m)
+    fn(ctypes.byref(oc), _fptr(f), int(col), pix.ctypes.data)
+    return pix

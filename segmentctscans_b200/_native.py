@@ -60,6 +60,22 @@ class PottsBatchInfo(ctypes.Structure):
     ]
 
 
+class PottsArchiveInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_images", ctypes.c_uint32), ("rows", ctypes.c_uint32), ("cols", ctypes.c_uint32),
+        ("nstride", ctypes.c_uint32), ("col_begin", ctypes.c_uint32), ("col_end", ctypes.c_uint32),
+        ("span", ctypes.c_uint64), ("lo", ctypes.c_float), ("hi", ctypes.c_float),
+        ("header_bits", ctypes.c_uint64), ("voxels", ctypes.c_uint64), ("total_bytes", ctypes.c_uint64),
+    ]
+
+
+class PottsIoStats(ctypes.Structure):
+    _fields_ = [("kernel_ms", ctypes.c_double), ("launches", ctypes.c_int)]
+
+
+ELEM_F32, ELEM_U16 = 0, 1
+ELEMENTS = {"f32": ELEM_F32, "u16": ELEM_U16}
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _F = ctypes.c_float
@@ -120,6 +136,20 @@ SIGNATURES = {
     "potts_uv_hist_span": (_U64, [_U32]),
     "potts_uv_hist": (_I, [_P, _MP, _P, _P, _F, _F, _F, _F, _U32, _P]),
     "potts_uv_hist_auto": (_I, [_P, _MP, _P, _P, _U32, _P, _FP]),
+    "potts_archive_read_header": (_I, [_P, _U64, _I, ctypes.POINTER(PottsArchiveInfo), _P, _P]),
+    "potts_archive_size": (_I, [_MP, _I, ctypes.POINTER(_U64), ctypes.POINTER(_U64)]),
+    "potts_archive_load": (_I, [_P, _P, _U64, _I, _P, _U64, ctypes.POINTER(PottsArchiveInfo),
+                                ctypes.POINTER(PottsIoStats)]),
+    "potts_archive_save": (_I, [_P, _MP, _I, _P, _F, _F, _P, _U64, ctypes.POINTER(_U64),
+                                ctypes.POINTER(PottsIoStats)]),
+    "potts_convert_to_fp": (_I, [_P, _MP, _I, _P, _F, _F, _P]),
+    "potts_find_intensity_range": (_I, [_P, _MP, _P, ctypes.c_double, ctypes.POINTER(ctypes.c_uint16),
+                                        ctypes.POINTER(ctypes.c_uint16), _P]),
+    "potts_raw_labels_dims": (_I, [_MP, ctypes.POINTER(_U32), ctypes.POINTER(_U32), ctypes.POINTER(_U32),
+                                   ctypes.POINTER(_U32)]),
+    "potts_raw_labels": (_I, [_P, _MP, _P, _P]),
+    "potts_vtk_labels": (_I, [_P, _MP, _P, _P, _U64, ctypes.POINTER(_U64), ctypes.POINTER(PottsIoStats)]),
+    "potts_png_slice": (_I, [_P, _MP, _P, _U32, _P, _U64, ctypes.POINTER(_U64)]),
 }
 STATIC_MAX_COLS = 16384
 

@@ -19,6 +19,7 @@
 #include "kernels_tiled.cuh"
 #include "kernels_hist.cuh"
 #include "kernels_tv.cuh"
+#include "kernels_fieldio.cuh"
 #include "voxel.cuh"
 
 // Sets the message potts_last_error() returns on this thread; used by the
@@ -198,6 +199,7 @@ struct potts_context {
     bool mapping_valid = false;
     DevBuf lines, state, dq, energy, partial, host_u, host_res, host_labels, ustage, err;
     DevBuf hist;  // min/max partials and histogram counters of the label-finding inputs
+    DevBuf io, io_tables;  // archive payload / raw label box staging, mask tables of the box kernel
     float *pinned_dq = nullptr;
     // tiled-kernel tables: per column (depends on the mapping) and the work
     // items of the last (slab extent, tile shape) planned
@@ -935,6 +937,7 @@ int context_init(int device, void *stream, bool use_stream, potts_context **out)
 #include "adjoint.cuh"
 #include "batch.cuh"
 #include "label_inputs.cuh"
+#include "field_io.cuh"
 #include "stepper.cuh"
 
 // Work items, shared-memory size and the tensor maps of the two xi buffers (3 planes each,
@@ -1114,7 +1117,7 @@ void potts_context_destroy(potts_context *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (DevBuf *b : {&ctx->lines, &ctx->state, &ctx->dq, &ctx->energy, &ctx->partial, &ctx->host_u,
                       &ctx->host_res, &ctx->host_labels, &ctx->ustage, &ctx->err, &ctx->cols, &ctx->work, &ctx->vols,
-                      &ctx->hist})
+                      &ctx->hist, &ctx->io, &ctx->io_tables})
         if (b->p) cudaFree(b->p);
     if (ctx->pinned_dq) cudaFreeHost(ctx->pinned_dq);
     for (cudaEvent_t e : ctx->seg_ev) cudaEventDestroy(e);
@@ -1669,6 +1672,117 @@ int potts_uv_hist_auto(potts_context *ctx, const potts_mapping *map, const float
     POTTS_TRY(potts_min_max(ctx, map, d_u, &out_ranges[0], &out_ranges[1]));
     return potts_uv_hist(ctx, map, d_u, d_v, out_ranges[0], out_ranges[1], out_ranges[2], out_ranges[3], nbins,
                          out_hist);
+}
+
+int potts_archive_read_header(const uint8_t *bytes, uint64_t n_bytes, int elem, potts_archive_info *info,
+                              uint32_t *start_row, uint32_t *base)
+{
+    const int bits = elem_bits_of(elem);
+    if (!bits) return fail(POTTS_EINVAL, "unknown element type");
+    ArchiveHeader h;
+    POTTS_TRY(decode_header(bytes, n_bytes, bits, h));
+    fill_info(h, info);
+    if (start_row) std::memcpy(start_row, h.mc.start_row.data(), sizeof(uint32_t) * h.mc.m.cols);
+    if (base) std::memcpy(base, h.mc.base.data(), sizeof(uint32_t) * ((size_t)h.mc.m.cols + 1));
+    return POTTS_OK;
+}
+
+int potts_archive_size(const potts_mapping *map, int elem, uint64_t *total_bytes, uint64_t *header_bits)
+{
+    const int bits = elem_bits_of(elem);
+    if (!bits) return fail(POTTS_EINVAL, "unknown element type");
+    POTTS_TRY(validate_mapping(map));
+    BitWriter w;
+    encode_header(*map, bits, 0.0f, 0.0f, w);
+    const uint64_t voxels = (uint64_t)(map->base[map->cols] / map->nstride) * map->n_images;
+    if (total_bytes) *total_bytes = (w.bits + voxels * (uint64_t)bits + 7) / 8;
+    if (header_bits) *header_bits = w.bits;
+    return POTTS_OK;
+}
+
+int potts_archive_load(potts_context *ctx, const uint8_t *bytes, uint64_t n_bytes, int elem, void *d_field,
+                       uint64_t capacity, potts_archive_info *info, potts_io_stats *stats)
+{
+    io_stats_reset(stats);
+    const int bits = elem_bits_of(elem);
+    if (!ctx || !d_field) return fail(POTTS_EINVAL, "NULL argument");
+    if (!bits) return fail(POTTS_EINVAL, "unknown element type");
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    return archive_load_run(ctx, bytes, n_bytes, bits, d_field, capacity, info, stats);
+}
+
+int potts_archive_save(potts_context *ctx, const potts_mapping *map, int elem, const void *d_field, float lo,
+                       float hi, uint8_t *out, uint64_t capacity, uint64_t *out_bytes, potts_io_stats *stats)
+{
+    io_stats_reset(stats);
+    const int bits = elem_bits_of(elem);
+    if (!ctx) return fail(POTTS_EINVAL, "context is NULL");
+    if (!bits) return fail(POTTS_EINVAL, "unknown element type");
+    POTTS_TRY(validate_mapping(map));
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    return archive_save_run(ctx, map, bits, d_field, lo, hi, out, capacity, out_bytes, stats);
+}
+
+int potts_convert_to_fp(potts_context *ctx, const potts_mapping *map, int elem, const void *d_in, float lo, float hi,
+                        float *d_out)
+{
+    const int bits = elem_bits_of(elem);
+    if (!ctx || !d_in || !d_out) return fail(POTTS_EINVAL, "NULL argument");
+    if (!bits) return fail(POTTS_EINVAL, "unknown element type");
+    if (bits == 32 && d_in == (const void *)d_out) return fail(POTTS_EINVAL, "input and output must differ");
+    POTTS_TRY(validate_mapping(map));
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    return convert_to_fp_run(ctx, map, bits, d_in, lo, hi, d_out);
+}
+
+int potts_find_intensity_range(potts_context *ctx, const potts_mapping *map, const uint16_t *d_field,
+                               double tail_thr, uint16_t *out_lo, uint16_t *out_hi, uint64_t *out_hist)
+{
+    if (!ctx || !d_field || !out_lo || !out_hi) return fail(POTTS_EINVAL, "NULL argument");
+    if (!std::isfinite(tail_thr)) return fail(POTTS_EINVAL, "tail_thr must be finite");
+    POTTS_TRY(validate_mapping(map));
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    return intensity_range_run(ctx, map, d_field, tail_thr, out_lo, out_hi, out_hist);
+}
+
+int potts_raw_labels_dims(const potts_mapping *map, uint32_t *slices, uint32_t *rows, uint32_t *cols,
+                          uint32_t *row_begin)
+{
+    POTTS_TRY(validate_mapping(map));
+    uint32_t rb = 0, r = 0, c = 0;
+    POTTS_TRY(raw_box_dims(*map, &rb, &r, &c));
+    if (slices) *slices = map->n_images;
+    if (rows) *rows = r;
+    if (cols) *cols = c;
+    if (row_begin) *row_begin = rb;
+    return POTTS_OK;
+}
+
+int potts_raw_labels(potts_context *ctx, const potts_mapping *map, const float *d_field, uint8_t *d_box)
+{
+    if (!ctx || !d_field || !d_box) return fail(POTTS_EINVAL, "NULL argument");
+    POTTS_TRY(validate_mapping(map));
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    return raw_box_run(ctx, map, d_field, d_box);
+}
+
+int potts_vtk_labels(potts_context *ctx, const potts_mapping *map, const float *d_field, uint8_t *out,
+                     uint64_t capacity, uint64_t *out_bytes, potts_io_stats *stats)
+{
+    io_stats_reset(stats);
+    if (!ctx) return fail(POTTS_EINVAL, "context is NULL");
+    POTTS_TRY(validate_mapping(map));
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    return vtk_labels_run(ctx, map, d_field, out, capacity, out_bytes, stats);
+}
+
+int potts_png_slice(potts_context *ctx, const potts_mapping *map, const float *d_field, uint32_t col, uint8_t *out,
+                    uint64_t capacity, uint64_t *out_bytes)
+{
+    if (!ctx) return fail(POTTS_EINVAL, "context is NULL");
+    POTTS_TRY(validate_mapping(map));
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    return png_slice_run(ctx, map, d_field, col, out, capacity, out_bytes);
 }
 
 }  // extern "C"

@@ -535,3 +535,167 @@ def uv_hist_auto(ctx: CudaContext, mapping: CylinderMapping, u_ptr: int, v_ptr: 
                                                 ctypes.c_void_p(int(v_ptr)), int(nbins), hist.ctypes.data,
                                                 rng.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
     return hist, tuple(float(x) for x in rng)
+
+
+# ---- field archive (.bin), convert_to_fp, find_intensity_range, output writers ------------
+
+def _elem(elem: str) -> int:
+    if elem not in _native.ELEMENTS:
+        raise ValueError(f"unknown element type {elem!r}; one of {sorted(_native.ELEMENTS)}")
+    return _native.ELEMENTS[elem]
+
+
+def _bytes_ptr(data) -> tuple[np.ndarray, int]:
+    buf = np.frombuffer(data, np.uint8) if isinstance(data, (bytes, bytearray, memoryview)) else np.asarray(data)
+    if buf.dtype != np.uint8 or not buf.flags.c_contiguous:
+        buf = np.ascontiguousarray(buf).view(np.uint8)
+    return buf, buf.ctypes.data
+
+
+@dataclass
+class ArchiveInfo:
+    mapping: CylinderMapping
+    lo: float
+    hi: float
+    header_bits: int
+    voxels: int
+    total_bytes: int
+
+
+def archive_read_header(data, elem: str = "f32") -> ArchiveInfo:
+    """mapping_storage::load + Field<float>::load's lo/hi (include/layout_cylinder.h:259-312,
+    include/field.h:121-131): the mapping and sizes of a .bin archive (host only)."""
+    buf, ptr = _bytes_ptr(data)
+    lib = _native.host_lib()
+    info = _native.PottsArchiveInfo()
+    check(lib.potts_archive_read_header(ptr, buf.size, _elem(elem), ctypes.byref(info), None, None))
+    sr = np.zeros(info.cols, np.uint32)
+    bs = np.zeros(info.cols + 1, np.uint32)
+    check(lib.potts_archive_read_header(ptr, buf.size, _elem(elem), ctypes.byref(info), sr.ctypes.data,
+                                        bs.ctypes.data))
+    m = CylinderMapping(info.n_images, info.rows, info.cols, info.nstride, info.col_begin, info.col_end, sr, bs)
+    return ArchiveInfo(m, info.lo, info.hi, info.header_bits, info.voxels, info.total_bytes)
+
+
+def archive_size(mapping: CylinderMapping, elem: str = "f32") -> tuple[int, int]:
+    """(archive bytes, header bits) of a field with this mapping (host only)."""
+    tb, hb = ctypes.c_uint64(), ctypes.c_uint64()
+    check(_native.host_lib().potts_archive_size(ctypes.byref(mapping.as_c()), _elem(elem), ctypes.byref(tb),
+                                                ctypes.byref(hb)))
+    return int(tb.value), int(hb.value)
+
+
+def archive_load(ctx: CudaContext, data, elem: str, d_ptr: int, capacity: int) -> tuple[ArchiveInfo, float]:
+    """Field<T>::load (include/field.h:121-147) of host archive bytes into the device field at d_ptr
+    (float32 or uint16 elements, `capacity` of them); returns (header, unpack kernel ms)."""
+    buf, ptr = _bytes_ptr(data)
+    info = _native.PottsArchiveInfo()
+    st = _native.PottsIoStats()
+    check(_native.host_lib().potts_archive_load(ctx.handle, ptr, buf.size, _elem(elem), ctypes.c_void_p(int(d_ptr)),
+                                                int(capacity), ctypes.byref(info), ctypes.byref(st)))
+    hdr = archive_read_header(buf, elem)
+    return hdr, st.kernel_ms
+
+
+def archive_save(ctx: CudaContext, mapping: CylinderMapping, elem: str, d_ptr: int, lo: float = 0.0, hi: float = 0.0,
+                 out: Optional[np.ndarray] = None) -> tuple[np.ndarray, float]:
+    """Field<T>::save (include/field.h:92-119) of the device field at d_ptr: (archive bytes as uint8 array,
+    pack kernel ms).  `out` (uint8, e.g. pinned) receives the bytes when given."""
+    lib = _native.host_lib()
+    n = ctypes.c_uint64()
+    mc = mapping.as_c()
+    check(lib.potts_archive_save(ctx.handle, ctypes.byref(mc), _elem(elem), None, 0.0, 0.0, None, 0, ctypes.byref(n),
+                                 None))
+    if out is None:
+        out = np.zeros(int(n.value), np.uint8)
+    st = _native.PottsIoStats()
+    check(lib.potts_archive_save(ctx.handle, ctypes.byref(mc), _elem(elem), ctypes.c_void_p(int(d_ptr)), float(lo),
+                                 float(hi), out.ctypes.data, out.size, ctypes.byref(n), ctypes.byref(st)))
+    return out[: int(n.value)], st.kernel_ms
+
+
+def convert_to_fp(ctx: CudaContext, mapping: CylinderMapping, elem: str, in_ptr: int, lo: float, hi: float,
+                  out_ptr: int) -> None:
+    """convert_to_fp(ctx, in, lo, hi) (transpose/convert_to_fp.cpp:11-79) into the float32 field at
+    out_ptr; enqueued on the context's stream."""
+    check(_native.host_lib().potts_convert_to_fp(ctx.handle, ctypes.byref(mapping.as_c()), _elem(elem),
+                                                 ctypes.c_void_p(int(in_ptr)), float(lo), float(hi),
+                                                 ctypes.c_void_p(int(out_ptr))))
+
+
+def find_intensity_range(ctx: CudaContext, mapping: CylinderMapping, u16_ptr: int,
+                         tail_thr: float) -> tuple[int, int, np.ndarray]:
+    """find_intensity_range(ctx, field, tail_thr) (transpose/find_intensity_range.cpp:64-110) of a
+    uint16 device field: (lo, hi, the 65536 counts)."""
+    lo, hi = ctypes.c_uint16(), ctypes.c_uint16()
+    hist = np.zeros(65536, np.uint64)
+    check(_native.host_lib().potts_find_intensity_range(ctx.handle, ctypes.byref(mapping.as_c()),
+                                                        ctypes.c_void_p(int(u16_ptr)), float(tail_thr),
+                                                        ctypes.byref(lo), ctypes.byref(hi), hist.ctypes.data))
+    return int(lo.value), int(hi.value), hist
+
+
+def raw_labels_dims(mapping: CylinderMapping) -> tuple[int, int, int, int]:
+    """(slices, rows, cols, row_begin) of the raw label box (potts-model.cpp:186-202); host only."""
+    v = [ctypes.c_uint32() for _ in range(4)]
+    check(_native.host_lib().potts_raw_labels_dims(ctypes.byref(mapping.as_c()), *[ctypes.byref(x) for x in v]))
+    return tuple(int(x.value) for x in v)
+
+
+def raw_labels(ctx: CudaContext, mapping: CylinderMapping, f_ptr: int, box_ptr: int) -> None:
+    """The raw label box (potts-model.cpp:203-217) into device bytes at box_ptr (cols x rows x slices)."""
+    check(_native.host_lib().potts_raw_labels(ctx.handle, ctypes.byref(mapping.as_c()), ctypes.c_void_p(int(f_ptr)),
+                                              ctypes.c_void_p(int(box_ptr))))
+
+
+def vtk_labels(ctx: CudaContext, mapping: CylinderMapping, f_ptr: int,
+               out: Optional[np.ndarray] = None) -> tuple[np.ndarray, float]:
+    """The --rawout VTK file (potts-model.cpp:184-243) of the device field at f_ptr: (file bytes, box
+    kernel ms)."""
+    lib = _native.host_lib()
+    n = ctypes.c_uint64()
+    mc = mapping.as_c()
+    check(lib.potts_vtk_labels(ctx.handle, ctypes.byref(mc), ctypes.c_void_p(int(f_ptr)), None, 0, ctypes.byref(n),
+                               None))
+    if out is None:
+        out = np.zeros(int(n.value), np.uint8)
+    st = _native.PottsIoStats()
+    check(lib.potts_vtk_labels(ctx.handle, ctypes.byref(mc), ctypes.c_void_p(int(f_ptr)), out.ctypes.data, out.size,
+                               ctypes.byref(n), ctypes.byref(st)))
+    return out[: int(n.value)], st.kernel_ms
+
+
+def write_vtk_labels(ctx: CudaContext, mapping: CylinderMapping, f_ptr: int, path) -> None:
+    """Writes the --rawout file of potts-model (potts-model.cpp:184-243) to `path`."""
+    data, _ = vtk_labels(ctx, mapping, f_ptr)
+    with open(path, "wb") as fh:
+        fh.write(data.tobytes())
+
+
+def png_slice(ctx: CudaContext, mapping: CylinderMapping, f_ptr: int, col: int) -> bytes:
+    """write_png's image of column `col` (potts-model.cpp:34-49) as PNG bytes."""
+    lib = _native.host_lib()
+    n = ctypes.c_uint64()
+    mc = mapping.as_c()
+    check(lib.potts_png_slice(ctx.handle, ctypes.byref(mc), ctypes.c_void_p(int(f_ptr)), int(col), None, 0,
+                              ctypes.byref(n)))
+    out = np.zeros(int(n.value), np.uint8)
+    check(lib.potts_png_slice(ctx.handle, ctypes.byref(mc), ctypes.c_void_p(int(f_ptr)), int(col), out.ctypes.data,
+                              out.size, ctypes.byref(n)))
+    return out.tobytes()
+
+
+def png_slice_name(col: int, lam: float) -> str:
+    """The file name write_png uses (potts-model.cpp:48): "slice-{col} (𝜆 = {lam:07.3f}).png"."""
+    return f"slice-{int(col)} (\U0001d706 = {float(lam):07.3f}).png"
+
+
+def write_png(ctx: CudaContext, mapping: CylinderMapping, f_ptr: int, col: int, lam: float, directory=".") -> str:
+    """write_png(img, col, lambda) (potts-model.cpp:34-49): writes the slice PNG under the reference's
+    file name in `directory`; returns the path."""
+    import os
+
+    path = os.path.join(str(directory), png_slice_name(col, lam))
+    with open(path, "wb") as fh:
+        fh.write(png_slice(ctx, mapping, f_ptr, col))
+    return path
