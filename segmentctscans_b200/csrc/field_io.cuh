@@ -216,6 +216,11 @@ potts::IoLines io_lines(const potts_mapping &m)
     return g;
 }
 
+bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+// Lines of `per` voxels' worth of 16 bytes each (voxel count and stride multiples of `per`).
+bool lines_vec(const potts::IoLines &g, int per) { return g.ns % per == 0 && g.nstride % per == 0; }
+
 unsigned io_blocks(const potts_context *ctx, int64_t n_lines)
 {
     const int64_t want = (int64_t)std::max(ctx->n_sm, 1) * 8;
@@ -258,12 +263,22 @@ int archive_load_run(potts_context *ctx, const uint8_t *bytes, uint64_t n_bytes,
     POTTS_CUDA(cudaMemcpyAsync(d_words, bytes + first, payload, cudaMemcpyHostToDevice, ctx->stream));
     const potts::IoLines g = io_lines(h.mc.m);
     POTTS_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
-    if (bits == 32)
-        potts::archive_unpack_kernel<32><<<io_blocks(ctx, g.n_lines), potts::kIoThreads, 0, ctx->stream>>>(
-            g, reinterpret_cast<const uint32_t *>(d_words), (int)shift, static_cast<uint32_t *>(d_field));
-    else
-        potts::archive_unpack_kernel<16><<<io_blocks(ctx, g.n_lines), potts::kIoThreads, 0, ctx->stream>>>(
-            g, reinterpret_cast<const uint32_t *>(d_words), (int)shift, static_cast<uint16_t *>(d_field));
+    const unsigned nb = io_blocks(ctx, g.n_lines);
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(d_words);
+    const bool vec = aligned16(d_field) && lines_vec(g, 128 / bits);
+    if (bits == 32) {
+        uint32_t *o = static_cast<uint32_t *>(d_field);
+        if (vec)
+            potts::archive_unpack_kernel<32, true><<<nb, potts::kIoThreads, 0, ctx->stream>>>(g, w, (int)shift, o);
+        else
+            potts::archive_unpack_kernel<32, false><<<nb, potts::kIoThreads, 0, ctx->stream>>>(g, w, (int)shift, o);
+    } else {
+        uint16_t *o = static_cast<uint16_t *>(d_field);
+        if (vec)
+            potts::archive_unpack_kernel<16, true><<<nb, potts::kIoThreads, 0, ctx->stream>>>(g, w, (int)shift, o);
+        else
+            potts::archive_unpack_kernel<16, false><<<nb, potts::kIoThreads, 0, ctx->stream>>>(g, w, (int)shift, o);
+    }
     POTTS_CUDA(cudaGetLastError());
     POTTS_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     ctx->total_launches += 1;
@@ -314,12 +329,22 @@ int convert_to_fp_run(potts_context *ctx, const potts_mapping *map, int bits, co
 {
     const potts::IoLines g = io_lines(*map);
     if (g.n_lines == 0) return POTTS_OK;
-    if (bits == 32)
-        potts::convert_to_fp_kernel<float><<<io_blocks(ctx, g.n_lines), potts::kIoThreads, 0, ctx->stream>>>(
-            g, static_cast<const float *>(d_in), lo, hi, d_out);
-    else
-        potts::convert_to_fp_kernel<uint16_t><<<io_blocks(ctx, g.n_lines), potts::kIoThreads, 0, ctx->stream>>>(
-            g, static_cast<const uint16_t *>(d_in), lo, hi, d_out);
+    const unsigned nb = io_blocks(ctx, g.n_lines);
+    const bool vec = aligned16(d_in) && aligned16(d_out) && lines_vec(g, 4);
+    if (bits == 32) {
+        const float *in = static_cast<const float *>(d_in);
+        if (vec)
+            potts::convert_to_fp_kernel<float, true><<<nb, potts::kIoThreads, 0, ctx->stream>>>(g, in, lo, hi, d_out);
+        else
+            potts::convert_to_fp_kernel<float, false><<<nb, potts::kIoThreads, 0, ctx->stream>>>(g, in, lo, hi, d_out);
+    } else {
+        const uint16_t *in = static_cast<const uint16_t *>(d_in);
+        if (vec)
+            potts::convert_to_fp_kernel<uint16_t, true><<<nb, potts::kIoThreads, 0, ctx->stream>>>(g, in, lo, hi, d_out);
+        else
+            potts::convert_to_fp_kernel<uint16_t, false><<<nb, potts::kIoThreads, 0, ctx->stream>>>(g, in, lo, hi,
+                                                                                                  d_out);
+    }
     ctx->total_launches += 1;
     POTTS_CUDA(cudaGetLastError());
     return POTTS_OK;
@@ -339,8 +364,9 @@ int intensity_range_run(potts_context *ctx, const potts_mapping *map, const uint
     POTTS_CUDA(cudaMemsetAsync(d_hist, 0, sizeof(unsigned long long) * kU16Bins, ctx->stream));
     if (g.n_lines > 0) {
         const int smem = (int)sizeof(uint32_t) * potts::kU16Slice;
-        POTTS_CUDA(cudaFuncSetAttribute(potts::u16_hist_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        smem));
+        const bool vec = ((uintptr_t)d_f & 7u) == 0 && lines_vec(g, 4);
+        void *kfn = vec ? (void *)potts::u16_hist_cluster_kernel<true> : (void *)potts::u16_hist_cluster_kernel<false>;
+        POTTS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3((unsigned)std::max(potts::kU16Cluster,
                                               std::max(ctx->n_sm, 1) / potts::kU16Cluster * potts::kU16Cluster));
@@ -348,15 +374,17 @@ int intensity_range_run(potts_context *ctx, const potts_mapping *map, const uint
         cfg.dynamicSmemBytes = (size_t)smem;
         cfg.stream = ctx->stream;
         int clusters = 0;
-        if (cudaOccupancyMaxActiveClusters(&clusters, (void *)potts::u16_hist_cluster_kernel, &cfg) != cudaSuccess ||
-            clusters < 1) {
+        if (cudaOccupancyMaxActiveClusters(&clusters, kfn, &cfg) != cudaSuccess || clusters < 1) {
             cudaGetLastError();
             clusters = 1;
         }
         const int64_t want = (g.n_lines + potts::kU16Cluster - 1) / potts::kU16Cluster;
         clusters = (int)std::max<int64_t>(1, std::min<int64_t>(clusters, want));
-        potts::u16_hist_cluster_kernel<<<(unsigned)(clusters * potts::kU16Cluster), potts::kIoThreads, smem,
-                                         ctx->stream>>>(g, d_f, d_hist);
+        const unsigned blocks = (unsigned)(clusters * potts::kU16Cluster);
+        if (vec)
+            potts::u16_hist_cluster_kernel<true><<<blocks, potts::kIoThreads, smem, ctx->stream>>>(g, d_f, d_hist);
+        else
+            potts::u16_hist_cluster_kernel<false><<<blocks, potts::kIoThreads, smem, ctx->stream>>>(g, d_f, d_hist);
         ctx->total_launches += 1;
         POTTS_CUDA(cudaGetLastError());
     }
@@ -422,7 +450,10 @@ int raw_box_run(potts_context *ctx, const potts_mapping *map, const float *d_f, 
     g.ns = (int)map->n_images;
     g.nstride = (int)map->nstride;
     POTTS_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
-    potts::raw_box_kernel<<<io_blocks(ctx, g.box_lines), potts::kIoThreads, 0, ctx->stream>>>(g, d_f, d_box);
+    if (aligned16(d_f) && ((uintptr_t)d_box & 3u) == 0 && g.ns % 4 == 0)
+        potts::raw_box_kernel<true><<<io_blocks(ctx, g.box_lines), potts::kIoThreads, 0, ctx->stream>>>(g, d_f, d_box);
+    else
+        potts::raw_box_kernel<false><<<io_blocks(ctx, g.box_lines), potts::kIoThreads, 0, ctx->stream>>>(g, d_f, d_box);
     POTTS_CUDA(cudaGetLastError());
     POTTS_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     ctx->total_launches += 1;

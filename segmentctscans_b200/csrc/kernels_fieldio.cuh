@@ -45,10 +45,8 @@ struct IoLines {
 };
 
 // Word w of the staged payload in stream order (the bytes were loaded little-endian).
-__device__ __forceinline__ uint32_t stream_word(const uint32_t *__restrict__ w, int64_t i)
-{
-    return __byte_perm(__ldcs(w + i), 0u, 0x0123u);
-}
+__device__ __forceinline__ uint32_t bswap32(uint32_t v) { return __byte_perm(v, 0u, 0x0123u); }
+__device__ __forceinline__ uint32_t stream_word(const uint32_t *__restrict__ w, int64_t i) { return bswap32(__ldg(w + i)); }
 
 // The stream unit that starts `shift` bits into staged unit i (i counts kBits-wide units).
 template <int kBits>
@@ -65,17 +63,42 @@ __device__ __forceinline__ typename IoElem<kBits>::T unpack_unit(const uint32_t 
 }
 
 // Payload -> field (Field<T>::load, include/field.h:121-147): every in-mask voxel of every line;
-// the padding n >= ns is not written.
-template <int kBits>
+// the padding n >= ns is not written.  kVec: each thread turns 16 staged bytes (one uint4 load plus
+// the next word) into 16 output bytes (4 FP32 voxels or 8 uint16 voxels); needs lines whose voxel
+// count and stride are multiples of 16 bytes' worth and a 16-byte aligned field.
+template <int kBits, bool kVec>
 __global__ void __launch_bounds__(kIoThreads) archive_unpack_kernel(IoLines g, const uint32_t *__restrict__ words,
                                                                      int shift,
                                                                      typename IoElem<kBits>::T *__restrict__ out)
 {
+    constexpr int kPer = 128 / kBits;  // voxels per 16 bytes
     for (int64_t L = blockIdx.x; L < g.n_lines; L += gridDim.x) {
         const int64_t i0 = L * g.ns;
         typename IoElem<kBits>::T *dst = out + L * g.nstride;
+        if constexpr (kVec) {
+            const uint32_t *wl = words + i0 * kBits / 32;  // 16-byte aligned: i0 is a multiple of kPer
+            for (int q = threadIdx.x; q < g.ns / kPer; q += kIoThreads) {
+                const uint4 a = __ldg(reinterpret_cast<const uint4 *>(wl) + q);
+                const uint32_t w0 = bswap32(a.x), w1 = bswap32(a.y), w2 = bswap32(a.z), w3 = bswap32(a.w);
+                const uint32_t w4 = bswap32(__ldg(wl + 4 * q + 4));
+                const unsigned sh = (unsigned)shift;
+                uint4 r;
+                if constexpr (kBits == 32) {
+                    r = make_uint4(__funnelshift_l(w1, w0, sh), __funnelshift_l(w2, w1, sh), __funnelshift_l(w3, w2, sh),
+                                   __funnelshift_l(w4, w3, sh));
+                } else {
+                    // 16-bit units: the shifted words hold units (2k, 2k+1) as (high, low) halves
+                    const uint32_t s0 = __funnelshift_l(w1, w0, sh), s1 = __funnelshift_l(w2, w1, sh),
+                                   s2 = __funnelshift_l(w3, w2, sh), s3 = __funnelshift_l(w4, w3, sh);
+                    r = make_uint4(__byte_perm(s0, 0u, 0x1032u), __byte_perm(s1, 0u, 0x1032u),
+                                   __byte_perm(s2, 0u, 0x1032u), __byte_perm(s3, 0u, 0x1032u));
+                }
+                reinterpret_cast<uint4 *>(dst)[q] = r;
+            }
+        } else {
 #pragma unroll 4
-        for (int n = threadIdx.x; n < g.ns; n += kIoThreads) dst[n] = unpack_unit<kBits>(words, i0 + n, shift);
+            for (int n = threadIdx.x; n < g.ns; n += kIoThreads) dst[n] = unpack_unit<kBits>(words, i0 + n, shift);
+        }
     }
 }
 
@@ -115,7 +138,15 @@ __global__ void __launch_bounds__(kIoThreads) archive_pack_kernel(IoLines g,
 
 // convert_to_fp_kernel (transpose/convert_to_fp.cpp:11-47): 0 at or below lo, 1 at or above hi,
 // else (v - lo) / (hi - lo) in single precision.
-template <typename T>
+__device__ __forceinline__ float to_unit(float v, float lo, float hi, float range)
+{
+    if (v <= lo) return 0.0f;
+    if (v >= hi) return 1.0f;
+    return __fdiv_rn(__fsub_rn(v, lo), range);
+}
+
+// kVec: 4 voxels per thread (lines of a multiple of 4 voxels, 16-byte aligned fields).
+template <typename T, bool kVec>
 __global__ void __launch_bounds__(kIoThreads) convert_to_fp_kernel(IoLines g, const T *__restrict__ in, float lo,
                                                                     float hi, float *__restrict__ out)
 {
@@ -123,50 +154,63 @@ __global__ void __launch_bounds__(kIoThreads) convert_to_fp_kernel(IoLines g, co
     for (int64_t L = blockIdx.x; L < g.n_lines; L += gridDim.x) {
         const T *src = in + L * g.nstride;
         float *dst = out + L * g.nstride;
+        if constexpr (kVec) {
+            for (int q = threadIdx.x; q < g.ns / 4; q += kIoThreads) {
+                float4 v;
+                if constexpr (sizeof(T) == 2) {
+                    const uint2 p = __ldg(reinterpret_cast<const uint2 *>(src) + q);
+                    v = make_float4((float)(p.x & 0xffffu), (float)(p.x >> 16), (float)(p.y & 0xffffu),
+                                    (float)(p.y >> 16));
+                } else {
+                    v = __ldg(reinterpret_cast<const float4 *>(src) + q);
+                }
+                reinterpret_cast<float4 *>(dst)[q] = make_float4(to_unit(v.x, lo, hi, range), to_unit(v.y, lo, hi, range),
+                                                                 to_unit(v.z, lo, hi, range), to_unit(v.w, lo, hi, range));
+            }
+        } else {
 #pragma unroll 4
-        for (int n = threadIdx.x; n < g.ns; n += kIoThreads) {
-            const float v = (float)__ldcs(src + n);
-            float r;
-            if (v <= lo)
-                r = 0.0f;
-            else if (v >= hi)
-                r = 1.0f;
-            else
-                r = __fdiv_rn(__fsub_rn(v, lo), range);
-            __stcs(dst + n, r);
+            for (int n = threadIdx.x; n < g.ns; n += kIoThreads) dst[n] = to_unit((float)__ldg(src + n), lo, hi, range);
         }
     }
 }
 
 // histogram_kernel + histogram_reduce_kernel (transpose/find_intensity_range.cpp:22-62): the
-// 65536-bin histogram of a uint16 field.  The counters live in the distributed shared memory of
-// a two-block cluster (block rank k owns bins [32768 k, 32768 (k + 1)), 128 KB each); lanes of a
-// warp holding the same value add once; each cluster flushes its non-zero bins to the 64-bit
-// global counts.
+// 65536-bin histogram of a uint16 field.  A two-block cluster reads the same lines; block rank k
+// counts the values whose top bit is k into its own 32768 shared-memory counters (128 KB), so every
+// value is counted once, with a shared-memory atomic, and the second read of a line is served by L2.
+// Each block flushes its non-zero bins to the 64-bit global counts.
 constexpr int kU16Cluster = 2;
 constexpr int kU16Slice = 32768;
 
+template <bool kVec>
 __global__ void __cluster_dims__(kU16Cluster, 1, 1) __launch_bounds__(kIoThreads, 1)
     u16_hist_cluster_kernel(IoLines g, const uint16_t *__restrict__ f, unsigned long long *__restrict__ ghist)
 {
     namespace cg = cooperative_groups;
-    cg::cluster_group cluster = cg::this_cluster();
     extern __shared__ uint32_t sh_u16[];
     for (int i = threadIdx.x; i < kU16Slice; i += blockDim.x) sh_u16[i] = 0u;
-    cluster.sync();
-    for (int64_t L = blockIdx.x; L < g.n_lines; L += gridDim.x) {
+    __syncthreads();
+    const uint32_t half = cg::this_cluster().block_rank();
+    const int64_t pair = blockIdx.x / kU16Cluster, pairs = gridDim.x / kU16Cluster;
+    auto count = [&](uint32_t v) {
+        if ((v >> 15) == half) atomicAdd(sh_u16 + (v & 0x7fffu), 1u);
+    };
+    for (int64_t L = pair; L < g.n_lines; L += pairs) {
         const uint16_t *line = f + L * g.nstride;
-        for (int n0 = 0; n0 < g.ns; n0 += blockDim.x) {  // whole warps, for the lane combining
-            const int n = n0 + threadIdx.x;
-            const int id = n < g.ns ? (int)__ldcs(line + n) : -1;
-            warp_count(id, [&](int b, uint32_t c) {
-                uint32_t *dst = cluster.map_shared_rank(sh_u16, (unsigned)(b / kU16Slice));
-                atomicAdd(dst + (b % kU16Slice), c);
-            });
+        if constexpr (kVec) {
+            for (int q = threadIdx.x; q < g.ns / 4; q += kIoThreads) {
+                const uint2 p = __ldg(reinterpret_cast<const uint2 *>(line) + q);
+                count(p.x & 0xffffu);
+                count(p.x >> 16);
+                count(p.y & 0xffffu);
+                count(p.y >> 16);
+            }
+        } else {
+            for (int n = threadIdx.x; n < g.ns; n += kIoThreads) count(__ldg(line + n));
         }
     }
-    cluster.sync();
-    const int base = (int)cluster.block_rank() * kU16Slice;
+    __syncthreads();
+    const int base = (int)half * kU16Slice;
     for (int i = threadIdx.x; i < kU16Slice; i += blockDim.x)
         if (sh_u16[i]) atomicAdd(ghist + base + i, (unsigned long long)sh_u16[i]);
 }
@@ -189,6 +233,8 @@ __device__ __forceinline__ uint8_t label_byte(float v)
     return (uint8_t)(s >= 255.0f ? 255 : (s <= 0.0f ? 0 : (int)s));
 }
 
+// kVec: 4 voxels per thread (a float4 in, 4 bytes out): slices a multiple of 4, aligned buffers.
+template <bool kVec>
 __global__ void __launch_bounds__(kIoThreads) raw_box_kernel(BoxGeom g, const float *__restrict__ f,
                                                               uint8_t *__restrict__ out)
 {
@@ -198,10 +244,21 @@ __global__ void __launch_bounds__(kIoThreads) raw_box_kernel(BoxGeom g, const fl
         const int64_t sr = g.start_row[col];
         const int64_t cnt = (int64_t)(g.base[col + 1] - g.base[col]) / g.nstride;
         uint8_t *dst = out + b * g.ns;
-        if (cnt > 0 && row >= sr && row < sr + cnt) {
-            const float *src = f + (int64_t)g.base[col] + (row - sr) * g.nstride;
+        const bool inside = cnt > 0 && row >= sr && row < sr + cnt;
+        const float *src = inside ? f + (int64_t)g.base[col] + (row - sr) * g.nstride : f;
+        if constexpr (kVec) {
+            for (int q = threadIdx.x; q < g.ns / 4; q += kIoThreads) {
+                uint32_t r = 0xffffffffu;
+                if (inside) {
+                    const float4 v = __ldg(reinterpret_cast<const float4 *>(src) + q);
+                    r = (uint32_t)label_byte(v.x) | ((uint32_t)label_byte(v.y) << 8) |
+                        ((uint32_t)label_byte(v.z) << 16) | ((uint32_t)label_byte(v.w) << 24);
+                }
+                reinterpret_cast<uint32_t *>(dst)[q] = r;
+            }
+        } else if (inside) {
 #pragma unroll 4
-            for (int n = threadIdx.x; n < g.ns; n += kIoThreads) dst[n] = label_byte(__ldcs(src + n));
+            for (int n = threadIdx.x; n < g.ns; n += kIoThreads) dst[n] = label_byte(__ldg(src + n));
         } else {
             for (int n = threadIdx.x; n < g.ns; n += kIoThreads) dst[n] = 255;
         }

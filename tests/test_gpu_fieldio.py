@@ -12,8 +12,10 @@ from tests._cases import phantom_volume, random_volume
 
 pytestmark = pytest.mark.gpu
 
-# (n_images, rows, cols, r): the header lengths of these mappings put the payload at several bit
-# offsets within a byte
+# (n_images, rows, cols, r): the header lengths of these mappings put the payload at each of the
+# bit offsets 1, 3, 5, 7 within a byte (a header is 2 cols + 9 Exp-Golomb codes of odd length, plus
+# 64 bits for FP32 fields, so its length is always odd); n_images 64 and 300 take the vectorised
+# kernels, the others the per-voxel ones
 GEOMS = [(5, 6, 7, 2.6), (33, 12, 10, 5.2), (1, 9, 9, 4.0), (3, 5, 40, 1.3), (300, 14, 13, 6.1), (64, 40, 41, 19.7),
          (17, 23, 19, 10.4), (2, 31, 30, 14.2), (129, 11, 12, 5.3), (7, 50, 48, 22.9)]
 
@@ -68,7 +70,23 @@ def test_archive_load_bitwise(cuda_device, oracle_mod, elem):
             assert np.array_equal(mv(got).view(np.uint8), mv(ref.field).view(np.uint8))
             pad = got.reshape(m.n_lines, m.nstride)[:, m.n_images:]
             assert np.array_equal(pad.view(np.uint8), sentinel.reshape(m.n_lines, m.nstride)[:, m.n_images:].view(np.uint8))
-    assert len(shifts) >= 5, shifts
+    assert shifts == {1, 3, 5, 7}, shifts
+
+
+@pytest.mark.parametrize("elem", ["f32", "u16"])
+def test_archive_load_unaligned_field(cuda_device, oracle_mod, elem):
+    """A field pointer off a 16-byte boundary takes the per-voxel kernel: the same values."""
+    torch = _torch()
+    m = CylinderMapping.cylinder(64, 40, 41, 19.7)
+    f = _field(m, elem, 7)
+    data, _ = oracle_mod.archive_encode(m, f, elem)
+    with potts.make_context(0) as ctx:
+        buf = torch.zeros(m.span + 8, dtype=torch.int16 if elem == "u16" else torch.float32, device="cuda")
+        potts.archive_load(ctx, data, elem, buf[1:].data_ptr(), m.span)
+        torch.cuda.synchronize()
+    got = buf[1:1 + m.span].cpu().numpy().view(np.uint16 if elem == "u16" else np.float32)
+    mv = m.mask_values
+    assert np.array_equal(mv(got).view(np.uint8), mv(f).view(np.uint8))
 
 
 @pytest.mark.parametrize("elem", ["f32", "u16"])
@@ -102,10 +120,11 @@ def test_archive_round_trip_and_errors(cuda_device, oracle_mod):
             potts.archive_save(ctx, m, "f32", d.data_ptr(), out=np.zeros(len(data) - 1, np.uint8))
 
 
+@pytest.mark.parametrize("n", [70, 64], ids=["per-voxel", "vector"])
 @pytest.mark.parametrize("elem", ["f32", "u16"])
-def test_convert_to_fp_bitwise(cuda_device, oracle_mod, elem):
+def test_convert_to_fp_bitwise(cuda_device, oracle_mod, elem, n):
     torch = _torch()
-    m, u, _ = random_volume(70, 22, 21, 10.3, 3, seed=9)
+    m, u, _ = random_volume(n, 22, 21, 10.3, 3, seed=9)
     if elem == "f32":
         f = (u * 2.0 - 0.5).astype(np.float32)
         lo, hi = -0.25, 1.1
@@ -122,9 +141,9 @@ def test_convert_to_fp_bitwise(cuda_device, oracle_mod, elem):
     assert np.array_equal(m.mask_values(out.cpu().numpy()), m.mask_values(ref))
 
 
-@pytest.mark.parametrize("tail", [0.0, 1e-3, 0.02, 0.5])
-def test_find_intensity_range(cuda_device, oracle_mod, tail):
-    m, u, _ = random_volume(96, 40, 41, 19.2, 3, seed=11)
+@pytest.mark.parametrize("n,tail", [(96, 0.0), (96, 1e-3), (96, 0.02), (97, 0.5), (97, 1e-3)])
+def test_find_intensity_range(cuda_device, oracle_mod, n, tail):
+    m, u, _ = random_volume(n, 40, 41, 19.2, 3, seed=11)
     rng = np.random.default_rng(5)
     w = np.clip(u * 40000 + rng.normal(8000, 2500, m.span), 0, 65535).astype(np.uint16)
     w[: m.nstride] = 65535  # the top bin is used

@@ -173,3 +173,13 @@ def test_oracle_raw_box_and_dims(native_lib, oracle_mod):
     f = oracle_mod.vtk_file(m, v)
     assert f.startswith(b"<?xml version=\"1.0\"?>\n<VTKFile type=\"ImageData\"")
     assert f.endswith(b"\n  </AppendedData>\n</VTKFile>\n")
+
+
+def test_header_length_is_odd(native_lib):
+    """Every code of the header has odd length and there are 2 cols + 9 of them (64 more bits for FP32
+    fields): the voxel payload always starts at an odd bit offset within a byte."""
+    for geom in [(5, 6, 7, 2.6), (33, 12, 10, 5.2), (64, 40, 41, 19.7), (1, 5, 40, 1.3), (1024, 768, 768, 370.0)]:
+        m = CylinderMapping.cylinder(*geom)
+        for elem in ("f32", "u16"):
+            _, hb = potts.archive_size(m, elem)
+            assert hb % 2 == 1 and hb == len(header_bits(m, elem))
