@@ -364,13 +364,13 @@ int intensity_range_run(potts_context *ctx, const potts_mapping *map, const uint
     POTTS_CUDA(cudaMemsetAsync(d_hist, 0, sizeof(unsigned long long) * kU16Bins, ctx->stream));
     if (g.n_lines > 0) {
         const int smem = (int)sizeof(uint32_t) * potts::kU16Slice;
-        const bool vec = ((uintptr_t)d_f & 7u) == 0 && lines_vec(g, 4);
+        const bool vec = aligned16(d_f) && lines_vec(g, 8);
         void *kfn = vec ? (void *)potts::u16_hist_cluster_kernel<true> : (void *)potts::u16_hist_cluster_kernel<false>;
         POTTS_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3((unsigned)std::max(potts::kU16Cluster,
                                               std::max(ctx->n_sm, 1) / potts::kU16Cluster * potts::kU16Cluster));
-        cfg.blockDim = dim3(potts::kIoThreads);
+        cfg.blockDim = dim3(potts::kU16Threads);
         cfg.dynamicSmemBytes = (size_t)smem;
         cfg.stream = ctx->stream;
         int clusters = 0;
@@ -378,13 +378,13 @@ int intensity_range_run(potts_context *ctx, const potts_mapping *map, const uint
             cudaGetLastError();
             clusters = 1;
         }
-        const int64_t want = (g.n_lines + potts::kU16Cluster - 1) / potts::kU16Cluster;
+        const int64_t want = (g.n_lines + 31) / 32;  // a warp per line in each block of a cluster
         clusters = (int)std::max<int64_t>(1, std::min<int64_t>(clusters, want));
         const unsigned blocks = (unsigned)(clusters * potts::kU16Cluster);
         if (vec)
-            potts::u16_hist_cluster_kernel<true><<<blocks, potts::kIoThreads, smem, ctx->stream>>>(g, d_f, d_hist);
+            potts::u16_hist_cluster_kernel<true><<<blocks, potts::kU16Threads, smem, ctx->stream>>>(g, d_f, d_hist);
         else
-            potts::u16_hist_cluster_kernel<false><<<blocks, potts::kIoThreads, smem, ctx->stream>>>(g, d_f, d_hist);
+            potts::u16_hist_cluster_kernel<false><<<blocks, potts::kU16Threads, smem, ctx->stream>>>(g, d_f, d_hist);
         ctx->total_launches += 1;
         POTTS_CUDA(cudaGetLastError());
     }

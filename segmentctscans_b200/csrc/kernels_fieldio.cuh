@@ -145,17 +145,21 @@ __device__ __forceinline__ float to_unit(float v, float lo, float hi, float rang
     return __fdiv_rn(__fsub_rn(v, lo), range);
 }
 
-// kVec: 4 voxels per thread (lines of a multiple of 4 voxels, 16-byte aligned fields).
+// One warp per line, so that each lane has several independent loads in flight.  kVec: 4 voxels
+// per lane and step (lines of a multiple of 4 voxels, 16-byte aligned fields).
 template <typename T, bool kVec>
 __global__ void __launch_bounds__(kIoThreads) convert_to_fp_kernel(IoLines g, const T *__restrict__ in, float lo,
                                                                     float hi, float *__restrict__ out)
 {
     const float range = __fsub_rn(hi, lo);
-    for (int64_t L = blockIdx.x; L < g.n_lines; L += gridDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (kIoThreads / 32);
+    for (int64_t L = (int64_t)blockIdx.x * (kIoThreads / 32) + (threadIdx.x >> 5); L < g.n_lines; L += warps) {
         const T *src = in + L * g.nstride;
         float *dst = out + L * g.nstride;
         if constexpr (kVec) {
-            for (int q = threadIdx.x; q < g.ns / 4; q += kIoThreads) {
+#pragma unroll 8
+            for (int q = lane; q < g.ns / 4; q += 32) {
                 float4 v;
                 if constexpr (sizeof(T) == 2) {
                     const uint2 p = __ldg(reinterpret_cast<const uint2 *>(src) + q);
@@ -169,7 +173,7 @@ __global__ void __launch_bounds__(kIoThreads) convert_to_fp_kernel(IoLines g, co
             }
         } else {
 #pragma unroll 4
-            for (int n = threadIdx.x; n < g.ns; n += kIoThreads) dst[n] = to_unit((float)__ldg(src + n), lo, hi, range);
+            for (int n = lane; n < g.ns; n += 32) dst[n] = to_unit((float)__ldg(src + n), lo, hi, range);
         }
     }
 }
@@ -178,12 +182,14 @@ __global__ void __launch_bounds__(kIoThreads) convert_to_fp_kernel(IoLines g, co
 // 65536-bin histogram of a uint16 field.  A two-block cluster reads the same lines; block rank k
 // counts the values whose top bit is k into its own 32768 shared-memory counters (128 KB), so every
 // value is counted once, with a shared-memory atomic, and the second read of a line is served by L2.
-// Each block flushes its non-zero bins to the 64-bit global counts.
+// One block of 1024 threads per multiprocessor, one warp per line; each block flushes its non-zero
+// bins to the 64-bit global counts.  kVec: 8 values per lane and step (16-byte loads).
 constexpr int kU16Cluster = 2;
 constexpr int kU16Slice = 32768;
+constexpr int kU16Threads = 1024;
 
 template <bool kVec>
-__global__ void __cluster_dims__(kU16Cluster, 1, 1) __launch_bounds__(kIoThreads, 1)
+__global__ void __cluster_dims__(kU16Cluster, 1, 1) __launch_bounds__(kU16Threads, 1)
     u16_hist_cluster_kernel(IoLines g, const uint16_t *__restrict__ f, unsigned long long *__restrict__ ghist)
 {
     namespace cg = cooperative_groups;
@@ -191,22 +197,29 @@ __global__ void __cluster_dims__(kU16Cluster, 1, 1) __launch_bounds__(kIoThreads
     for (int i = threadIdx.x; i < kU16Slice; i += blockDim.x) sh_u16[i] = 0u;
     __syncthreads();
     const uint32_t half = cg::this_cluster().block_rank();
-    const int64_t pair = blockIdx.x / kU16Cluster, pairs = gridDim.x / kU16Cluster;
+    constexpr int kWarps = kU16Threads / 32;
+    const int lane = threadIdx.x & 31;
+    const int64_t pairs = gridDim.x / kU16Cluster;
     auto count = [&](uint32_t v) {
         if ((v >> 15) == half) atomicAdd(sh_u16 + (v & 0x7fffu), 1u);
     };
-    for (int64_t L = pair; L < g.n_lines; L += pairs) {
+    for (int64_t L = (blockIdx.x / kU16Cluster) * kWarps + (threadIdx.x >> 5); L < g.n_lines; L += pairs * kWarps) {
         const uint16_t *line = f + L * g.nstride;
         if constexpr (kVec) {
-            for (int q = threadIdx.x; q < g.ns / 4; q += kIoThreads) {
-                const uint2 p = __ldg(reinterpret_cast<const uint2 *>(line) + q);
+#pragma unroll 4
+            for (int q = lane; q < g.ns / 8; q += 32) {
+                const uint4 p = __ldg(reinterpret_cast<const uint4 *>(line) + q);
                 count(p.x & 0xffffu);
                 count(p.x >> 16);
                 count(p.y & 0xffffu);
                 count(p.y >> 16);
+                count(p.z & 0xffffu);
+                count(p.z >> 16);
+                count(p.w & 0xffffu);
+                count(p.w >> 16);
             }
         } else {
-            for (int n = threadIdx.x; n < g.ns; n += kIoThreads) count(__ldg(line + n));
+            for (int n = lane; n < g.ns; n += 32) count(__ldg(line + n));
         }
     }
     __syncthreads();
@@ -233,21 +246,27 @@ __device__ __forceinline__ uint8_t label_byte(float v)
     return (uint8_t)(s >= 255.0f ? 255 : (s <= 0.0f ? 0 : (int)s));
 }
 
-// kVec: 4 voxels per thread (a float4 in, 4 bytes out): slices a multiple of 4, aligned buffers.
+// One warp per box line.  kVec: 4 voxels per lane and step (a float4 in, 4 bytes out): slices a
+// multiple of 4, aligned buffers.  Box lines are fewer than 2^32 (rows and columns are below 2^16).
 template <bool kVec>
 __global__ void __launch_bounds__(kIoThreads) raw_box_kernel(BoxGeom g, const float *__restrict__ f,
                                                               uint8_t *__restrict__ out)
 {
-    for (int64_t b = blockIdx.x; b < g.box_lines; b += gridDim.x) {
-        const uint32_t col = g.col_begin + (uint32_t)(b / g.row_size);
-        const int64_t row = (int64_t)g.row_begin + (b % g.row_size);
-        const int64_t sr = g.start_row[col];
-        const int64_t cnt = (int64_t)(g.base[col + 1] - g.base[col]) / g.nstride;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (kIoThreads / 32);
+    for (int64_t b = (int64_t)blockIdx.x * (kIoThreads / 32) + (threadIdx.x >> 5); b < g.box_lines; b += warps) {
+        const uint32_t bl = (uint32_t)b;
+        const uint32_t col = g.col_begin + bl / (uint32_t)g.row_size;
+        const int64_t row = (int64_t)g.row_begin + bl % (uint32_t)g.row_size;
+        const int64_t sr = __ldg(g.start_row + col);
+        const uint32_t b0 = __ldg(g.base + col), b1 = __ldg(g.base + col + 1);
+        const int64_t cnt = (int64_t)(b1 - b0) / g.nstride;
         uint8_t *dst = out + b * g.ns;
         const bool inside = cnt > 0 && row >= sr && row < sr + cnt;
-        const float *src = inside ? f + (int64_t)g.base[col] + (row - sr) * g.nstride : f;
+        const float *src = inside ? f + (int64_t)b0 + (row - sr) * g.nstride : f;
         if constexpr (kVec) {
-            for (int q = threadIdx.x; q < g.ns / 4; q += kIoThreads) {
+#pragma unroll 8
+            for (int q = lane; q < g.ns / 4; q += 32) {
                 uint32_t r = 0xffffffffu;
                 if (inside) {
                     const float4 v = __ldg(reinterpret_cast<const float4 *>(src) + q);
@@ -258,9 +277,9 @@ __global__ void __launch_bounds__(kIoThreads) raw_box_kernel(BoxGeom g, const fl
             }
         } else if (inside) {
 #pragma unroll 4
-            for (int n = threadIdx.x; n < g.ns; n += kIoThreads) dst[n] = label_byte(__ldg(src + n));
+            for (int n = lane; n < g.ns; n += 32) dst[n] = label_byte(__ldg(src + n));
         } else {
-            for (int n = threadIdx.x; n < g.ns; n += kIoThreads) dst[n] = 255;
+            for (int n = lane; n < g.ns; n += 32) dst[n] = 255;
         }
     }
 }
