@@ -31,6 +31,13 @@ voxel-iterations of forward + backward per second; the gradients of c, lambda
 and --fd-coords random u coordinates are checked against FP64 central
 differences of the oracle (step 1e-6 relative; also 1e-4 for u).
 
+--workload tv is TV-L2 denoising (chambolle(), 768^2 x 1024, 150 iterations).
+--workload fieldio is the field I/O around the solve on the same core: the
+.bin archive of an FP32 field saved and loaded, a uint16 scan's
+find_intensity_range + convert_to_fp, and the --rawout VTK label box; value =
+in-mask voxels per second through those five kernels, e2e = the same through
+host bytes.  tvmid / fieldiomid / mid / mid4 are 384^2 x 256 profiling sizes.
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Under torchrun each rank solves its own phantom (weak scaling, no data-path
 collective: the ranks' volumes are independent).
