@@ -195,3 +195,28 @@ def test_png_slice(cuda_device, oracle_mod, tmp_path):
     assert path.endswith(f"slice-{col} (\U0001d706 = 030.000).png")
     with open(path, "rb") as fh:
         assert fh.read() == png
+
+
+def test_empty_mask_and_single_slice_archives(cuda_device, oracle_mod):
+    """Edge cases of the payload: no voxel at all (the archive is the header) and one slice per line."""
+    torch = _torch()
+    with potts.make_context(0) as ctx:
+        empty = CylinderMapping.cylinder(4, 10, 10, 0.3)
+        dummy = torch.zeros(16, dtype=torch.float32, device="cuda")
+        data, _ = potts.archive_save(ctx, empty, "f32", dummy.data_ptr(), 1.0, 2.0)
+        ref, _ = oracle_mod.archive_encode(empty, np.zeros(0, np.float32), "f32", 1.0, 2.0)
+        assert data.tobytes() == ref
+        info, _ = potts.archive_load(ctx, ref, "f32", dummy.data_ptr(), 0)
+        assert info.voxels == 0 and (info.lo, info.hi) == (1.0, 2.0)
+        for elem in ("f32", "u16"):
+            m = CylinderMapping.cylinder(1, 33, 31, 15.2)
+            f = _field(m, elem, 3)
+            d = _device_u16(f) if elem == "u16" else _device_f32(f)
+            got, _ = potts.archive_save(ctx, m, elem, d.data_ptr())
+            ref, _ = oracle_mod.archive_encode(m, f, elem)
+            assert got.tobytes() == ref
+            back = torch.zeros_like(d)
+            potts.archive_load(ctx, ref, elem, back.data_ptr(), m.span)
+            torch.cuda.synchronize()
+            b = back.cpu().numpy().view(np.uint16 if elem == "u16" else np.float32)
+            assert np.array_equal(m.mask_values(b).view(np.uint8), m.mask_values(f).view(np.uint8))

@@ -183,3 +183,27 @@ def test_header_length_is_odd(native_lib):
         for elem in ("f32", "u16"):
             _, hb = potts.archive_size(m, elem)
             assert hb % 2 == 1 and hb == len(header_bits(m, elem))
+
+
+def test_empty_mask_header(native_lib, oracle_mod):
+    """A radius that keeps no row: col_begin stays ~0 and every table entry is ~0 or 0; the archive is
+    the header alone and parses back."""
+    m = CylinderMapping.cylinder(4, 10, 10, 0.3)
+    assert m.span == 0 and m.col_begin == 0xFFFFFFFF and m.col_end == 0
+    for elem in ("f32", "u16"):
+        data, hb = oracle_mod.archive_encode(m, np.zeros(0, np.float32 if elem == "f32" else np.uint16), elem)
+        assert data == archive_bits(m, np.zeros(0, np.float32 if elem == "f32" else np.uint16), elem)
+        info = potts.archive_read_header(data, elem)
+        assert info.voxels == 0 and info.total_bytes == len(data) == (hb + 7) // 8
+        assert info.mapping.col_begin == 0xFFFFFFFF and np.array_equal(info.mapping.start_row, m.start_row)
+        assert potts.archive_size(m, elem) == (len(data), hb)
+    with pytest.raises(PottsError):
+        potts.raw_labels_dims(m)
+
+
+def test_header_value_beyond_32_bits_is_rejected(native_lib):
+    bits = ue_bits(2**32) + "".join(ue_bits(v) for v in (4, 4, 32, 0, 4, 4)) + "1" * 200
+    bits += "0" * (-len(bits) % 8)
+    with pytest.raises(PottsError) as e:
+        potts.archive_read_header(bytes(int(bits[i:i + 8], 2) for i in range(0, len(bits), 8)), "u16")
+    assert e.value.status == POTTS_EINVAL
