@@ -510,19 +510,23 @@ int vtk_labels_run(potts_context *ctx, const potts_mapping *map, const float *d_
 // ---- PNG slice (potts-model.cpp:34-49): the lines of one column as an 8-bit grey image, rows
 // down, slices across, gray = saturate(round-half-even(255 |x|^(1/2.2))) computed in double.  The
 // image is written as a PNG with stored (uncompressed) deflate blocks.
-uint32_t crc32_update(uint32_t crc, const uint8_t *p, size_t n)
-{
-    static uint32_t table[256];
-    static bool init = false;
-    if (!init) {
+// CRC-32 of PNG chunks (reflected polynomial 0xedb88320); the table is built once, thread-safely.
+struct Crc32Table {
+    uint32_t t[256];
+    Crc32Table()
+    {
         for (uint32_t i = 0; i < 256; ++i) {
             uint32_t c = i;
             for (int k = 0; k < 8; ++k) c = (c & 1u) ? 0xedb88320u ^ (c >> 1) : c >> 1;
-            table[i] = c;
+            t[i] = c;
         }
-        init = true;
     }
-    for (size_t i = 0; i < n; ++i) crc = table[(crc ^ p[i]) & 0xffu] ^ (crc >> 8);
+};
+
+uint32_t crc32_update(uint32_t crc, const uint8_t *p, size_t n)
+{
+    static const Crc32Table table;
+    for (size_t i = 0; i < n; ++i) crc = table.t[(crc ^ p[i]) & 0xffu] ^ (crc >> 8);
     return crc;
 }
 
