@@ -274,10 +274,21 @@ int ensure(potts_context *ctx, DevBuf &b, size_t bytes)
     return POTTS_OK;
 }
 
+// Frees a context buffer once the stream has finished with it.
+int release(potts_context *ctx, DevBuf &b)
+{
+    if (!b.p) return POTTS_OK;
+    POTTS_CUDA(cudaStreamSynchronize(ctx->stream));
+    POTTS_CUDA(cudaFree(b.p));
+    b.p = nullptr;
+    b.bytes = 0;
+    return POTTS_OK;
+}
+
 size_t cached_bytes(const potts_context *ctx)
 {
     return ctx->state.bytes + ctx->partial.bytes + ctx->host_u.bytes + ctx->host_res.bytes + ctx->host_labels.bytes +
-           ctx->ustage.bytes + ctx->hist.bytes;
+           ctx->ustage.bytes + ctx->hist.bytes + ctx->io.bytes + ctx->io_tables.bytes;
 }
 
 int upload_lines(potts_context *ctx, const potts_mapping *map)
@@ -750,7 +761,10 @@ int solve_k(potts_context *ctx, const float *d_u, const float *ci, float lam, fl
     const int planes = state_planes(K, o.variant);
 
     // Slab planner (potts-min-partition.cpp:560-577): as many n-slices as the
-    // free memory holds, halo = iters on each side of a slab.
+    // free memory holds, halo = iters on each side of a slab.  The field-I/O
+    // staging buffers are scratch of earlier calls: the solve gets their memory.
+    POTTS_TRY(release(ctx, ctx->io));
+    POTTS_TRY(release(ctx, ctx->io_tables));
     size_t free_b = 0, total_b = 0;
     POTTS_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t margin = size_t(512) << 20;

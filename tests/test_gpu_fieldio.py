@@ -220,3 +220,27 @@ def test_empty_mask_and_single_slice_archives(cuda_device, oracle_mod):
             torch.cuda.synchronize()
             b = back.cpu().numpy().view(np.uint16 if elem == "u16" else np.float32)
             assert np.array_equal(m.mask_values(b).view(np.uint8), m.mask_values(f).view(np.uint8))
+
+
+def test_archive_to_solve_to_vtk_pipeline(cuda_device, oracle_mod):
+    """potts-model's path on one context: read the .bin archive (Field<float>, lo/hi), solve with the
+    labels normalised by lo/hi (potts-model.cpp:145-148), write the --rawout file.  The staging
+    buffers of the archive call are released when the solve plans its slabs."""
+    torch = _torch()
+    m, u, ci, _ = phantom_volume(32, 14.0, seed=4)
+    lo, hi = 0.0125, 0.0625
+    raw_labels = [lo + c * (hi - lo) for c in ci]
+    data, _ = oracle_mod.archive_encode(m, u, "f32", lo, hi)
+    tau = potts.reference_tau()
+    with potts.make_context(0, stream=torch.cuda.current_stream().cuda_stream) as ctx:
+        du = torch.zeros(m.span, dtype=torch.float32, device="cuda")
+        info, _ = potts.archive_load(ctx, data, "f32", du.data_ptr(), m.span)
+        cn = [(np.float32(x) - np.float32(info.lo)) / (np.float32(info.hi) - np.float32(info.lo)) for x in raw_labels]
+        res = torch.zeros(m.span, dtype=torch.float32, device="cuda")
+        potts.solve_device(ctx, info.mapping, du.data_ptr(), cn, 30.0, tau, tau, 30, res_ptr=res.data_ptr())
+        vtk, _ = potts.vtk_labels(ctx, info.mapping, res.data_ptr())
+        torch.cuda.synchronize()
+    ref = oracle_mod.solve(m, u, [float(c) for c in cn], 30.0, tau, tau, 30, precision="f32")
+    got = res.cpu().numpy()
+    assert np.array_equal(m.mask_values(got), m.mask_values(ref.res.astype(np.float32)))
+    assert vtk.tobytes() == oracle_mod.vtk_file(m, got)
