@@ -309,12 +309,18 @@ int archive_save_run(potts_context *ctx, const potts_mapping *map, int bits, con
     POTTS_TRY(ensure(ctx, ctx->io, (payload + 15) / 16 * 16 + 16));
     uint8_t *d_words = static_cast<uint8_t *>(ctx->io.p);
     POTTS_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
-    if (bits == 32)
-        potts::archive_pack_kernel<32><<<io_blocks(ctx, g.n_lines), potts::kIoThreads, 0, ctx->stream>>>(
-            g, static_cast<const uint32_t *>(d_field), (int)shift, reinterpret_cast<uint32_t *>(d_words));
-    else
-        potts::archive_pack_kernel<16><<<io_blocks(ctx, g.n_lines), potts::kIoThreads, 0, ctx->stream>>>(
+    const unsigned nb = io_blocks(ctx, g.n_lines);
+    if (bits == 32) {
+        const uint32_t *in = static_cast<const uint32_t *>(d_field);
+        uint32_t *o = reinterpret_cast<uint32_t *>(d_words);
+        if (aligned16(d_field) && lines_vec(g, 4))
+            potts::archive_pack_kernel<32, true><<<nb, potts::kIoThreads, 0, ctx->stream>>>(g, in, (int)shift, o);
+        else
+            potts::archive_pack_kernel<32, false><<<nb, potts::kIoThreads, 0, ctx->stream>>>(g, in, (int)shift, o);
+    } else {
+        potts::archive_pack_kernel<16, false><<<nb, potts::kIoThreads, 0, ctx->stream>>>(
             g, static_cast<const uint16_t *>(d_field), (int)shift, reinterpret_cast<uint16_t *>(d_words));
+    }
     POTTS_CUDA(cudaGetLastError());
     POTTS_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     ctx->total_launches += 1;
@@ -339,7 +345,14 @@ int convert_to_fp_run(potts_context *ctx, const potts_mapping *map, int bits, co
             potts::convert_to_fp_kernel<float, false><<<nb, potts::kIoThreads, 0, ctx->stream>>>(g, in, lo, hi, d_out);
     } else {
         const uint16_t *in = static_cast<const uint16_t *>(d_in);
-        if (vec)
+        const uint64_t items = (uint64_t)g.n_lines * (uint64_t)(g.ns / 8);
+        if (aligned16(d_in) && aligned16(d_out) && lines_vec(g, 8) && items < (uint64_t{1} << 32)) {
+            const unsigned fb = (unsigned)std::max<uint64_t>(
+                1, std::min<uint64_t>((items + potts::kIoThreads - 1) / potts::kIoThreads,
+                                      (uint64_t)std::max(ctx->n_sm, 1) * 8));
+            potts::convert_u16_flat_kernel<<<fb, potts::kIoThreads, 0, ctx->stream>>>(g, (uint32_t)items, in, lo, hi,
+                                                                                     d_out);
+        } else if (vec)
             potts::convert_to_fp_kernel<uint16_t, true><<<nb, potts::kIoThreads, 0, ctx->stream>>>(g, in, lo, hi, d_out);
         else
             potts::convert_to_fp_kernel<uint16_t, false><<<nb, potts::kIoThreads, 0, ctx->stream>>>(g, in, lo, hi,

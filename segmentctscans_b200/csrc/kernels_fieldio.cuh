@@ -110,24 +110,40 @@ __device__ __forceinline__ uint16_t to_stream_order(uint16_t v) { return (uint16
 // low `shift` bits of voxel i - 1 and the high kBits - shift bits of voxel i (voxel -1 is 0: those
 // bits belong to the header, which the host merges into byte 0).  With shift > 0 one more unit
 // carries the low bits of the last voxel.
-template <int kBits>
+// kVec (FP32 only): 4 voxels per thread, one 16-byte load and one 16-byte store (lines of a
+// multiple of 4 voxels, 16-byte aligned field).
+template <int kBits, bool kVec>
 __global__ void __launch_bounds__(kIoThreads) archive_pack_kernel(IoLines g,
                                                                    const typename IoElem<kBits>::T *__restrict__ in,
                                                                    int shift,
                                                                    typename IoElem<kBits>::T *__restrict__ out)
 {
     using T = typename IoElem<kBits>::T;
+    static_assert(!kVec || kBits == 32, "vector packing of FP32 archives");
     for (int64_t L = blockIdx.x; L < g.n_lines; L += gridDim.x) {
         const int64_t i0 = L * g.ns;
         const T *src = in + L * g.nstride;
         // the voxel before the line's first one: the last voxel of the previous line
         const T before = L > 0 ? in[(L - 1) * g.nstride + g.ns - 1] : (T)0;
+        if constexpr (kVec) {
+            const unsigned sh = (unsigned)shift;
+            for (int q = threadIdx.x; q < g.ns / 4; q += kIoThreads) {
+                const uint4 v = __ldg(reinterpret_cast<const uint4 *>(src) + q);
+                const uint32_t p = q > 0 ? __ldg(src + 4 * q - 1) : (uint32_t)before;
+                // unit k = low `shift` bits of voxel k-1, then the high bits of voxel k
+                const uint4 u = make_uint4(__funnelshift_r(v.x, p, sh), __funnelshift_r(v.y, v.x, sh),
+                                           __funnelshift_r(v.z, v.y, sh), __funnelshift_r(v.w, v.z, sh));
+                reinterpret_cast<uint4 *>(out + i0)[q] =
+                    make_uint4(bswap32(u.x), bswap32(u.y), bswap32(u.z), bswap32(u.w));
+            }
+        } else {
 #pragma unroll 4
-        for (int n = threadIdx.x; n < g.ns; n += kIoThreads) {
-            const uint32_t v = src[n];
-            const uint32_t p = n > 0 ? (uint32_t)src[n - 1] : (uint32_t)before;
-            const uint32_t u = shift ? ((v >> shift) | (p << (kBits - shift))) : v;
-            out[i0 + n] = to_stream_order((T)u);
+            for (int n = threadIdx.x; n < g.ns; n += kIoThreads) {
+                const uint32_t v = src[n];
+                const uint32_t p = n > 0 ? (uint32_t)src[n - 1] : (uint32_t)before;
+                const uint32_t u = shift ? ((v >> shift) | (p << (kBits - shift))) : v;
+                out[i0 + n] = to_stream_order((T)u);
+            }
         }
     }
     if (shift && blockIdx.x == 0 && threadIdx.x == 0 && g.n_lines > 0) {
@@ -143,6 +159,27 @@ __device__ __forceinline__ float to_unit(float v, float lo, float hi, float rang
     if (v <= lo) return 0.0f;
     if (v >= hi) return 1.0f;
     return __fdiv_rn(__fsub_rn(v, lo), range);
+}
+
+// uint16 -> FP32 over a flat range of 8-voxel items (item = line * per_line + q): every thread
+// has a 16-byte load and two 16-byte stores in flight, whatever the line length (lines of a
+// multiple of 8 voxels and of stride, 16-byte aligned fields, fewer than 2^32 items).
+__global__ void __launch_bounds__(kIoThreads) convert_u16_flat_kernel(IoLines g, uint32_t items,
+                                                                       const uint16_t *__restrict__ in, float lo,
+                                                                       float hi, float *__restrict__ out)
+{
+    const float range = __fsub_rn(hi, lo);
+    const uint32_t per_line = (uint32_t)g.ns / 8u;
+    const uint64_t stride = (uint64_t)gridDim.x * kIoThreads;
+    for (uint64_t it = (uint64_t)blockIdx.x * kIoThreads + threadIdx.x; it < items; it += stride) {
+        const uint32_t L = (uint32_t)it / per_line, q = (uint32_t)it - L * per_line;
+        const uint4 p = __ldg(reinterpret_cast<const uint4 *>(in + (int64_t)L * g.nstride) + q);
+        float4 *dst = reinterpret_cast<float4 *>(out + (int64_t)L * g.nstride) + 2 * q;
+        dst[0] = make_float4(to_unit((float)(p.x & 0xffffu), lo, hi, range), to_unit((float)(p.x >> 16), lo, hi, range),
+                             to_unit((float)(p.y & 0xffffu), lo, hi, range), to_unit((float)(p.y >> 16), lo, hi, range));
+        dst[1] = make_float4(to_unit((float)(p.z & 0xffffu), lo, hi, range), to_unit((float)(p.z >> 16), lo, hi, range),
+                             to_unit((float)(p.w & 0xffffu), lo, hi, range), to_unit((float)(p.w >> 16), lo, hi, range));
+    }
 }
 
 // One block per line (a pure stream: fewer, longer concurrent streams measured faster at
