@@ -345,18 +345,7 @@ int convert_to_fp_run(potts_context *ctx, const potts_mapping *map, int bits, co
             potts::convert_to_fp_kernel<float, false><<<nb, potts::kIoThreads, 0, ctx->stream>>>(g, in, lo, hi, d_out);
     } else {
         const uint16_t *in = static_cast<const uint16_t *>(d_in);
-        const uint64_t items = (uint64_t)g.n_lines * (uint64_t)(g.ns / 8);
-        if (aligned16(d_in) && aligned16(d_out) && lines_vec(g, 8) && items < (uint64_t{1} << 32)) {
-            const unsigned fb = (unsigned)std::max<uint64_t>(
-                1, std::min<uint64_t>((items + potts::kIoThreads - 1) / potts::kIoThreads,
-                                      (uint64_t)std::max(ctx->n_sm, 1) * 8));
-            POTTS_TRY(ensure(ctx, ctx->lut, sizeof(float) * 65536));
-            float *lut = static_cast<float *>(ctx->lut.p);
-            potts::u16_lut_kernel<<<65536 / potts::kIoThreads, potts::kIoThreads, 0, ctx->stream>>>(lo, hi, lut);
-            potts::convert_u16_lut_kernel<<<fb, potts::kIoThreads, 0, ctx->stream>>>(g, (uint32_t)items, in, lut,
-                                                                                    d_out);
-            ctx->total_launches += 1;
-        } else if (vec)
+        if (vec)
             potts::convert_to_fp_kernel<uint16_t, true><<<nb, potts::kIoThreads, 0, ctx->stream>>>(g, in, lo, hi, d_out);
         else
             potts::convert_to_fp_kernel<uint16_t, false><<<nb, potts::kIoThreads, 0, ctx->stream>>>(g, in, lo, hi,

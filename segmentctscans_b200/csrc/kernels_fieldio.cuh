@@ -161,39 +161,10 @@ __device__ __forceinline__ float to_unit(float v, float lo, float hi, float rang
     return __fdiv_rn(__fsub_rn(v, lo), range);
 }
 
-// A uint16 voxel has 65536 possible values, so its FP32 result is a table entry: u16_lut_kernel
-// evaluates the same expression (to_unit, one IEEE division) once per value, and the conversion
-// becomes a lookup (the 256 KB table stays in L1/L2), bit-identical to dividing per voxel.
-__global__ void __launch_bounds__(kIoThreads) u16_lut_kernel(float lo, float hi, float *__restrict__ lut)
-{
-    const float range = __fsub_rn(hi, lo);
-    const int v = blockIdx.x * kIoThreads + threadIdx.x;
-    if (v < 65536) lut[v] = to_unit((float)v, lo, hi, range);
-}
-
-// uint16 -> FP32 through the table, over a flat range of 8-voxel items (item = line * per_line +
-// q): every thread has a 16-byte load and two 16-byte stores in flight, whatever the line length
-// (lines of a multiple of 8 voxels and of stride, 16-byte aligned fields, fewer than 2^32 items).
-__global__ void __launch_bounds__(kIoThreads) convert_u16_lut_kernel(IoLines g, uint32_t items,
-                                                                      const uint16_t *__restrict__ in,
-                                                                      const float *__restrict__ lut,
-                                                                      float *__restrict__ out)
-{
-    const uint32_t per_line = (uint32_t)g.ns / 8u;
-    const uint64_t stride = (uint64_t)gridDim.x * kIoThreads;
-    for (uint64_t it = (uint64_t)blockIdx.x * kIoThreads + threadIdx.x; it < items; it += stride) {
-        const uint32_t L = (uint32_t)it / per_line, q = (uint32_t)it - L * per_line;
-        const uint4 p = __ldg(reinterpret_cast<const uint4 *>(in + (int64_t)L * g.nstride) + q);
-        float4 *dst = reinterpret_cast<float4 *>(out + (int64_t)L * g.nstride) + 2 * q;
-        dst[0] = make_float4(__ldg(lut + (p.x & 0xffffu)), __ldg(lut + (p.x >> 16)), __ldg(lut + (p.y & 0xffffu)),
-                             __ldg(lut + (p.y >> 16)));
-        dst[1] = make_float4(__ldg(lut + (p.z & 0xffffu)), __ldg(lut + (p.z >> 16)), __ldg(lut + (p.w & 0xffffu)),
-                             __ldg(lut + (p.w >> 16)));
-    }
-}
-
-// One block per line (a pure stream: fewer, longer concurrent streams measured faster at
-// 768^2 x 1024 than one warp per line).  kVec: 4 voxels per thread (lines of a multiple of 4
+// One block per line.  At 768^2 x 1024 (uint16 in, FP32 out: 2 B read, 4 B written per voxel)
+// this measured faster than one warp per line, than a flat range of 8-voxel items, and than a
+// table of the 65536 uint16 results in place of the division: the write-heavy stream, not the
+// arithmetic, is the limit.  kVec: 4 voxels per thread (lines of a multiple of 4
 // voxels, 16-byte aligned fields).
 template <typename T, bool kVec>
 __global__ void __launch_bounds__(kIoThreads) convert_to_fp_kernel(IoLines g, const T *__restrict__ in, float lo,

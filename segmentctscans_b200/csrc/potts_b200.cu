@@ -200,7 +200,6 @@ struct potts_context {
     DevBuf lines, state, dq, energy, partial, host_u, host_res, host_labels, ustage, err;
     DevBuf hist;  // min/max partials and histogram counters of the label-finding inputs
     DevBuf io, io_tables;  // archive payload / raw label box staging, mask tables of the box kernel
-    DevBuf lut;            // convert_to_fp's table of the 65536 uint16 values
     float *pinned_dq = nullptr;
     // tiled-kernel tables: per column (depends on the mapping) and the work
     // items of the last (slab extent, tile shape) planned
@@ -1132,7 +1131,7 @@ void potts_context_destroy(potts_context *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (DevBuf *b : {&ctx->lines, &ctx->state, &ctx->dq, &ctx->energy, &ctx->partial, &ctx->host_u,
                       &ctx->host_res, &ctx->host_labels, &ctx->ustage, &ctx->err, &ctx->cols, &ctx->work, &ctx->vols,
-                      &ctx->hist, &ctx->io, &ctx->io_tables, &ctx->lut})
+                      &ctx->hist, &ctx->io, &ctx->io_tables})
         if (b->p) cudaFree(b->p);
     if (ctx->pinned_dq) cudaFreeHost(ctx->pinned_dq);
     for (cudaEvent_t e : ctx->seg_ev) cudaEventDestroy(e);

@@ -120,7 +120,7 @@ def test_archive_round_trip_and_errors(cuda_device, oracle_mod):
             potts.archive_save(ctx, m, "f32", d.data_ptr(), out=np.zeros(len(data) - 1, np.uint8))
 
 
-@pytest.mark.parametrize("n", [70, 68, 64], ids=["per-voxel", "vector", "flat-u16"])
+@pytest.mark.parametrize("n", [70, 68, 64], ids=["per-voxel", "vector-68", "vector-64"])
 @pytest.mark.parametrize("elem", ["f32", "u16"])
 def test_convert_to_fp_bitwise(cuda_device, oracle_mod, elem, n):
     torch = _torch()
