@@ -36,7 +36,9 @@ differences of the oracle (step 1e-6 relative; also 1e-4 for u).
 .bin archive of an FP32 field saved and loaded, a uint16 scan's
 find_intensity_range + convert_to_fp, and the --rawout VTK label box; value =
 in-mask voxels per second through those five kernels, e2e = the same through
-host bytes.  tvmid / fieldiomid / mid / mid4 are 384^2 x 256 profiling sizes.
+host bytes.  --workload labels times the label-finding inputs (min_max,
+grad_magn, calc_hist, uv_hist) on the same core.  tvmid / fieldiomid /
+labelsmid / mid / mid4 are 384^2 x 256 profiling sizes.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Under torchrun each rank solves its own phantom (weak scaling, no data-path
@@ -82,7 +84,7 @@ def parse_args():
     p.add_argument("--no-storage-compare", action="store_true",
                    help="skip the FP32-plain / BF16 / FP16 comparison solves")
     p.add_argument("--workload", choices=["config1", "config2", "config3", "config4", "config0", "mid", "mid4", "tv", "tvmid",
-                            "fieldio", "fieldiomid"],
+                            "fieldio", "fieldiomid", "labels", "labelsmid"],
                    default="config1",
                    help="config1: 768x768x1024 r=370 (the benchmark); config0: 128^3 r=60; "
                         "mid: 384x384x256 r=180 (profiling size, state > L2)")
@@ -1037,6 +1039,130 @@ def run_fieldio(args, dist_: Dist) -> None:
     dist_.close()
 
 
+def run_labels(args, dist_: Dist) -> None:
+    """Label-finding inputs (the GPU steps before the solve: min_max, grad_magn, calc_hist, uv_hist)
+    on the 768^2 x 1024 core.  value = in-mask voxels per second through the four calls of one step;
+    each call's device time (CUDA events around it on the context's stream, including its small
+    result copy) against its algorithmic bytes."""
+    import torch
+
+    from segmentctscans_b200 import potts
+    from segmentctscans_b200.phantom import config1_phantom, make_phantom
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    dev = torch.device("cuda", dist_.local)
+    torch.cuda.set_device(dev)
+    dist_.init("nccl")
+    if args.workload == "labelsmid":
+        ph = make_phantom(256, 384, 384, 180.0, seed=dist_.rank, radius_range=(6.0, 30.0), noise=7e-3, device=dev)
+    else:
+        ph = config1_phantom(seed=dist_.rank, device=dev)
+    m, u = ph.mapping, ph.u
+    vox = m.data_size
+    stream = torch.cuda.current_stream(dev)
+    ctx = potts.make_context(dev.index, stream=stream.cuda_stream)
+    v = torch.empty_like(u)
+
+    def step():
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+        e[0].record(stream)
+        potts.min_max(ctx, m, u.data_ptr())
+        e[1].record(stream)
+        potts.grad_magn(ctx, m, u.data_ptr(), v.data_ptr())
+        e[2].record(stream)
+        potts.calc_hist_auto(ctx, m, u.data_ptr(), 1024)
+        e[3].record(stream)
+        potts.uv_hist_auto(ctx, m, u.data_ptr(), v.data_ptr(), 512)
+        e[4].record(stream)
+        torch.cuda.synchronize(dev)
+        return {k: e[i].elapsed_time(e[i + 1]) for i, k in enumerate(("min_max", "grad_magn", "calc_hist_auto",
+                                                                          "uv_hist_auto"))}
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    dist_.barrier()
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    times = [step() for _ in range(args.steps)]
+    torch.cuda.synchronize(dev)
+    dist_.barrier()
+    clk = clocks.stop()
+    avg = {k: sum(t[k] for t in times) / len(times) for k in times[0]}
+    t_max = dist_.reduce(sum(avg.values()) / 1000.0 * args.steps, "max")
+    value = dist_.reduce(float(vox) * args.steps, "sum") / t_max / 1e9
+    # algorithmic bytes per call: min_max reads u; grad_magn reads u (neighbours from cache) and
+    # writes v; calc_hist_auto = min_max + histogram, two reads of u; uv_hist_auto = the min/max of v
+    # and of u, then the histogram of (u, v): reads v, u, then u and v
+    algo = {"min_max": 4 * vox, "grad_magn": 8 * vox, "calc_hist_auto": 8 * vox, "uv_hist_auto": 16 * vox}
+    peaks = measured_peaks()
+    kernels = {k: {"avg_ms": round(avg[k], 4), "gbs": round(algo[k] / (avg[k] / 1000.0) / 1e9, 1),
+                   "frac": round(algo[k] / (avg[k] / 1000.0) / 1e9 / peaks["hbm_gbs"], 4),
+                   "bytes_per_call": algo[k]} for k in avg}
+    roofline = {"bound": "hbm", "achieved": kernels["grad_magn"]["gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": kernels["grad_magn"]["frac"], "traffic": None, "kernel": "potts::grad_magn_kernel",
+                "bytes_per_voxel": 8, "avg_launch_ms": kernels["grad_magn"]["avg_ms"],
+                "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)"}
+    e2e = None
+    if not args.no_e2e:
+        hu = torch.empty(m.span, dtype=torch.float32, pin_memory=True)
+        hu.copy_(u.cpu())
+        d_in = torch.empty_like(u)
+
+        def e2e_step():
+            d_in.copy_(hu, non_blocking=True)
+            potts.min_max(ctx, m, d_in.data_ptr())
+            potts.grad_magn(ctx, m, d_in.data_ptr(), v.data_ptr())
+            potts.calc_hist_auto(ctx, m, d_in.data_ptr(), 1024)
+            potts.uv_hist_auto(ctx, m, d_in.data_ptr(), v.data_ptr(), 512)
+
+        e2e_step()
+        torch.cuda.synchronize(dev)
+        w0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        torch.cuda.synchronize(dev)
+        te = dist_.reduce(time.perf_counter() - w0, "max")
+        e2e = {"value": dist_.reduce(float(vox) * args.steps, "sum") / te / 1e9, "unit": "Gvox/s",
+               "h2d_bytes_per_step": 4 * m.span,
+               "d2h_bytes_per_step": 8 + (8 + 4 * 1024) + (16 + 4 * potts._native.host_lib().potts_uv_hist_span(512)),
+               "note": "u copied in from pinned host memory each step; results (ranges, histograms) read back"}
+    cpu = None
+    if dist_.rank == 0 and dist_.world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle
+
+        sph = cpu_sample_phantom()
+        su = sph.u.numpy().copy()
+        reps, t0 = 0, time.perf_counter()
+        while reps == 0 or time.perf_counter() - t0 < min(args.cpu_seconds, 15.0):
+            lo, hi = oracle.min_max(sph.mapping, su)
+            sv = oracle.grad_magn(sph.mapping, su)
+            oracle.calc_hist(sph.mapping, su, lo, hi, 1024)
+            vs, ve = oracle.min_max(sph.mapping, sv, positive=True)
+            oracle.uv_hist(sph.mapping, su, sv, lo, hi, vs, ve, 512)
+            reps += 1
+        tc = time.perf_counter() - t0
+        cpu = {"value": sph.mapping.data_size * reps / tc / 1e9, "unit": "Gvox/s", "cores": 1, "kind": "port",
+               "sample": f"C oracle, 1 thread: min_max, grad_magn, calc_hist, uv_hist of the 768x768 cross-section, "
+                         f"16 slices ({sph.mapping.data_size} voxels), {reps} rounds in {tc:.1f} s"}
+    if dist_.rank == 0:
+        out = {
+            "metric": "label-finding inputs Gvox/s (min_max, grad_magn, calc_hist 1024 bins, uv_hist 512x512)",
+            "value": round(value, 3), "unit": "Gvox/s", "n_gpus": dist_.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1000 * t_max / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"labels_{m.rows}x{m.cols}x{m.n_images}", "in_mask_voxels": vox,
+                       "parallelism": f"replica x{dist_.world}" if dist_.world > 1 else "single",
+                       "l2": "inputs larger than L2"},
+            "roofline": roofline, "kernels": kernels, "e2e": e2e, "gpu_launches": 11 * args.steps, "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    dist_.close()
+
+
 def main():
     args = parse_args()
     d = Dist()
@@ -1054,6 +1180,9 @@ def main():
         return
     if args.workload in ("fieldio", "fieldiomid"):
         run_fieldio(args, d)
+        return
+    if args.workload in ("labels", "labelsmid"):
+        run_labels(args, d)
         return
     run_ours(args, d)
 
