@@ -24,21 +24,35 @@ constexpr int kHistThreads = 256;
 // ---------------------------------------------------------------------------
 // min / max
 // ---------------------------------------------------------------------------
-// Per block: min and max over the in-mask values (only those > 0 when kPositive) of lines
-// blockIdx.x, blockIdx.x + gridDim.x, ...; FLT_MAX / -FLT_MAX when the block saw none.
-template <bool kPositive>
+// Per block: min and max over the in-mask values (only those > 0 when kPositive), one warp per
+// line (lines blockIdx.x * 8 + warp, then every gridDim.x * 8); FLT_MAX / -FLT_MAX when the block
+// saw none.  kVec: 16-byte loads (lines of a multiple of 4 values and stride, aligned field).
+template <bool kPositive, bool kVec>
 __global__ void __launch_bounds__(kHistThreads) minmax_partial_kernel(Geometry g, const float *__restrict__ f,
                                                                       float2 *__restrict__ partial)
 {
     float lo = 3.402823466e38f, hi = -3.402823466e38f;
-    for (int64_t L = blockIdx.x; L < g.n_lines; L += gridDim.x) {
+    auto see = [&](float x) {
+        if (!kPositive || x > 0.0f) {
+            lo = fminf(lo, x);
+            hi = fmaxf(hi, x);
+        }
+    };
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (kHistThreads / 32);
+    for (int64_t L = (int64_t)blockIdx.x * (kHistThreads / 32) + (threadIdx.x >> 5); L < g.n_lines; L += warps) {
         const float *line = f + L * g.nstride_w;
-        for (int n = threadIdx.x; n < g.ns; n += blockDim.x) {
-            const float x = __ldcs(line + n);
-            if (!kPositive || x > 0.0f) {
-                lo = fminf(lo, x);
-                hi = fmaxf(hi, x);
+        if constexpr (kVec) {
+#pragma unroll 4
+            for (int q = lane; q < g.ns / 4; q += 32) {
+                const float4 v = __ldg(reinterpret_cast<const float4 *>(line) + q);
+                see(v.x);
+                see(v.y);
+                see(v.z);
+                see(v.w);
             }
+        } else {
+            for (int n = lane; n < g.ns; n += 32) see(__ldg(line + n));
         }
     }
     __shared__ float slo[kHistThreads / 32], shi[kHistThreads / 32];
@@ -192,7 +206,7 @@ __global__ void __launch_bounds__(kHistThreads) hist1d_kernel(Geometry g, const 
             const int n = n0 + threadIdx.x;
             int id = -1;
             if (n < g.ns) {
-                float x = __ldcs(line + n);
+                float x = __ldg(line + n);
                 if (kJitter) x = __fadd_rn(x, hist_jitter(seed, (uint64_t)L * g.ns + n, delta));
                 if (lo <= x && __fadd_rn(x, hd) <= re) id = hist_bin(x, rs, re, nb);
             }
@@ -218,7 +232,7 @@ __global__ void __launch_bounds__(kHistThreads) hist1d_global_kernel(Geometry g,
             const int n = n0 + threadIdx.x;
             int id = -1;
             if (n < g.ns) {
-                float x = __ldcs(line + n);
+                float x = __ldg(line + n);
                 if (kJitter) x = __fadd_rn(x, hist_jitter(seed, (uint64_t)L * g.ns + n, delta));
                 if (lo <= x && __fadd_rn(x, hd) <= re) id = hist_bin(x, rs, re, nb);
             }
@@ -244,9 +258,10 @@ __device__ __forceinline__ int uv_bin(float x, float y, const UvRange &r)
 // cluster adds into whichever block owns a bin.  Each cluster flushes its non-zero bins to the
 // global histogram once.  1 MB of 32-bit counters: 512 x 512 bins fit.
 constexpr int kUvCluster = 8;
-constexpr int kUvSlice = 32768;  // counters per block (128 KB)
+constexpr int kUvSlice = 32768;   // counters per block (128 KB)
+constexpr int kUvThreads = 1024;  // one block per multiprocessor: as many warps as it holds
 
-__global__ void __cluster_dims__(kUvCluster, 1, 1) __launch_bounds__(kHistThreads, 1)
+__global__ void __cluster_dims__(kUvCluster, 1, 1) __launch_bounds__(kUvThreads, 1)
     uv_hist_cluster_kernel(Geometry g, const float *__restrict__ u, const float *__restrict__ v, UvRange r,
                            int total_bins, uint32_t *__restrict__ ghist)
 {
@@ -260,7 +275,7 @@ __global__ void __cluster_dims__(kUvCluster, 1, 1) __launch_bounds__(kHistThread
         for (int n0 = 0; n0 < g.ns; n0 += blockDim.x) {
             const int n = n0 + threadIdx.x;
             int id = -1;
-            if (n < g.ns) id = uv_bin(__ldcs(u + o0 + n), __ldcs(v + o0 + n), r);
+            if (n < g.ns) id = uv_bin(__ldg(u + o0 + n), __ldg(v + o0 + n), r);
             warp_count(id, [&](int b, uint32_t c) {
                 uint32_t *dst = cluster.map_shared_rank(sh_uv, (unsigned)(b / kUvSlice));
                 atomicAdd(dst + (b % kUvSlice), c);
@@ -283,7 +298,7 @@ __global__ void __launch_bounds__(kHistThreads) uv_hist_global_kernel(Geometry g
         for (int n0 = 0; n0 < g.ns; n0 += blockDim.x) {
             const int n = n0 + threadIdx.x;
             int id = -1;
-            if (n < g.ns) id = uv_bin(__ldcs(u + o0 + n), __ldcs(v + o0 + n), r);
+            if (n < g.ns) id = uv_bin(__ldg(u + o0 + n), __ldg(v + o0 + n), r);
             warp_count(id, [&](int b, uint32_t c) { atomicAdd(ghist + b, c); });
         }
     }

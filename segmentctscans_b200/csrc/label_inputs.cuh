@@ -38,10 +38,15 @@ int minmax_run(potts_context *ctx, const float *d_f, bool positive, float *out_m
         POTTS_TRY(ensure(ctx, ctx->hist, sizeof(float2) * nb + 2 * sizeof(float)));
         float2 *part = static_cast<float2 *>(ctx->hist.p);
         float *d_res = reinterpret_cast<float *>(part + nb);
-        if (positive)
-            potts::minmax_partial_kernel<true><<<nb, potts::kHistThreads, 0, ctx->stream>>>(g, d_f, part);
+        const bool vec = ((uintptr_t)d_f & 15u) == 0 && g.ns % 4 == 0 && g.nstride_w % 4 == 0;
+        if (positive && vec)
+            potts::minmax_partial_kernel<true, true><<<nb, potts::kHistThreads, 0, ctx->stream>>>(g, d_f, part);
+        else if (positive)
+            potts::minmax_partial_kernel<true, false><<<nb, potts::kHistThreads, 0, ctx->stream>>>(g, d_f, part);
+        else if (vec)
+            potts::minmax_partial_kernel<false, true><<<nb, potts::kHistThreads, 0, ctx->stream>>>(g, d_f, part);
         else
-            potts::minmax_partial_kernel<false><<<nb, potts::kHistThreads, 0, ctx->stream>>>(g, d_f, part);
+            potts::minmax_partial_kernel<false, false><<<nb, potts::kHistThreads, 0, ctx->stream>>>(g, d_f, part);
         potts::minmax_final_kernel<<<1, potts::kHistThreads, 0, ctx->stream>>>(part, (int)nb, d_res);
         ctx->total_launches += 2;
         POTTS_CUDA(cudaGetLastError());
@@ -128,7 +133,7 @@ int uv_hist_run(potts_context *ctx, const float *d_u, const float *d_v, const po
             // one block per multiprocessor: as many whole clusters as fit at once
             cudaLaunchConfig_t cfg{};
             cfg.gridDim = dim3((unsigned)(std::max(ctx->n_sm, 1) / potts::kUvCluster * potts::kUvCluster));
-            cfg.blockDim = dim3(potts::kHistThreads);
+            cfg.blockDim = dim3(potts::kUvThreads);
             cfg.dynamicSmemBytes = (size_t)smem;
             cfg.stream = ctx->stream;
             int clusters = 0;
@@ -138,7 +143,7 @@ int uv_hist_run(potts_context *ctx, const float *d_u, const float *d_v, const po
                 clusters = 1;
             }
             const unsigned blocks = (unsigned)(clusters * potts::kUvCluster);
-            potts::uv_hist_cluster_kernel<<<blocks, potts::kHistThreads, smem, ctx->stream>>>(g, d_u, d_v, r, (int)span,
+            potts::uv_hist_cluster_kernel<<<blocks, potts::kUvThreads, smem, ctx->stream>>>(g, d_u, d_v, r, (int)span,
                                                                                            d_hist);
         } else {
             potts::uv_hist_global_kernel<<<field_blocks(ctx, g.n_lines, 8), potts::kHistThreads, 0, ctx->stream>>>(
