@@ -244,10 +244,17 @@ def bytes_per_voxel_iter(variant: str, k: int = K_LABELS, storage: str = "f32") 
 
 # ----------------------------------------------------------------------------- CPU baseline (oracle)
 def cpu_sample_phantom():
+    """The config-1 cross-section and recipe, 16 slices along the axis, built on the CPU.  The
+    cylinder mask comes from the oracle's restatement of the mask constructor, so that this
+    phantom (used by the CPU baseline and the reference arm) never loads the GPU library."""
+    from oracle import oracle
+    from segmentctscans_b200.layout import CylinderMapping, get_stride
     from segmentctscans_b200.phantom import make_phantom
 
-    # the config-1 cross-section and recipe, 16 slices along the axis, built on the CPU
-    return make_phantom(16, 768, 768, 370.0, seed=0, radius_range=(6.0, 30.0), noise=7e-3, device="cpu")
+    n, rows, cols, r = 16, 768, 768, 370.0
+    sr, base, cb, ce, _ = oracle.cylinder_mask(rows, cols, (cols - 1) / 2.0, (rows - 1) / 2.0, r, get_stride(n))
+    m = CylinderMapping(n, rows, cols, get_stride(n), cb, ce, sr, base)
+    return make_phantom(n, rows, cols, r, seed=0, radius_range=(6.0, 30.0), noise=7e-3, device="cpu", mapping=m)
 
 
 def run_cpu_oracle(ph, iters: int, threads: int) -> float:

@@ -73,7 +73,12 @@ enum potts_variant {
 enum potts_storage {
     POTTS_STORE_F32 = 0,  /* FP32, as the reference */
     POTTS_STORE_BF16 = 1, /* bfloat16 (8-bit mantissa) */
-    POTTS_STORE_F16 = 2   /* IEEE binary16 (11-bit mantissa); Xi and V lie in [-1, 1] */
+    POTTS_STORE_F16 = 2,  /* IEEE binary16 (11-bit mantissa); Xi and V lie in [-1, 1] */
+    POTTS_STORE_F64 = 3   /* FP64 state and FP64 arithmetic, always in the split kernel structure (the
+                             variant option is ignored): the reference iteration in double precision,
+                             the same bits as the FP64 CPU oracle; the yardstick of the other formats
+                             on volumes too large for the CPU.  potts_solve_device rounds its V / Xi
+                             outputs to FP32; potts_solve_device_f64 returns them in FP64. */
 };
 
 typedef struct potts_options {
@@ -163,6 +168,16 @@ int potts_solve_device(potts_context *ctx, const potts_mapping *map, const float
                        uint8_t *d_labels, float *d_V, float *d_Xi, potts_stats *stats);
 
 /*
+ * The same solve with the FP64 state (POTTS_STORE_F64 whatever opts->storage
+ * says): V and Xi come back as FP64 planes (d_V: K-1 planes, d_Xi: 3(K-1)
+ * planes of span doubles; each may be NULL).  The split kernels of
+ * potts-model/potts-min-partition.cpp:96-488 in double precision.
+ */
+int potts_solve_device_f64(potts_context *ctx, const potts_mapping *map, const float *d_u, int K, const float *ci,
+                           float lambda, float tau1, float tau2, int iters, const potts_options *opts, float *d_res,
+                           uint8_t *d_labels, double *d_V, double *d_Xi, potts_stats *stats);
+
+/*
  * Host-buffer form (what potts-model.cpp does around the call: upload, solve,
  * download).  h_u is span floats on the host (pinned memory is faster); the
  * outputs h_res (span floats) and h_labels (span bytes) may be NULL.  Blocks
@@ -185,11 +200,14 @@ int potts_solve_host(potts_context *ctx, const potts_mapping *map, const float *
  * with `map` (span = base[cols] per plane); h_out receives 3 doubles; the
  * work runs on `stream` (a cudaStream_t, NULL = default stream) on the
  * current device, and the call returns after the result is on the host.
- * The first call on a device looks up the working memory's device address:
- * make it before any stream capture.  Every call uses the same working
- * memory, so calls that overlap on the GPU race; a call's working memory is
- * fully rewritten before it is read.  Returns POTTS_EINVAL for more than
- * POTTS_STATIC_MAX_COLS columns.
+ * Every call looks up the working memory's device address on the current
+ * device (cudaGetSymbolAddress, which allocates nothing); the first lookup in
+ * a process may load the library's device code, so make the first call before
+ * any stream capture.  Every call uses the same working memory, so calls that
+ * overlap on the GPU race; a call's working memory is fully rewritten before
+ * it is read.  The mapping gets the same checks as in every solver entry
+ * point, on the host, before anything runs on the GPU.  Returns POTTS_EINVAL
+ * for more than POTTS_STATIC_MAX_COLS columns or an invalid mapping.
  */
 #define POTTS_STATIC_MAX_COLS 16384
 int potts_energies_static(const potts_mapping *map, const float *d_u, int K, const float *ci, float lambda,

@@ -12,8 +12,8 @@ from .build import LIB_PATH
 
 POTTS_OK, POTTS_EINVAL, POTTS_ENOMEM, POTTS_ECUDA, POTTS_ETIMEOUT, POTTS_ENODEV = range(6)
 VARIANT_FUSED, VARIANT_PLAIN = 0, 1
-STORE_F32, STORE_BF16, STORE_F16 = 0, 1, 2
-STORAGE = {"f32": STORE_F32, "bf16": STORE_BF16, "f16": STORE_F16}
+STORE_F32, STORE_BF16, STORE_F16, STORE_F64 = 0, 1, 2, 3
+STORAGE = {"f32": STORE_F32, "bf16": STORE_BF16, "f16": STORE_F16, "f64": STORE_F64}
 MAX_PHASES = 6
 
 
@@ -104,6 +104,7 @@ SIGNATURES = {
     "potts_field_destroy": (None, [_P]),
     "potts_min_partition": (_I, [_P, _P, _MP, _I, _FP, _F, _F, _F, _I, _OP, ctypes.POINTER(_P), _SP]),
     "potts_solve_device": (_I, [_P, _MP, _P, _I, _FP, _F, _F, _F, _I, _OP, _P, _P, _P, _P, _SP]),
+    "potts_solve_device_f64": (_I, [_P, _MP, _P, _I, _FP, _F, _F, _F, _I, _OP, _P, _P, _P, _P, _SP]),
     "potts_solve_host": (_I, [_P, _MP, _P, _I, _FP, _F, _F, _F, _I, _OP, _P, _P, _SP]),
     "potts_cylinder_mapping": (_U64, [_U32, _U32, ctypes.c_double, ctypes.c_double, ctypes.c_double, _U32,
                                       ctypes.POINTER(_U32), ctypes.POINTER(_U32), ctypes.POINTER(_U32),

@@ -6,9 +6,12 @@
 
 #include <cstdint>
 
+#include <type_traits>
+
 #include "geometry.cuh"
 #include "storage.cuh"
 #include "voxel.cuh"
+#include "voxel_f64.cuh"
 
 namespace potts {
 
@@ -41,10 +44,14 @@ __global__ void __launch_bounds__(kPlainThreads) init_kernel(Geometry g, const f
     if (!p.valid) return;
     const int64_t o = p.line * g.nstride_w + p.n;
     const float x = u[p.line * g.nstride_in + g.slab_start + p.n];
-    const int cl = nearest_label<K>(x, pp.c);
+    int cl;
+    if constexpr (std::is_same_v<ST, double>)
+        cl = nearest_label_f64<K>((double)x, pp.c);
+    else
+        cl = nearest_label<K>(x, pp.c);
 #pragma unroll
     for (int i = 0; i < K - 1; ++i) {
-        const float one = (i == cl) ? 1.0f : 0.0f;
+        const typename Store<ST>::Real one = (i == cl) ? 1.0f : 0.0f;
         V[i * g.plane_w + o] = Store<ST>::st(one);
         if (Vb) Vb[i * g.plane_w + o] = Store<ST>::st(one);
     }
@@ -64,18 +71,22 @@ __global__ void __launch_bounds__(kPlainThreads) dual_kernel(Geometry g, ST *__r
     const bool hr = li.flags & kHasNextRow;
     const bool hc = li.next_col >= 0;
     const int64_t oc = hc ? (int64_t)li.next_col * g.nstride_w + p.n : o;
-    float vx[K - 1], vn[K - 1], vr[K - 1], vc[K - 1], x[3 * (K - 1)], xo[3 * (K - 1)];
+    using R = typename Store<ST>::Real;
+    R vx[K - 1], vn[K - 1], vr[K - 1], vc[K - 1], x[3 * (K - 1)], xo[3 * (K - 1)];
 #pragma unroll
     for (int i = 0; i < K - 1; ++i) {
         const ST *b = vb + i * g.plane_w;
         vx[i] = Store<ST>::ld(b[o]);
-        vn[i] = hn ? Store<ST>::ld(b[o + 1]) : 0.0f;
-        vr[i] = hr ? Store<ST>::ld(b[o + g.nstride_w]) : 0.0f;
-        vc[i] = hc ? Store<ST>::ld(b[oc]) : 0.0f;
+        vn[i] = hn ? Store<ST>::ld(b[o + 1]) : R(0);
+        vr[i] = hr ? Store<ST>::ld(b[o + g.nstride_w]) : R(0);
+        vc[i] = hc ? Store<ST>::ld(b[oc]) : R(0);
     }
 #pragma unroll
     for (int j = 0; j < 3 * (K - 1); ++j) x[j] = Store<ST>::ld(xi[j * g.plane_w + o]);
-    dual_voxel<K>(xo, x, vx, vn, vr, vc, hn, hr, hc, tau2, thr);
+    if constexpr (std::is_same_v<R, double>)
+        dual_voxel_f64<K>(xo, x, vx, vn, vr, vc, hn, hr, hc, (double)tau2);
+    else
+        dual_voxel<K>(xo, x, vx, vn, vr, vc, hn, hr, hc, tau2, thr);
 #pragma unroll
     for (int j = 0; j < 3 * (K - 1); ++j) xi[j * g.plane_w + o] = Store<ST>::st(xo[j]);
 }
@@ -117,7 +128,8 @@ __global__ void __launch_bounds__(kPlainThreads) primal_kernel(Geometry g, const
         const bool hr = li.flags & kHasNextRow, pr = li.flags & kHasPrevRow;
         const bool hc = li.next_col >= 0, pc = li.prev_col >= 0;
         const int64_t opc = pc ? (int64_t)li.prev_col * g.nstride_w + p.n : o;
-        float x[3 * (K - 1)], xn[K - 1], xr[K - 1], xc[K - 1], v[K - 1], vnew[K - 1], vbar[K - 1];
+        using R = typename Store<ST>::Real;
+        R x[3 * (K - 1)], xn[K - 1], xr[K - 1], xc[K - 1], v[K - 1], vnew[K - 1], vbar[K - 1];
 #pragma unroll
         for (int i = 0; i < K - 1; ++i) {
             const ST *b0 = xi + (3 * i) * g.plane_w;
@@ -126,13 +138,17 @@ __global__ void __launch_bounds__(kPlainThreads) primal_kernel(Geometry g, const
             x[3 * i] = Store<ST>::ld(b0[o]);
             x[3 * i + 1] = Store<ST>::ld(b1[o]);
             x[3 * i + 2] = Store<ST>::ld(b2[o]);
-            xn[i] = pn ? Store<ST>::ld(b0[o - 1]) : 0.0f;
-            xr[i] = pr ? Store<ST>::ld(b1[o - g.nstride_w]) : 0.0f;
-            xc[i] = pc ? Store<ST>::ld(b2[opc]) : 0.0f;
+            xn[i] = pn ? Store<ST>::ld(b0[o - 1]) : R(0);
+            xr[i] = pr ? Store<ST>::ld(b1[o - g.nstride_w]) : R(0);
+            xc[i] = pc ? Store<ST>::ld(b2[opc]) : R(0);
             v[i] = Store<ST>::ld(V[i * g.plane_w + o]);
         }
         const float uu = u[p.line * g.nstride_in + g.slab_start + p.n];
-        d = primal_voxel<K>(vnew, vbar, v, x, xn, xr, xc, pn, hn, pr, hr, pc, hc, uu, pp.c, pp.lam, pp.tau1);
+        if constexpr (std::is_same_v<R, double>)
+            d = (float)primal_voxel_f64<K>(vnew, vbar, v, x, xn, xr, xc, pn, hn, pr, hr, pc, hc, (double)uu, pp.c,
+                                           (double)pp.lam, (double)pp.tau1);
+        else
+            d = primal_voxel<K>(vnew, vbar, v, x, xn, xr, xc, pn, hn, pr, hr, pc, hc, uu, pp.c, pp.lam, pp.tau1);
         uint32_t h[(K - 1 + 1) / 2];
         if constexpr (Store<ST>::kStochasticV) {
 #pragma unroll
@@ -153,30 +169,40 @@ __global__ void __launch_bounds__(kPlainThreads) primal_kernel(Geometry g, const
 
 // update_kernel: argmax over n in [res_begin, res_end) of the slab, written
 // with the input mapping; optionally copies V and Xi out.
-template <int K, typename ST>
+// V and Xi are written as OT (FP32, or FP64 from the FP64 state); OT is
+// given, never deduced from the (possibly null) output pointers.
+template <typename T>
+struct Given {
+    using type = T;
+};
+template <int K, typename ST, typename OT = float>
 __global__ void __launch_bounds__(kPlainThreads) update_kernel(Geometry g, const ST *__restrict__ V,
                                                                 const ST *__restrict__ xi, PhaseParams<K> pp,
                                                                 int res_begin, int res_end, float *res,
-                                                                uint8_t *labels, float *V_out, float *Xi_out,
-                                                                int64_t plane_out)
+                                                                uint8_t *labels, typename Given<OT>::type *V_out,
+                                                                typename Given<OT>::type *Xi_out, int64_t plane_out)
 {
     const PlainIndex p = plain_index(g, res_begin, res_end);
     if (!p.valid) return;
     const int64_t o = p.line * g.nstride_w + p.n;
     const int64_t oo = p.line * g.nstride_in + g.slab_start + p.n;
-    float v[K - 1];
+    typename Store<ST>::Real v[K - 1];
 #pragma unroll
     for (int i = 0; i < K - 1; ++i) v[i] = Store<ST>::ld(V[i * g.plane_w + o]);
-    const int lab = argmax_label<K>(v);
+    int lab;
+    if constexpr (std::is_same_v<ST, double>)
+        lab = argmax_label_f64<K>(v);
+    else
+        lab = argmax_label<K>(v);
     if (res) res[oo] = pp.c[lab];
     if (labels) labels[oo] = (uint8_t)lab;
     if (V_out) {
 #pragma unroll
-        for (int i = 0; i < K - 1; ++i) V_out[i * plane_out + oo] = v[i];
+        for (int i = 0; i < K - 1; ++i) V_out[i * plane_out + oo] = (OT)v[i];
     }
     if (Xi_out) {
 #pragma unroll
-        for (int j = 0; j < 3 * (K - 1); ++j) Xi_out[j * plane_out + oo] = Store<ST>::ld(xi[j * g.plane_w + o]);
+        for (int j = 0; j < 3 * (K - 1); ++j) Xi_out[j * plane_out + oo] = (OT)Store<ST>::ld(xi[j * g.plane_w + o]);
     }
 }
 

@@ -12,7 +12,6 @@
 
 #include <cmath>
 #include <cstdint>
-#include <mutex>
 #include <string>
 
 #include "../../include/potts_b200.h"
@@ -21,7 +20,7 @@ namespace {
 
 constexpr int kBlocks = 1184;  // 8 blocks per SM of a 148-SM B200
 constexpr int kThreads = 256;
-constexpr int kMaxDevices = 64;
+constexpr int kWarps = kThreads / 32;
 constexpr uint32_t kTableChunk = 512;
 
 // Working memory: per column (line of its first row, first row, end row), one
@@ -36,29 +35,22 @@ struct StaticAddresses {
     double *out = nullptr;
 };
 
-std::mutex g_setup_mutex;
-StaticAddresses g_addr[kMaxDevices];
-bool g_ready[kMaxDevices] = {};
-
-// Device addresses of the arrays on `device` (the current device), looked up
-// once per device: in host code the arrays' names are host-side stand-ins,
-// not device addresses.
-int device_addresses(int device, StaticAddresses *a, std::string *err)
+// Device addresses of the arrays on the current device.  In host code the
+// arrays' names are host-side stand-ins, not device addresses.  The lookup
+// allocates nothing and is repeated on every call, so that an address is never
+// stale (a cudaDeviceReset between calls reloads the module, possibly at a new
+// address); the first lookup in a process may load the library's device code.
+int device_addresses(StaticAddresses *a, std::string *err)
 {
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_ready[device]) {
-        StaticAddresses s;
-        cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&s.cols), g_static_cols);
-        if (e == cudaSuccess) e = cudaGetSymbolAddress(reinterpret_cast<void **>(&s.partial), g_static_partial);
-        if (e == cudaSuccess) e = cudaGetSymbolAddress(reinterpret_cast<void **>(&s.out), g_static_out);
-        if (e != cudaSuccess) {
-            *err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
-            return POTTS_ECUDA;
-        }
-        g_addr[device] = s;
-        g_ready[device] = true;
+    StaticAddresses s;
+    cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&s.cols), g_static_cols);
+    if (e == cudaSuccess) e = cudaGetSymbolAddress(reinterpret_cast<void **>(&s.partial), g_static_partial);
+    if (e == cudaSuccess) e = cudaGetSymbolAddress(reinterpret_cast<void **>(&s.out), g_static_out);
+    if (e != cudaSuccess) {
+        *err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+        return POTTS_ECUDA;
     }
-    *a = g_addr[device];
+    *a = s;
     return POTTS_OK;
 }
 
@@ -73,23 +65,24 @@ struct Labels {
     double c[POTTS_MAX_PHASES];
 };
 
-// Block-strided pass over the columns, each column's voxels over the block's
-// threads.  Per voxel the solver's energy terms: e_i = lam (u - c_i)^2 -
-// div Xi_i, L += sum_i V_i e_i, D += min_i e_i.
+// Block-strided pass over the columns; in a column, the warps take its lines
+// (rows) in turn and the lanes the slices of a line.  Per voxel the solver's
+// energy terms: e_i = lam (u - c_i)^2 - div Xi_i, L += sum_i V_i e_i,
+// D += min_i e_i.
 template <int K>
 __global__ void __launch_bounds__(kThreads)
     static_energy_kernel(StaticGeom g, const int4 *__restrict__ cols, const float *__restrict__ u,
                          const float *__restrict__ V, const float *__restrict__ xi, double lam, Labels lb,
                          double2 *partial)
 {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double lag = 0.0, dual = 0.0;
     for (int col = g.col_begin + blockIdx.x; col < g.col_end; col += gridDim.x) {
         const int4 ci = cols[col];
         const int4 cp = col > g.col_begin ? cols[col - 1] : make_int4(0, 0, 0, 0);
         const int4 cn = col + 1 < g.col_end ? cols[col + 1] : make_int4(0, 0, 0, 0);
-        const int64_t voxels = (int64_t)(ci.z - ci.y) * g.n;
-        for (int64_t k = threadIdx.x; k < voxels; k += blockDim.x) {
-            const int row = ci.y + (int)(k / g.n), n = (int)(k % g.n);
+        for (int row = ci.y + warp; row < ci.z; row += kWarps) {
+            for (int n = lane; n < g.n; n += 32) {
             const int64_t o = (int64_t)(ci.x + row - ci.y) * g.nstride + n;
             const bool hn = n + 1 < g.n, pn = n > 0;
             const bool hr = row + 1 < ci.z, pr = row > ci.y;
@@ -138,18 +131,19 @@ __global__ void __launch_bounds__(kThreads)
             }
             lag += l;
             dual += mn;
+            }
         }
     }
-    __shared__ double2 red[kThreads / 32];
+    __shared__ double2 red[kWarps];
     for (int s = 16; s > 0; s >>= 1) {
         lag += __shfl_xor_sync(0xffffffffu, lag, s);
         dual += __shfl_xor_sync(0xffffffffu, dual, s);
     }
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = make_double2(lag, dual);
+    if (lane == 0) red[warp] = make_double2(lag, dual);
     __syncthreads();
     if (threadIdx.x == 0) {
         double2 t = red[0];
-        for (int w = 1; w < kThreads / 32; ++w) t.x += red[w].x, t.y += red[w].y;
+        for (int w = 1; w < kWarps; ++w) t.x += red[w].x, t.y += red[w].y;
         partial[blockIdx.x] = t;
     }
 }
@@ -173,8 +167,10 @@ void launch_energy(const StaticGeom &g, const StaticAddresses &a, const float *u
 
 }  // namespace
 
-// defined with the rest of the C ABI: sets what potts_last_error() returns
+// defined with the rest of the C ABI: sets what potts_last_error() returns,
+// and runs the solver's host-side checks of a mapping
 void potts_set_last_error(const std::string &msg);
+int potts_check_mapping(const potts_mapping *map);
 
 namespace {
 int static_fail(int code, const std::string &msg)
@@ -193,23 +189,22 @@ extern "C" int potts_energies_static(const potts_mapping *map, const float *d_u,
     if (map->cols > POTTS_STATIC_MAX_COLS)
         return static_fail(POTTS_EINVAL, "more columns than POTTS_STATIC_MAX_COLS (" +
                                              std::to_string(POTTS_STATIC_MAX_COLS) + ")");
-    if (map->nstride == 0 || map->nstride < map->n_images || map->col_end > map->cols ||
-        (map->col_begin > map->col_end && map->col_end != 0))
-        return static_fail(POTTS_EINVAL, "invalid mapping");
+    // the same checks as every solver entry point (non-decreasing base[] of
+    // multiples of nstride, rows inside the row extent, ...): a bad table
+    // would make the kernel read outside u, V and Xi
+    if (const int st = potts_check_mapping(map); st != POTTS_OK) return st;
     Labels lb;
     for (int i = 0; i < K; ++i) {
         if (!std::isfinite(ci[i])) return static_fail(POTTS_EINVAL, "labels must be finite");
         lb.c[i] = (double)ci[i];
     }
     if (!std::isfinite(lambda)) return static_fail(POTTS_EINVAL, "lambda must be finite");
-    int device = 0;
-    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices) {
-        cudaGetLastError();
-        return static_fail(POTTS_ENODEV, "no usable CUDA device");
-    }
     StaticAddresses a;
     std::string err;
-    if (device_addresses(device, &a, &err) != POTTS_OK) return static_fail(POTTS_ECUDA, err);
+    if (device_addresses(&a, &err) != POTTS_OK) {
+        cudaGetLastError();
+        return static_fail(POTTS_ECUDA, err);
+    }
 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     // the column table, in chunks through a host array; a copy from pageable

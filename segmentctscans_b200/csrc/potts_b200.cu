@@ -330,8 +330,9 @@ int state_planes(int K, int variant)
 struct Outputs {
     float *res;
     uint8_t *labels;
-    float *V;
-    float *Xi;
+    void *V;            // float, or double when v64
+    void *Xi;           // float, or double when v64
+    bool v64 = false;   // V and Xi are FP64 planes (FP64 state only)
 };
 
 inline unsigned plain_blocks(const Geometry &g, int n_begin, int n_end)
@@ -682,7 +683,7 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
     if (dq && iters > 0) POTTS_CUDA(cudaMemsetAsync(dq, 0, sizeof(float) * iters, s));
 
     int cur = 0;
-    if (o.variant == POTTS_VARIANT_PLAIN) {
+    if (o.variant == POTTS_VARIANT_PLAIN || std::is_same_v<ST, double>) {
         ST *xi = st.xi[0], *V = st.v[0], *Vb = st.v[1];
         potts::init_kernel<K, ST><<<nb, potts::kPlainThreads, 0, s>>>(g, d_u, V, Vb, pp);
         ctx->total_launches += 1;
@@ -698,7 +699,7 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
         }
         POTTS_TRY(seg_end(ctx));
         POTTS_CUDA(cudaGetLastError());
-    } else {
+    } else if constexpr (!std::is_same_v<ST, double>) {
         // Fused schedule: a dual step gives Xi^1 from V^0 (= Vbar^0); launch m
         // (m = 1 .. iters-1) turns (Xi^m, V^{m-1}) into (Xi^{m+1}, V^m); a final
         // primal step gives V^iters from Xi^iters.
@@ -743,10 +744,15 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
     if (res_end > res_begin) {
         const unsigned nbu = plain_blocks(g, res_begin, res_end);
         ctx->total_launches += 1;
-        const ST *Vf = o.variant == POTTS_VARIANT_PLAIN ? st.v[0] : st.v[cur];
-        const ST *Xf = o.variant == POTTS_VARIANT_PLAIN ? st.xi[0] : st.xi[cur];
-        potts::update_kernel<K, ST><<<nbu, potts::kPlainThreads, 0, s>>>(g, Vf, Xf, pp, res_begin, res_end, out.res,
-                                                                      out.labels, out.V, out.Xi, plane_out);
+        const bool split = o.variant == POTTS_VARIANT_PLAIN || std::is_same_v<ST, double>;
+        const ST *Vf = split ? st.v[0] : st.v[cur];
+        const ST *Xf = split ? st.xi[0] : st.xi[cur];
+        if (out.v64)
+            potts::update_kernel<K, ST, double><<<nbu, potts::kPlainThreads, 0, s>>>(
+                g, Vf, Xf, pp, res_begin, res_end, out.res, out.labels, (double *)out.V, (double *)out.Xi, plane_out);
+        else
+            potts::update_kernel<K, ST, float><<<nbu, potts::kPlainThreads, 0, s>>>(
+                g, Vf, Xf, pp, res_begin, res_end, out.res, out.labels, (float *)out.V, (float *)out.Xi, plane_out);
         POTTS_CUDA(cudaGetLastError());
     }
     return POTTS_OK;
@@ -875,7 +881,8 @@ int check_params(int K, const float *ci, float lam, float tau1, float tau2, int 
     if (iters < 0) return fail(POTTS_EINVAL, "iters must be >= 0");
     if (o.variant != POTTS_VARIANT_FUSED && o.variant != POTTS_VARIANT_PLAIN)
         return fail(POTTS_EINVAL, "unknown variant");
-    if (o.storage != POTTS_STORE_F32 && o.storage != POTTS_STORE_BF16 && o.storage != POTTS_STORE_F16)
+    if (o.storage != POTTS_STORE_F32 && o.storage != POTTS_STORE_BF16 && o.storage != POTTS_STORE_F16 &&
+        o.storage != POTTS_STORE_F64)
         return fail(POTTS_EINVAL, "unknown storage");
     if (o.gap_every < 0 || o.slab_w < 0) return fail(POTTS_EINVAL, "gap_every and slab_w must be >= 0");
     if (o.tile_rows < 0 || o.tile_slices < 0 || o.segment_cols < 0 || o.tile_vpt < 0)
@@ -910,8 +917,13 @@ int solve_dispatch(potts_context *ctx, const potts_mapping *map, const float *d_
     if (!d_u) return fail(POTTS_EINVAL, "u is NULL");
     POTTS_CUDA(cudaSetDevice(ctx->device));
     POTTS_TRY(upload_lines(ctx, map));
+    if (out.v64 && o.storage != POTTS_STORE_F64) return fail(POTTS_EINVAL, "FP64 outputs need the FP64 state");
     if (o.storage == POTTS_STORE_BF16) return solve_store<__nv_bfloat16>(ctx, d_u, K, ci, lam, tau1, tau2, iters, o, out, stats);
     if (o.storage == POTTS_STORE_F16) return solve_store<__half>(ctx, d_u, K, ci, lam, tau1, tau2, iters, o, out, stats);
+    if (o.storage == POTTS_STORE_F64) {
+        o.variant = POTTS_VARIANT_PLAIN;  // the FP64 state runs the split kernels only
+        return solve_store<double>(ctx, d_u, K, ci, lam, tau1, tau2, iters, o, out, stats);
+    }
     return solve_store<float>(ctx, d_u, K, ci, lam, tau1, tau2, iters, o, out, stats);
 }
 
@@ -1083,6 +1095,13 @@ int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int 
 
 __attribute__((visibility("hidden"))) void potts_set_last_error(const std::string &msg) { g_last_error = msg; }
 
+// The mapping checks of every solver entry point, for the library's other
+// translation units (host only; sets potts_last_error on failure).
+__attribute__((visibility("hidden"))) int potts_check_mapping(const potts_mapping *map)
+{
+    return validate_mapping(map);
+}
+
 extern "C" {
 
 void potts_default_options(potts_options *o)
@@ -1224,6 +1243,18 @@ int potts_solve_device(potts_context *ctx, const potts_mapping *map, const float
 {
     Outputs out{d_res, d_labels, d_V, d_Xi};
     return solve_dispatch(ctx, map, d_u, K, ci, lambda, tau1, tau2, iters, opts, out, stats);
+}
+
+int potts_solve_device_f64(potts_context *ctx, const potts_mapping *map, const float *d_u, int K, const float *ci,
+                           float lambda, float tau1, float tau2, int iters, const potts_options *opts, float *d_res,
+                           uint8_t *d_labels, double *d_V, double *d_Xi, potts_stats *stats)
+{
+    potts_options o;
+    potts_default_options(&o);
+    if (opts) o = *opts;
+    o.storage = POTTS_STORE_F64;
+    Outputs out{d_res, d_labels, d_V, d_Xi, true};
+    return solve_dispatch(ctx, map, d_u, K, ci, lambda, tau1, tau2, iters, &o, out, stats);
 }
 
 int potts_min_partition(potts_context *ctx, const potts_field *g, const potts_mapping *cpu_map, int K,

@@ -1,5 +1,6 @@
-// Storage formats of the solver state (Xi, V, Vbar).  Arithmetic is always
-// FP32: a load widens exactly, a store rounds to nearest, ties to even.  So
+// Storage formats of the solver state (Xi, V, Vbar).  Arithmetic is FP32 for
+// the FP32 and 16-bit formats (FP64 for the FP64 state): a load widens
+// exactly, a store rounds to nearest, ties to even.  So
 // that every kernel form sees the same values, anything the reference keeps in
 // memory (Xi, V, Vbar) is rounded to the storage format before it is used
 // again, also when a kernel keeps it on chip.
@@ -47,6 +48,7 @@ struct Store;
 
 template <>
 struct Store<float> {
+    using Real = float;  // arithmetic type of the kernels for this format
     static constexpr bool kExact = true;
     static constexpr bool kStochasticV = false;
     __device__ __forceinline__ static float st_v(float x, uint32_t) { return x; }
@@ -59,6 +61,7 @@ struct Store<float> {
 
 template <>
 struct Store<__nv_bfloat16> {
+    using Real = float;
     static constexpr bool kExact = false;
     static constexpr bool kStochasticV = true;
     // stored V: add 16 random bits below the kept half of the binary32
@@ -84,6 +87,7 @@ struct Store<__nv_bfloat16> {
 
 template <>
 struct Store<__half> {
+    using Real = float;
     static constexpr bool kExact = false;
     static constexpr bool kStochasticV = false;
     __device__ __forceinline__ static __half st_v(float x, uint32_t) { return __float2half_rn(x); }
@@ -98,6 +102,19 @@ struct Store<__half> {
     {
         *reinterpret_cast<__half2 *>(p) = __float22half2_rn(v);
     }
+};
+
+// FP64 state with FP64 arithmetic: the split kernels only (the FP64 solve,
+// large-volume counterpart of the CPU oracle).
+template <>
+struct Store<double> {
+    using Real = double;
+    static constexpr bool kExact = true;
+    static constexpr bool kStochasticV = false;
+    __device__ __forceinline__ static double st_v(double x, uint32_t) { return x; }
+    __device__ __forceinline__ static double ld(double x) { return x; }
+    __device__ __forceinline__ static double st(double x) { return x; }
+    __device__ __forceinline__ static double round(double x) { return x; }
 };
 
 }  // namespace potts

@@ -82,15 +82,21 @@ def _blur_axis(x, axis: int, kernel):
 
 def make_phantom(n: int, rows: int, cols: int, r: float, *, seed: int = 0, radius_range=(4.0, 12.0),
                  noise: float = 7e-3, porosity: float = 0.2, p_scco2: float = 0.4, k: int = 3,
-                 p_phase4: float = 0.15, blur_sigma: float = 1.0, device="cpu") -> Phantom:
+                 p_phase4: float = 0.15, blur_sigma: float = 1.0, device="cpu",
+                 mapping: Optional[CylinderMapping] = None) -> Phantom:
     """Build one phantom.  k = 3: scCO2 / brine / glass; k = 4 adds a phase at 4.6e-2 on
-    p_phase4 of the pores.  Labels are returned in ascending intensity order."""
+    p_phase4 of the pores.  Labels are returned in ascending intensity order.  ``mapping``
+    (optional) is the cylinder mask of (n, rows, cols, r) built elsewhere; by default the
+    native library builds it."""
     import torch
 
     if k not in (3, 4):
         raise ValueError("k must be 3 or 4")
     rng = np.random.Generator(np.random.PCG64(seed))
-    mapping = CylinderMapping.cylinder(n, rows, cols, r)
+    if mapping is None:
+        mapping = CylinderMapping.cylinder(n, rows, cols, r)
+    elif (mapping.n_images, mapping.rows, mapping.cols) != (n, rows, cols):
+        raise ValueError("mapping does not match the phantom's extents")
     labels = [SCCO2, BRINE, GLASS] if k == 3 else [SCCO2, BRINE, PHASE4, GLASS]
     glass_id = len(labels) - 1
     cs = _rsa(rng, n, rows, cols, r, radius_range[0], radius_range[1], porosity)

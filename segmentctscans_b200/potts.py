@@ -211,6 +211,22 @@ def solve_device(ctx: CudaContext, mapping: CylinderMapping, u_ptr: int, ci: Seq
     return _stats_out(st, dq, en) if stats else None
 
 
+def solve_device_f64(ctx: CudaContext, mapping: CylinderMapping, u_ptr: int, ci: Sequence[float], lam: float,
+                     tau1: float, tau2: float, iters: int, *, res_ptr: int = 0, labels_ptr: int = 0,
+                     V_ptr: int = 0, Xi_ptr: int = 0, stats: bool = True, **options) -> Optional[SolveStats]:
+    """FP64 solve (potts_solve_device_f64): FP64 state and arithmetic in the split kernel structure;
+    V_ptr / Xi_ptr are FP64 planes.  The GPU counterpart of the FP64 oracle for large volumes."""
+    c = _ci_array(ci)
+    opts = _native.default_options(**options)
+    st, dq, en = _make_stats(iters, opts.gap_every, stats)
+    check(_native.host_lib().potts_solve_device_f64(
+        ctx.handle, ctypes.byref(mapping.as_c()), ctypes.c_void_p(int(u_ptr)), int(c.size),
+        c.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(lam), float(tau1), float(tau2), int(iters),
+        ctypes.byref(opts), ctypes.c_void_p(int(res_ptr)), ctypes.c_void_p(int(labels_ptr)),
+        ctypes.c_void_p(int(V_ptr)), ctypes.c_void_p(int(Xi_ptr)), ctypes.byref(st) if stats else None))
+    return _stats_out(st, dq, en) if stats else None
+
+
 def solve_host(ctx: CudaContext, mapping: CylinderMapping, u: np.ndarray, ci: Sequence[float], lam: float,
                tau1: float, tau2: float, iters: int, *, res: Optional[np.ndarray] = None,
                labels: Optional[np.ndarray] = None, stats: bool = False, **options) -> Optional[SolveStats]:
@@ -235,8 +251,8 @@ def solve_host(ctx: CudaContext, mapping: CylinderMapping, u: np.ndarray, ci: Se
 class PottsResult:
     labels: np.ndarray            # uint8 span: argmax index
     res: np.ndarray               # float32 span: ci[argmax]
-    V: Optional[np.ndarray]       # float32 [K-1, span]
-    Xi: Optional[np.ndarray]      # float32 [3(K-1), span]
+    V: Optional[np.ndarray]       # float32 [K-1, span] (float64 for storage="f64")
+    Xi: Optional[np.ndarray]      # float32 [3(K-1), span] (float64 for storage="f64")
     stats: SolveStats = field(default=None)
 
 
@@ -256,11 +272,14 @@ def solve(mapping: CylinderMapping, u: np.ndarray, ci: Sequence[float], lam: flo
         du = torch.from_numpy(np.ascontiguousarray(u, dtype=np.float32)).to(dev)
         dres = torch.zeros(span, dtype=torch.float32, device=dev)
         dlab = torch.zeros(span, dtype=torch.uint8, device=dev)
-        dV = torch.zeros((K - 1, span), dtype=torch.float32, device=dev) if want_state else None
-        dX = torch.zeros((3 * (K - 1), span), dtype=torch.float32, device=dev) if want_state else None
-        st = solve_device(ctx, mapping, du.data_ptr(), c, lam, tau1, tau2, iters, res_ptr=dres.data_ptr(),
-                          labels_ptr=dlab.data_ptr(), V_ptr=dV.data_ptr() if dV is not None else 0,
-                          Xi_ptr=dX.data_ptr() if dX is not None else 0, stats=True, **options)
+        f64 = options.get("storage") in ("f64", _native.STORE_F64)
+        sdt = torch.float64 if f64 else torch.float32
+        dV = torch.zeros((K - 1, span), dtype=sdt, device=dev) if want_state else None
+        dX = torch.zeros((3 * (K - 1), span), dtype=sdt, device=dev) if want_state else None
+        st = (solve_device_f64 if f64 else solve_device)(
+            ctx, mapping, du.data_ptr(), c, lam, tau1, tau2, iters, res_ptr=dres.data_ptr(),
+            labels_ptr=dlab.data_ptr(), V_ptr=dV.data_ptr() if dV is not None else 0,
+            Xi_ptr=dX.data_ptr() if dX is not None else 0, stats=True, **options)
         torch.cuda.synchronize(dev)
         return PottsResult(dlab.cpu().numpy(), dres.cpu().numpy(),
                            dV.cpu().numpy() if dV is not None else None,

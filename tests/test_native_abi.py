@@ -116,3 +116,31 @@ def test_uv_hist_layout(native_lib):
     assert native_lib.potts_uv_hist_stride(512) == 512 and native_lib.potts_uv_hist_stride(7) == 32
     assert native_lib.potts_uv_hist_span(512) == 511 * 512 + 512
     assert native_lib.potts_uv_hist_span(7) == 6 * 32 + 7 and native_lib.potts_uv_hist_span(1) == 1
+
+
+@pytest.mark.parametrize("flaw", ["decreasing_base", "unaligned_base", "rows_beyond_extent", "no_slices"])
+def test_static_energies_reject_bad_mappings_on_the_host(native_lib, flaw):
+    """potts_energies_static runs the solver's mapping checks before it touches the GPU: a
+    decreasing base[] would otherwise turn into ~2^32 rows and reads far outside u, V and Xi."""
+    import numpy as np
+
+    m = CylinderMapping.cylinder(8, 12, 12, 5.0)
+    base, start_row, n_images = m.base.copy(), m.start_row.copy(), m.n_images
+    c = m.col_begin + 2
+    if flaw == "decreasing_base":
+        base[c + 1] = base[c] - m.nstride
+    elif flaw == "unaligned_base":
+        base[c] += 1
+    elif flaw == "rows_beyond_extent":
+        start_row[c] = m.rows
+    else:
+        n_images = 0
+    bad = _native.PottsMapping(n_images, m.rows, m.cols, m.nstride, m.col_begin, m.col_end,
+                               start_row.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                               base.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+    ci = np.array([0.2, 0.5, 0.8], np.float32)
+    out = (ctypes.c_double * 3)()
+    fake = ctypes.c_void_p(0x1000)  # never dereferenced: the call is rejected on the host
+    st = native_lib.potts_energies_static(ctypes.byref(bad), fake, 3, ci.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                          30.0, fake, fake, None, out)
+    assert st == _native.POTTS_EINVAL, native_lib.potts_last_error()

@@ -48,7 +48,15 @@ def test_static_energies_match_solver_energies(cuda_device, K, variant):
                                 Xi_ptr=dX.data_ptr(), variant=variant, gap_every=iters)
     want = st.energy_trace[-1]
     first = _static_energies(m, du, ci, 30.0, dV, dX, stream)
+    # the second call allocates nothing: the device's free memory and torch's pool are unchanged
+    torch.cuda.synchronize(dev)
+    free_before, _ = torch.cuda.mem_get_info(dev)
+    reserved_before = torch.cuda.memory_reserved(dev)
     second = _static_energies(m, du, ci, 30.0, dV, dX, stream)
+    torch.cuda.synchronize(dev)
+    free_after, _ = torch.cuda.mem_get_info(dev)
+    assert free_after == free_before, (free_before, free_after)
+    assert torch.cuda.memory_reserved(dev) == reserved_before
     for got in (first, second):
         np.testing.assert_allclose(got[:2], want[:2], rtol=ENERGY_REL_TOL)
         np.testing.assert_allclose(got[2], want[2], rtol=1e-6, atol=1e-9)
