@@ -81,6 +81,21 @@ enum potts_storage {
                              outputs to FP32; potts_solve_device_f64 returns them in FP64. */
 };
 
+/* Arithmetic of the FP32 and 16-bit forms.  EXACT computes the reference's
+ * IEEE single-precision operations in the reference's order (multiply-adds
+ * fused where its clang build contracts them): every kernel form gives the
+ * same bits as the FP32 CPU oracle.  FAST computes the same iteration with
+ * fewer operations (the K-th label's terms derived from the others, no masks
+ * on terms that are zero by construction, a sort-free simplex threshold,
+ * reciprocal square roots in Dykstra's loop); it is held to the FP64 oracle
+ * (relative L2 of V within 1e-5 and the same labels off ties on the
+ * 128^3 case), and its split and fused forms give the same bits as each
+ * other.  The FP64 state ignores this option. */
+enum potts_arith {
+    POTTS_ARITH_EXACT = 0,
+    POTTS_ARITH_FAST = 1
+};
+
 typedef struct potts_options {
     int variant;      /* enum potts_variant */
     int storage;      /* enum potts_storage */
@@ -96,6 +111,11 @@ typedef struct potts_options {
                          (0 = default, < 0 = none, at most 16) */
     int autotune;     /* batches: 1 = time every compiled tile shape and segment length on the batch
                          and keep the fastest (used when no tile option is set); 0 = default tile */
+    int arith;        /* enum potts_arith (default EXACT) */
+    int stall_plane;  /* testing the bounded waits: > 0 makes the fused kernel's first work item skip
+                         the loads of that plane of its column march, so every wait for it gives up
+                         after its limit (about 2 s) and the solve returns POTTS_ETIMEOUT with the
+                         context still usable; 0 = off (default) */
 } potts_options;
 
 typedef struct potts_stats {

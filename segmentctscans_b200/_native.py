@@ -14,6 +14,8 @@ POTTS_OK, POTTS_EINVAL, POTTS_ENOMEM, POTTS_ECUDA, POTTS_ETIMEOUT, POTTS_ENODEV 
 VARIANT_FUSED, VARIANT_PLAIN = 0, 1
 STORE_F32, STORE_BF16, STORE_F16, STORE_F64 = 0, 1, 2, 3
 STORAGE = {"f32": STORE_F32, "bf16": STORE_BF16, "f16": STORE_F16, "f64": STORE_F64}
+ARITH_EXACT, ARITH_FAST = 0, 1
+ARITH = {"exact": ARITH_EXACT, "fast": ARITH_FAST}
 MAX_PHASES = 6
 
 
@@ -31,6 +33,7 @@ class PottsOptions(ctypes.Structure):
         ("slab_w", ctypes.c_int), ("track_dq", ctypes.c_int), ("sync_monitor", ctypes.c_int),
         ("tile_rows", ctypes.c_int), ("tile_slices", ctypes.c_int), ("segment_cols", ctypes.c_int),
         ("tile_vpt", ctypes.c_int), ("prefetch", ctypes.c_int), ("autotune", ctypes.c_int),
+        ("arith", ctypes.c_int), ("stall_plane", ctypes.c_int),
     ]
 
 
@@ -200,5 +203,9 @@ def default_options(**kw) -> PottsOptions:
             if v not in STORAGE:
                 raise ValueError(f"unknown storage {v!r}; one of {sorted(STORAGE)}")
             v = STORAGE[v]
+        if k == "arith" and isinstance(v, str):
+            if v not in ARITH:
+                raise ValueError(f"unknown arith {v!r}; one of {sorted(ARITH)}")
+            v = ARITH[v]
         setattr(o, k, int(v))
     return o

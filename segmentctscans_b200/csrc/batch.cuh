@@ -145,7 +145,7 @@ int batch_enqueue_head(potts_batch *b)
                                                                       batch_params<K>(bv, b->tau1));
         ctx->total_launches += 1;
         if (b->iters > 0) {
-            potts::dual_kernel<K, ST><<<nb, potts::kPlainThreads, 0, s>>>(bv.g, st.xi[0], st.v[0], b->tau2, ctx->thr);
+            launch_dual<K, ST>(b->opts.arith == POTTS_ARITH_FAST, nb, s, bv.g, st.xi[0], st.v[0], b->tau2, ctx->thr);
             ctx->total_launches += 1;
         }
     }
@@ -166,9 +166,8 @@ int batch_enqueue_tail(potts_batch *b, int cur)
         const PhaseParams<K> pp = batch_params<K>(bv, b->tau1);
         if (b->iters > 0) {
             float *dq = b->dq.p ? static_cast<float *>(b->dq.p) + v * (size_t)b->iters + (b->iters - 1) : nullptr;
-            potts::primal_kernel<K, ST><<<nb, potts::kPlainThreads, 0, s>>>(bv.g, st.xi[cur], st.v[cur],
-                                                                            (ST *)nullptr, bv.d_u, pp, dq,
-                                                                            b->iters - 1);
+            launch_primal<K, ST>(b->opts.arith == POTTS_ARITH_FAST, nb, s, bv.g, st.xi[cur], st.v[cur],
+                                 (ST *)nullptr, bv.d_u, pp, dq, b->iters - 1);
             ctx->total_launches += 1;
         }
         if (bv.res || bv.labels || bv.V) {
@@ -211,7 +210,7 @@ int batch_autotune(potts_batch *b, TileChoice *best)
             // one untimed launch, then kTrials timed ones
             for (int m = 0; m <= kTrials && rc == POTTS_OK; ++m) {
                 if (m == 1) cudaEventRecord(e0, ctx->stream);
-                rc = launch_tiled<K, ST>(ctx, tc, static_cast<const potts::FusedVolume<K, ST> *>(b->desc.p),
+                rc = launch_tiled<K, ST>(ctx, tc, b->opts.arith == POTTS_ARITH_FAST, static_cast<const potts::FusedVolume<K, ST> *>(b->desc.p),
                                          static_cast<const int4 *>(b->work.p), static_cast<const int *>(b->work_vol.p),
                                          b->n_work, m & 1, m, b->tau2);
             }
@@ -309,7 +308,7 @@ int batch_build(potts_batch *b)
     }
     POTTS_TRY((batch_plan_tiles<K, ST>(b, tile)));
     // the kernel's shared-memory attribute is set outside the capture
-    POTTS_TRY((launch_tiled<K, ST>(ctx, tile, nullptr, nullptr, nullptr, 0, 0, 0, b->tau2)));
+    POTTS_TRY((launch_tiled<K, ST>(ctx, tile, b->opts.arith == POTTS_ARITH_FAST, nullptr, nullptr, nullptr, 0, 0, 0, b->tau2)));
     POTTS_CUDA(cudaStreamSynchronize(ctx->stream));
 
     for (cudaEvent_t &e : b->ev) POTTS_CUDA(cudaEventCreate(&e));
@@ -337,7 +336,7 @@ int batch_capture(potts_batch *b, const TileChoice &tile)
             rc = batch_enqueue_head<K, ST>(b);
         } else if (part == 1) {
             for (int m = 1; m < b->iters && rc == POTTS_OK; ++m) {
-                rc = launch_tiled<K, ST>(ctx, tile, static_cast<const potts::FusedVolume<K, ST> *>(b->desc.p),
+                rc = launch_tiled<K, ST>(ctx, tile, b->opts.arith == POTTS_ARITH_FAST, static_cast<const potts::FusedVolume<K, ST> *>(b->desc.p),
                                          static_cast<const int4 *>(b->work.p), static_cast<const int *>(b->work_vol.p),
                                          b->n_work, cur, m - 1, b->tau2);
                 ctx->total_launches += 1;

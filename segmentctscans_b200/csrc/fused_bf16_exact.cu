@@ -1,0 +1,10 @@
+// Fused iteration kernels for the bf16 state with the exact arithmetic: every
+// compiled tile shape of K = 2 .. 6 (a translation unit of its own so that the
+// build compiles the kernel variants in parallel).
+#include "fused_launch.cuh"
+
+POTTS_FUSED_INSTANCES(2, __nv_bfloat16, false);
+POTTS_FUSED_INSTANCES(3, __nv_bfloat16, false);
+POTTS_FUSED_INSTANCES(4, __nv_bfloat16, false);
+POTTS_FUSED_INSTANCES(5, __nv_bfloat16, false);
+POTTS_FUSED_INSTANCES(6, __nv_bfloat16, false);

@@ -12,6 +12,7 @@
 #include "storage.cuh"
 #include "voxel.cuh"
 #include "voxel_f64.cuh"
+#include "voxel_fast.cuh"
 
 namespace potts {
 
@@ -57,8 +58,9 @@ __global__ void __launch_bounds__(kPlainThreads) init_kernel(Geometry g, const f
     }
 }
 
-// grad_kernel: Xi <- Pi_K(Xi + tau2 * grad+ Vbar), in place.
-template <int K, typename ST>
+// grad_kernel: Xi <- Pi_K(Xi + tau2 * grad+ Vbar), in place.  FAST: the fast
+// FP32 arithmetic (voxel_fast.cuh; missing neighbours read as zeros).
+template <int K, typename ST, bool FAST = false>
 __global__ void __launch_bounds__(kPlainThreads) dual_kernel(Geometry g, ST *__restrict__ xi,
                                                               const ST *__restrict__ vb, float tau2,
                                                               DykstraThresholds thr)
@@ -83,10 +85,16 @@ __global__ void __launch_bounds__(kPlainThreads) dual_kernel(Geometry g, ST *__r
     }
 #pragma unroll
     for (int j = 0; j < 3 * (K - 1); ++j) x[j] = Store<ST>::ld(xi[j * g.plane_w + o]);
-    if constexpr (std::is_same_v<R, double>)
+    if constexpr (std::is_same_v<R, double>) {
         dual_voxel_f64<K>(xo, x, vx, vn, vr, vc, hn, hr, hc, (double)tau2);
-    else
+    } else if constexpr (FAST) {
+        float q[K][3];
+        fast::dual_q<K, float>(q, x, vx, vn, vr, vc, hn ? tau2 : 0.0f, hr ? tau2 : 0.0f, hc ? tau2 : 0.0f);
+        if (fast::max_pair_dist2<K, float>(q) > 1.0f) fast::dual_project<K>(q);
+        dual_store<K>(xo, q);
+    } else {
         dual_voxel<K>(xo, x, vx, vn, vr, vc, hn, hr, hc, tau2, thr);
+    }
 #pragma unroll
     for (int j = 0; j < 3 * (K - 1); ++j) xi[j * g.plane_w + o] = Store<ST>::st(xo[j]);
 }
@@ -113,7 +121,7 @@ __device__ __forceinline__ void block_max_to(float v, float *dst)
 // div_kernel: V <- Pi_S(V + tau1 (div- Xi - G)), Vbar <- 2 V_new - V (optional),
 // max |dV|^2 into *dq (optional).  it: 0-based iteration (keys the stochastic
 // rounding of a bfloat16 V).
-template <int K, typename ST>
+template <int K, typename ST, bool FAST = false>
 __global__ void __launch_bounds__(kPlainThreads) primal_kernel(Geometry g, const ST *__restrict__ xi,
                                                                 ST *__restrict__ V, ST *__restrict__ Vb,
                                                                 const float *__restrict__ u, PhaseParams<K> pp,
@@ -147,6 +155,8 @@ __global__ void __launch_bounds__(kPlainThreads) primal_kernel(Geometry g, const
         if constexpr (std::is_same_v<R, double>)
             d = (float)primal_voxel_f64<K>(vnew, vbar, v, x, xn, xr, xc, pn, hn, pr, hr, pc, hc, (double)uu, pp.c,
                                            (double)pp.lam, (double)pp.tau1);
+        else if constexpr (FAST)
+            d = fast::primal<K, float>(vnew, vbar, v, x, xn, xr, xc, pc ? -1.0f : -0.0f, uu, pp.c, pp.lam, pp.tau1);
         else
             d = primal_voxel<K>(vnew, vbar, v, x, xn, xr, xc, pn, hn, pr, hr, pc, hc, uu, pp.c, pp.lam, pp.tau1);
         uint32_t h[(K - 1 + 1) / 2];
@@ -291,7 +301,8 @@ __global__ void __launch_bounds__(kPlainThreads) energy_kernel(Geometry g, const
 // Adds the block partials in a fixed order (one block of 1024 threads: each
 // thread a contiguous range, then a fixed tree), so the result is
 // deterministic; writes (lagrangian, dual, gap) to out[0..2].
-__global__ void __launch_bounds__(1024) energy_finish(const double2 *__restrict__ partial, int64_t count,
+// (internal linkage: the header is included by several translation units)
+static __global__ void __launch_bounds__(1024) energy_finish(const double2 *__restrict__ partial, int64_t count,
                                                       double *out)
 {
     __shared__ double2 red[1024];

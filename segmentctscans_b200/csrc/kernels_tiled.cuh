@@ -52,6 +52,7 @@
 #include "storage.cuh"
 #include "tma.cuh"
 #include "voxel.cuh"
+#include "voxel_fast.cuh"
 
 namespace potts {
 
@@ -69,6 +70,7 @@ struct TiledParams {
     int n_base;     // global slice of the slab's slice 0
     int it;         // 0-based iteration of the launch's primal step (keys stochastic rounding)
     int prefetch;   // planes ahead of the load ring prefetched into L2 (0: none)
+    int stall_plane;  // testing: > 0 = the first work item never loads that ring position (0: off)
 };
 
 template <int K, int R, int NT, int VPT, typename ST>
@@ -85,8 +87,13 @@ struct TileShape {
     static constexpr int HALO_WARPS = (Q + 31) / 32;  // the high halo row (and the slice n0+NT)
     static constexpr int PRODUCER_WARP = MAIN_WARPS + HALO_WARPS;
     // Dykstra warps run the projection loop of queued voxels; row warp r
-    // queues for Dykstra warp r % NW
-    static constexpr int NW = MAIN_WARPS >= 12 ? 6 : (MAIN_WARPS >= 2 ? MAIN_WARPS / 2 : 1);
+    // queues for Dykstra warp r % NW (about 5 % of the voxels need the loop,
+    // 2.5 sweeps on average: a few warps running full batches keep up)
+#ifdef POTTS_DYKSTRA_WARPS
+    static constexpr int NW = MAIN_WARPS >= 2 * POTTS_DYKSTRA_WARPS ? POTTS_DYKSTRA_WARPS : (MAIN_WARPS >= 2 ? MAIN_WARPS / 2 : 1);
+#else
+    static constexpr int NW = MAIN_WARPS >= 12 ? 3 : (MAIN_WARPS >= 4 ? 2 : 1);
+#endif
     static constexpr int DYKSTRA_WARP = PRODUCER_WARP + 1;  // the first one
     static constexpr int THREADS = MAIN + 32 * HALO_WARPS + 32 + 32 * NW;
     static constexpr int QSTRIDE = (3 * K + 1) | 1;  // queue entry: q (3K floats) + state offset; odd stride
@@ -223,7 +230,7 @@ struct TiledSmem {
 // Stage A for VPT consecutive slices n0+VPT*q .. of tile row rr (row r0+rr).
 // Planes are indexed by "ring position" p = c - ca + 1 (plane ca-1 is p = 0);
 // sc and sp are the ring slots of planes p and p-1.
-template <int K, int R, int NT, int VPT, typename ST>
+template <int K, int R, int NT, int VPT, typename ST, bool FAST>
 __device__ __forceinline__ void stage_a_chunk(const TiledSmem<K, R, NT, VPT, ST> &sm, const TiledParams &tp,
                                               const PhaseParams<K> &pp, int p, int sc, int sp, int r0, int rr,
                                               int n0, int q, bool store_v, ST *__restrict__ Vout, float &dqmax)
@@ -252,7 +259,46 @@ __device__ __forceinline__ void stage_a_chunk(const TiledSmem<K, R, NT, VPT, ST>
     constexpr int XH = S::XH;
 
     float onew[K - 1][VPT], obar[K - 1][VPT];
-    if constexpr (VPT == 2) {
+    if constexpr (FAST) {
+        // fast arithmetic, two slices at a time with paired FP32 instructions;
+        // the backward n and row terms read zeros where the neighbour is missing
+        float x[S::C3][VPT], xn[K - 1][VPT], xr[K - 1][VPT], xc[K - 1][VPT], v[K - 1][VPT], u[VPT];
+#pragma unroll
+        for (int comp = 0; comp < S::C3; ++comp) ldv<VPT>(x[comp], xs + T::xi_at(comp, rr + 1, off + XH));
+#pragma unroll
+        for (int i = 0; i < K - 1; ++i) {
+            ldv<VPT>(xn[i], xs + T::xi_at(3 * i, rr + 1, off + XH - VPT));  // slices nb-VPT .. nb-1
+            ldv<VPT>(xr[i], xs + T::xi_at(3 * i + 1, rr, off + XH));
+            ldv<VPT>(xc[i], xp + T::xi_at(3 * i + 2, rr + 1, off + XH));
+            ldv<VPT>(v[i], vs + T::vt_at(i, rr, off));
+        }
+        ldv<VPT>(u, us + T::v_at(0, rr, off));
+        const float2 mpc = f2(pc ? -1.0f : -0.0f);
+#pragma unroll
+        for (int j = 0; j < VPT; j += 2) {
+            float2 xj[S::C3], xinj[K - 1], xrj[K - 1], xcj[K - 1], vj[K - 1], vn[K - 1], vbar[K - 1];
+#pragma unroll
+            for (int comp = 0; comp < S::C3; ++comp) xj[comp] = f2(x[comp][j], x[comp][j + 1]);
+#pragma unroll
+            for (int i = 0; i < K - 1; ++i) {
+                xinj[i] = f2(j == 0 ? xn[i][VPT - 1] : x[3 * i][j - 1], x[3 * i][j]);
+                xrj[i] = f2(xr[i][j], xr[i][j + 1]);
+                xcj[i] = f2(xc[i][j], xc[i][j + 1]);
+                vj[i] = f2(v[i][j], v[i][j + 1]);
+            }
+            const float2 d = fast::primal<K, float2>(vn, vbar, vj, xj, xinj, xrj, xcj, mpc, f2(u[j], u[j + 1]), pp.c,
+                                                    pp.lam, pp.tau1);
+            const bool in0 = nb + j < tp.ns, in1 = nb + j + 1 < tp.ns;
+            if (store_v) dqmax = fmaxf(dqmax, in0 ? (in1 ? fmaxf(d.x, d.y) : d.x) : 0.0f);
+#pragma unroll
+            for (int i = 0; i < K - 1; ++i) {
+                onew[i][j] = in0 ? vn[i].x : 0.0f;
+                obar[i][j] = in0 ? Store<ST>::round(vbar[i].x) : 0.0f;  // Vbar as if stored
+                onew[i][j + 1] = in1 ? vn[i].y : 0.0f;
+                obar[i][j + 1] = in1 ? Store<ST>::round(vbar[i].y) : 0.0f;
+            }
+        }
+    } else if constexpr (VPT == 2) {
         // both slices with paired FP32 instructions
         float2 x[S::C3], xin[K - 1], xr[K - 1], xc[K - 1], v[K - 1], vn[K - 1], vbar[K - 1];
 #pragma unroll
@@ -364,7 +410,7 @@ __device__ __forceinline__ void stage_a_chunk(const TiledSmem<K, R, NT, VPT, ST>
 }
 
 // Stage A for the single slice n0+NT of tile row rr (the high halo along n).
-template <int K, int R, int NT, int VPT, typename ST>
+template <int K, int R, int NT, int VPT, typename ST, bool FAST>
 __device__ __forceinline__ void stage_a_nhalo(const TiledSmem<K, R, NT, VPT, ST> &sm, const TiledParams &tp,
                                               const PhaseParams<K> &pp, int p, int sc, int sp, int r0, int rr, int n0)
 {
@@ -394,25 +440,36 @@ __device__ __forceinline__ void stage_a_nhalo(const TiledSmem<K, R, NT, VPT, ST>
         v[i] = Store<ST>::ld(sm.v_slot(sc)[T::vt_at(i, rr, NT)]);
     }
     const float uu = sm.u_slot(sc)[T::v_at(0, rr, NT)];
-    primal_voxel<K>(vn, vbar, v, xi, xin, xir, xic, n > 0, n + 1 < tp.ns, pr, hr, pc, hc, uu, pp.c, pp.lam, pp.tau1);
+    if constexpr (FAST)
+        fast::primal<K, float>(vn, vbar, v, xi, xin, xir, xic, pc ? -1.0f : -0.0f, uu, pp.c, pp.lam, pp.tau1);
+    else
+        primal_voxel<K>(vn, vbar, v, xi, xin, xir, xic, n > 0, n + 1 < tp.ns, pr, hr, pc, hc, uu, pp.c, pp.lam,
+                        pp.tau1);
 #pragma unroll
     for (int i = 0; i < K - 1; ++i) vb[T::v_at(i, rr, NT)] = Store<ST>::round(vbar[i]);
 }
 
 // The Dykstra warp: runs the projection loop of the voxels that the row warps
-// queue.  Each lane takes one voxel, runs it a sweep at a time and, once it is
-// done, stores the result and takes the next waiting ticket, so that the loop
-// work of the block proceeds beside the stencil instead of stalling a row
-// warp.  It returns when every row warp has finished and the queue is empty,
-// or when the block aborts.  Every wait is bounded.
+// queue.  It sleeps until a batch of kBatch voxels has gathered in its queue
+// (or the row warps are done), then each lane takes one voxel, runs it a
+// sweep at a time and, once it is done, stores the result and takes the next
+// waiting ticket, until the queue is empty and every lane has finished.  Work
+// therefore runs in full batches instead of a sweep per arriving voxel, so
+// few warp instructions are issued with one or two lanes active.  It returns
+// when every row warp has finished and the queue is empty, or when the block
+// aborts.  Every wait is bounded.
 constexpr int kQueueSpin = 1 << 20;   // polls of an entry's publication flag
-constexpr int kIdleRounds = 1 << 24;  // idle polls (~200 ns each) while the row warps work
+constexpr int kIdleRounds = 1 << 23;  // idle polls (~400 ns each) while the row warps work
+#ifdef POTTS_DYKSTRA_BATCH
+constexpr uint32_t kBatch = POTTS_DYKSTRA_BATCH;
+#else
+constexpr uint32_t kBatch = 32;  // queued voxels that start a batch
+#endif
 
-template <int K, int R, int NT, int VPT, typename ST>
+template <int K, int R, int NT, int VPT, typename ST, bool FAST>
 __device__ __forceinline__ void dykstra_worker(const TiledSmem<K, R, NT, VPT, ST> &sm, int w, const TiledParams &tp,
                                                DykstraThresholds thr, ST *__restrict__ Xout, volatile int *abort)
 {
-    using S = TileShape<K, R, NT, VPT, ST>;
     constexpr int kPairs = K * (K - 1) / 2;
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
@@ -422,13 +479,31 @@ __device__ __forceinline__ void dykstra_worker(const TiledSmem<K, R, NT, VPT, ST
     float qe[K][3], P[kPairs][3];
     int64_t o = 0;
     int sweeps = 0;
-    bool active = false;
+    bool active = false, batch = false;
     uint32_t next = 0;  // next ticket to hand out (the same in every lane)
     int idle_rounds = 0;
     while (true) {
-        const uint32_t tail = __shfl_sync(0xffffffffu, *tail_v, 0);
+        if (!batch) {
+            // a row warp publishes its last entries before it counts itself
+            // done, so `done` is read before the tail
+            const bool done = __shfl_sync(0xffffffffu, (int)(*done_v == T::q_writers(w)), 0) != 0;
+            const uint32_t avail = __shfl_sync(0xffffffffu, *tail_v, 0) - next;
+            if (avail >= kBatch || (done && avail > 0u)) {
+                batch = true;
+            } else if (done || __shfl_sync(0xffffffffu, *abort, 0)) {
+                break;
+            } else {
+                if (++idle_rounds > kIdleRounds) {
+                    *abort = 1;
+                    break;
+                }
+                __nanosleep(400);
+                continue;
+            }
+            idle_rounds = 0;
+        }
+        const uint32_t avail = __shfl_sync(0xffffffffu, *tail_v, 0) - next;
         const unsigned idle = __ballot_sync(0xffffffffu, !active);
-        const uint32_t avail = tail - next;
         if (avail > 0u && idle != 0u) {
             const uint32_t take = min((uint32_t)__popc(idle), avail);
             const uint32_t rank = (uint32_t)__popc(idle & below);
@@ -465,21 +540,16 @@ __device__ __forceinline__ void dykstra_worker(const TiledSmem<K, R, NT, VPT, ST
             if (lane == 0) *sm.q_head(w) = next;  // the taken entries' slots are free again
         }
         if (!__any_sync(0xffffffffu, active)) {
+            batch = false;  // the queue ran dry: wait for the next batch
             if (__shfl_sync(0xffffffffu, *abort, 0)) break;
-            // a row warp publishes its last entries before it counts itself done
-            const bool finished =
-                __shfl_sync(0xffffffffu, (int)(*done_v == T::q_writers(w) && *tail_v == next), 0) != 0;
-            if (finished) break;
-            if (++idle_rounds > kIdleRounds) {
-                *abort = 1;
-                break;
-            }
-            __nanosleep(200);
             continue;
         }
-        idle_rounds = 0;
         if (active) {
-            const bool exit = dykstra_sweep<K>(qe, P, thr);
+            bool exit;
+            if constexpr (FAST)
+                exit = fast::dykstra_sweep<K>(qe, P);
+            else
+                exit = dykstra_sweep<K>(qe, P, thr);
             if (exit || ++sweeps == 20) {
 #pragma unroll
                 for (int i = 0; i < K - 1; ++i)
@@ -495,7 +565,7 @@ __device__ __forceinline__ void dykstra_worker(const TiledSmem<K, R, NT, VPT, ST
 // for VPT slices n0+VPT*q .. of tile row rr.  Called by every lane of the row
 // warps (warp-wide ballots); voxels that need the projection loop go to the
 // block's queue.
-template <int K, int R, int NT, int VPT, typename ST>
+template <int K, int R, int NT, int VPT, typename ST, bool FAST>
 __device__ __forceinline__ void stage_b_chunk(const TiledSmem<K, R, NT, VPT, ST> &sm, const TiledParams &tp, int p,
                                               int sc, int sn, int r0, int rr, int n0, int q, float tau2,
                                               DykstraThresholds thr, ST *__restrict__ Xout)
@@ -518,7 +588,44 @@ __device__ __forceinline__ void stage_b_chunk(const TiledSmem<K, R, NT, VPT, ST>
         const ST *xs = sm.xi_slot(sc);
         const float *vb0 = sm.vb_plane(sc), *vb1 = sm.vb_plane(sn);
         constexpr int XH = S::XH;
-        if constexpr (VPT == 2) {
+        if constexpr (FAST) {
+            float x[S::C3][VPT], b[K - 1][VPT], bnext[K - 1], br[K - 1][VPT], bc[K - 1][VPT];
+#pragma unroll
+            for (int comp = 0; comp < S::C3; ++comp) ldv<VPT>(x[comp], xs + T::xi_at(comp, rr + 1, off + XH));
+#pragma unroll
+            for (int i = 0; i < K - 1; ++i) {
+                ldv<VPT>(b[i], vb0 + T::v_at(i, rr, off));
+                bnext[i] = vb0[T::v_at(i, rr, off + VPT)];
+                ldv<VPT>(br[i], vb0 + T::v_at(i, rr + 1, off));
+                ldv<VPT>(bc[i], vb1 + T::v_at(i, rr, off));
+            }
+            const float2 t2r = f2(hr ? tau2 : 0.0f), t2c = f2(hc ? tau2 : 0.0f);
+#pragma unroll
+            for (int j = 0; j < VPT; j += 2) {
+                float2 xj[S::C3], bj[K - 1], bnj[K - 1], brj[K - 1], bcj[K - 1], q2[K][3];
+#pragma unroll
+                for (int comp = 0; comp < S::C3; ++comp) xj[comp] = f2(x[comp][j], x[comp][j + 1]);
+#pragma unroll
+                for (int i = 0; i < K - 1; ++i) {
+                    bj[i] = f2(b[i][j], b[i][j + 1]);
+                    bnj[i] = f2(b[i][j + 1], j + 2 < VPT ? b[i][j + 2] : bnext[i]);
+                    brj[i] = f2(br[i][j], br[i][j + 1]);
+                    bcj[i] = f2(bc[i][j], bc[i][j + 1]);
+                }
+                const float2 t2n = f2(nb + j + 1 < tp.ns ? tau2 : 0.0f, nb + j + 2 < tp.ns ? tau2 : 0.0f);
+                fast::dual_q<K, float2>(q2, xj, bj, bnj, brj, bcj, t2n, t2r, t2c);
+                const float2 m = fast::max_pair_dist2<K, float2>(q2);
+                if (m.x > 1.0f && nb + j < tp.ns) need |= 1u << j;
+                if (m.y > 1.0f && nb + j + 1 < tp.ns) need |= 2u << j;
+#pragma unroll
+                for (int i = 0; i < K; ++i)
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        qv[j][i][a] = q2[i][a].x;
+                        qv[j + 1][i][a] = q2[i][a].y;
+                    }
+            }
+        } else if constexpr (VPT == 2) {
             float2 x[S::C3], b[K - 1], bn[K - 1], br[K - 1], bc[K - 1], q2[K][3];
 #pragma unroll
             for (int comp = 0; comp < S::C3; ++comp)
@@ -610,7 +717,10 @@ __device__ __forceinline__ void stage_b_chunk(const TiledSmem<K, R, NT, VPT, ST>
                 __threadfence_block();
                 *sm.queue_seq(w, ticket) = ticket + 1u;
             } else {
-                dual_project<K>(qv[j], thr);
+                if constexpr (FAST)
+                    fast::dual_project<K>(qv[j]);
+                else
+                    dual_project<K>(qv[j], thr);
 #pragma unroll
                 for (int i = 0; i < K - 1; ++i)
 #pragma unroll
@@ -660,7 +770,7 @@ struct FusedVolume {
 // null); the items of every volume of a batch share one launch, and the
 // block scheduler hands them out as blocks finish.  The launch turns
 // (Xi^m, V^{m-1}) in half `in` into (Xi^{m+1}, V^m) in half in ^ 1; it = m - 1.
-template <int K, int R, int NT, int VPT, typename ST>
+template <int K, int R, int NT, int VPT, typename ST, bool FAST>
 __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
     fused_tiled_kernel(const FusedVolume<K, ST> *__restrict__ vols, const int4 *__restrict__ work,
                        const int *__restrict__ work_vol, int in, int it, float tau2, DykstraThresholds thr, int *err)
@@ -738,6 +848,8 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
                     const int c = ca - 1 + p;
                     if (p == 0 && c < tp.col_begin) {  // no plane before the first column
                         mbar_arrive(sm.full(0));
+                    } else if (p == tp.stall_plane && blockIdx.x == 0) {
+                        // testing: this plane never arrives, so the waits for it run out
                     } else {
                         const int4 ci = sm.cols()[p];
                         const int line = ci.x + (r0 - 1 - ci.y);  // line of row r0-1 in column c
@@ -771,7 +883,7 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
                 }
             }
         } else if (warp >= S::DYKSTRA_WARP) {
-            dykstra_worker<K, R, NT, VPT, ST>(sm, warp - S::DYKSTRA_WARP, tp, thr, Xout, abort);
+            dykstra_worker<K, R, NT, VPT, ST, FAST>(sm, warp - S::DYKSTRA_WARP, tp, thr, Xout, abort);
         } else {
             const bool is_main = warp < S::MAIN_WARPS;
             const int hq = tid - S::MAIN;  // chunk of the halo row (halo warps)
@@ -789,9 +901,9 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
                     if (ok) ok = mbar_wait_warp(sm.full(s_cur), ph_cur, abort);
                     if (!ok) break;
                     if (chunk_a)
-                        stage_a_chunk<K, R, NT, VPT, ST>(sm, tp, pp, p, s_cur, s_prev, r0, rr, n0, q,
+                        stage_a_chunk<K, R, NT, VPT, ST, FAST>(sm, tp, pp, p, s_cur, s_prev, r0, rr, n0, q,
                                                          is_main && ca - 1 + p < cb, Vout, dqmax);
-                    if (nhalo) stage_a_nhalo<K, R, NT, VPT, ST>(sm, tp, pp, p, s_cur, s_prev, r0, hq, n0);
+                    if (nhalo) stage_a_nhalo<K, R, NT, VPT, ST, FAST>(sm, tp, pp, p, s_cur, s_prev, r0, hq, n0);
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(sm.ready(s_cur));
@@ -800,7 +912,7 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
                         // dual step at position p-1 once every warp's Vbar of that plane is in
                         ok = mbar_wait_warp(sm.ready(s_prev), ph_prev, abort);
                         if (!ok) break;
-                        stage_b_chunk<K, R, NT, VPT, ST>(sm, tp, p - 1, s_prev, s_cur, r0, rr, n0, q, tau2, thr,
+                        stage_b_chunk<K, R, NT, VPT, ST, FAST>(sm, tp, p - 1, s_prev, s_cur, r0, rr, n0, q, tau2, thr,
                                                          Xout);
                     }
                     __syncwarp();
@@ -816,7 +928,7 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
             if (ok && is_main && c_last == cb - 1) {
                 ok = mbar_wait_warp(sm.ready(s_prev), ph_prev, abort);
                 if (ok)
-                    stage_b_chunk<K, R, NT, VPT, ST>(sm, tp, P, s_prev, s_cur, r0, rr, n0, q, tau2, thr, Xout);
+                    stage_b_chunk<K, R, NT, VPT, ST, FAST>(sm, tp, P, s_prev, s_cur, r0, rr, n0, q, tau2, thr, Xout);
             }
             if (is_main) {  // this warp queues nothing more (also after an abort)
                 __syncwarp();
@@ -832,9 +944,16 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
     }
 }
 
+// One launch of fused_tiled_kernel<K, R, NT, VPT, ST, FAST> over n_work
+// items on `stream`.  Defined in fused_launch.cuh and instantiated for the
+// compiled tile shapes in the fused_*.cu translation units.
+template <int K, int R, int NT, int VPT, typename ST, bool FAST>
+cudaError_t launch_fused(cudaStream_t stream, const FusedVolume<K, ST> *vols, const int4 *work, const int *work_vol,
+                         int n_work, int in, int it, float tau2, DykstraThresholds thr, int *err);
+
 // Copies the slab's part of u into a buffer with the state's stride, so that
 // every TMA box of u starts on a 16-byte boundary.
-__global__ void stage_u_kernel(Geometry g, const float *__restrict__ u, float *__restrict__ out)
+static __global__ void stage_u_kernel(Geometry g, const float *__restrict__ u, float *__restrict__ out)
 {
     const PlainIndex p = plain_index(g, 0, g.ns);
     if (!p.valid) return;

@@ -17,6 +17,7 @@
 #include "kernels_plain.cuh"
 #include "kernels_adjoint.cuh"
 #include "kernels_tiled.cuh"
+#include "tile_shapes.cuh"
 #include "kernels_hist.cuh"
 #include "kernels_tv.cuh"
 #include "kernels_fieldio.cuh"
@@ -27,6 +28,7 @@
 __attribute__((visibility("hidden"))) void potts_set_last_error(const std::string &msg);
 
 using potts::DykstraThresholds;
+using potts::ShapesOf;
 using potts::Geometry;
 using potts::PhaseParams;
 
@@ -421,23 +423,6 @@ struct TileChoice {
     int rows, slices, vpt, segment;
 };
 
-// Tile shapes compiled per K and state width (rows x slices x voxels per
-// thread; W = 4 for FP32, 2 for the 16-bit formats); the first entry is the
-// default.
-template <int K, int W>
-struct TileShapes;
-template <int W> struct TileShapes<2, W> { static constexpr int n = 2; static constexpr int r[n] = {8, 8}, t[n] = {128, 64}, v[n] = {2, 4}; };
-template <> struct TileShapes<3, 4> { static constexpr int n = 4; static constexpr int r[n] = {16, 8, 8, 8}, t[n] = {64, 128, 64, 128}, v[n] = {2, 2, 2, 4}; };
-template <> struct TileShapes<3, 2> { static constexpr int n = 2; static constexpr int r[n] = {16, 8}, t[n] = {64, 128}, v[n] = {2, 2}; };
-template <> struct TileShapes<4, 4> { static constexpr int n = 3; static constexpr int r[n] = {8, 8, 4}, t[n] = {64, 64, 128}, v[n] = {2, 4, 4}; };
-template <> struct TileShapes<4, 2> { static constexpr int n = 1; static constexpr int r[n] = {8}, t[n] = {64}, v[n] = {2}; };
-template <int W> struct TileShapes<5, W> { static constexpr int n = 2; static constexpr int r[n] = {4, 8}, t[n] = {64, 64}, v[n] = {4, 2}; };
-template <> struct TileShapes<6, 4> { static constexpr int n = 1; static constexpr int r[n] = {4}, t[n] = {64}, v[n] = {4}; };
-template <> struct TileShapes<6, 2> { static constexpr int n = 2; static constexpr int r[n] = {4, 8}, t[n] = {64, 64}, v[n] = {4, 2}; };
-
-template <int K, typename ST>
-using ShapesOf = TileShapes<K, (int)sizeof(ST) == 4 ? 4 : 2>;
-
 template <int K, typename ST>
 int choose_tile(const potts_options &o, TileChoice *tc)
 {
@@ -548,35 +533,26 @@ struct FusedPlan {
 };
 
 // One launch of the fused kernel over n_work items (work / work_vol on the
-// device), volumes in `vols`.
-template <int K, int R, int NT, int VPT, typename ST>
-int launch_tiled_shape(potts_context *ctx, const potts::FusedVolume<K, ST> *vols, const int4 *work,
-                       const int *work_vol, int n_work, int in, int it, float tau2)
-{
-    using S = potts::TileShape<K, R, NT, VPT, ST>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        POTTS_CUDA(cudaFuncSetAttribute(potts::fused_tiled_kernel<K, R, NT, VPT, ST>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM_ALLOC));
-        attr_set = true;
-    }
-    if (n_work == 0) return POTTS_OK;
-    potts::fused_tiled_kernel<K, R, NT, VPT, ST><<<n_work, S::THREADS, S::SMEM_ALLOC, ctx->stream>>>(
-        vols, work, work_vol, in, it, tau2, ctx->thr, (int *)ctx->err.p);
-    POTTS_CUDA(cudaGetLastError());
-    return POTTS_OK;
-}
-
+// device), volumes in `vols`; `fast` selects the fast arithmetic.
 template <int K, typename ST, int I = 0>
-int launch_tiled(potts_context *ctx, const TileChoice &tile, const potts::FusedVolume<K, ST> *vols,
+int launch_tiled(potts_context *ctx, const TileChoice &tile, bool fast, const potts::FusedVolume<K, ST> *vols,
                  const int4 *work, const int *work_vol, int n_work, int in, int it, float tau2)
 {
     using TS = ShapesOf<K, ST>;
     if constexpr (I < TS::n) {
         constexpr int R = TS::r[I], NT = TS::t[I], VPT = TS::v[I];
-        if (tile.rows == R && tile.slices == NT && tile.vpt == VPT)
-            return launch_tiled_shape<K, R, NT, VPT, ST>(ctx, vols, work, work_vol, n_work, in, it, tau2);
-        return launch_tiled<K, ST, I + 1>(ctx, tile, vols, work, work_vol, n_work, in, it, tau2);
+        if (tile.rows == R && tile.slices == NT && tile.vpt == VPT) {
+            const cudaError_t e =
+                fast ? potts::launch_fused<K, R, NT, VPT, ST, true>(ctx->stream, vols, work, work_vol, n_work, in, it,
+                                                                    tau2, ctx->thr, (int *)ctx->err.p)
+                     : potts::launch_fused<K, R, NT, VPT, ST, false>(ctx->stream, vols, work, work_vol, n_work, in,
+                                                                     it, tau2, ctx->thr, (int *)ctx->err.p);
+            if (e != cudaSuccess)
+                return fail(e == cudaErrorMemoryAllocation ? POTTS_ENOMEM : POTTS_ECUDA,
+                            std::string("fused kernel launch: ") + cudaGetErrorString(e));
+            return POTTS_OK;
+        }
+        return launch_tiled<K, ST, I + 1>(ctx, tile, fast, vols, work, work_vol, n_work, in, it, tau2);
     } else {
         return fail(POTTS_EINVAL, "no compiled tile shape matches");
     }
@@ -663,9 +639,39 @@ int prepare_fused(potts_context *ctx, const Geometry &g, const ST *const xi[2], 
     uint64_t ustride;
     int ux0;
     POTTS_TRY(fused_u_source(ctx, g, d_u, ctx->ustage, &ubase, &ustride, &ux0));
-    return build_volume<K, ST>(g, (const int4 *)ctx->cols.p, (int)ctx->mapping.m.col_begin,
-                               (int)ctx->mapping.m.col_end, xi, v, ubase, ustride, ux0, fp->tile, pp, dq, o.prefetch,
-                               &fp->vol);
+    POTTS_TRY((build_volume<K, ST>(g, (const int4 *)ctx->cols.p, (int)ctx->mapping.m.col_begin,
+                                   (int)ctx->mapping.m.col_end, xi, v, ubase, ustride, ux0, fp->tile, pp, dq,
+                                   o.prefetch, &fp->vol)));
+    fp->vol.tp.stall_plane = o.stall_plane;
+    return POTTS_OK;
+}
+
+// Split-kernel launches in the exact or the fast arithmetic (the FP64 state
+// has only the exact one).
+template <int K, typename ST>
+void launch_dual(bool fast, unsigned nb, cudaStream_t s, const Geometry &g, ST *xi, const ST *vb, float tau2,
+                 DykstraThresholds thr)
+{
+    if constexpr (!std::is_same_v<ST, double>) {
+        if (fast) {
+            potts::dual_kernel<K, ST, true><<<nb, potts::kPlainThreads, 0, s>>>(g, xi, vb, tau2, thr);
+            return;
+        }
+    }
+    potts::dual_kernel<K, ST, false><<<nb, potts::kPlainThreads, 0, s>>>(g, xi, vb, tau2, thr);
+}
+
+template <int K, typename ST>
+void launch_primal(bool fast, unsigned nb, cudaStream_t s, const Geometry &g, const ST *xi, ST *V, ST *Vb,
+                   const float *u, const PhaseParams<K> &pp, float *dq, int it)
+{
+    if constexpr (!std::is_same_v<ST, double>) {
+        if (fast) {
+            potts::primal_kernel<K, ST, true><<<nb, potts::kPlainThreads, 0, s>>>(g, xi, V, Vb, u, pp, dq, it);
+            return;
+        }
+    }
+    potts::primal_kernel<K, ST, false><<<nb, potts::kPlainThreads, 0, s>>>(g, xi, V, Vb, u, pp, dq, it);
 }
 
 // One slab: init, iters iterations, argmax of [res_begin, res_end).
@@ -682,6 +688,7 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
     cudaStream_t s = ctx->stream;
     if (dq && iters > 0) POTTS_CUDA(cudaMemsetAsync(dq, 0, sizeof(float) * iters, s));
 
+    const bool fast = o.arith == POTTS_ARITH_FAST;
     int cur = 0;
     if (o.variant == POTTS_VARIANT_PLAIN || std::is_same_v<ST, double>) {
         ST *xi = st.xi[0], *V = st.v[0], *Vb = st.v[1];
@@ -690,8 +697,8 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
         POTTS_CUDA(cudaMemsetAsync(xi, 0, xi_bytes, s));
         for (int it = 0; it < iters; ++it) {
             POTTS_TRY(seg_begin(ctx));
-            potts::dual_kernel<K, ST><<<nb, potts::kPlainThreads, 0, s>>>(g, xi, Vb, tau2, ctx->thr);
-            potts::primal_kernel<K, ST><<<nb, potts::kPlainThreads, 0, s>>>(g, xi, V, Vb, d_u, pp, dq ? dq + it : nullptr, it);
+            launch_dual<K, ST>(fast, nb, s, g, xi, Vb, tau2, ctx->thr);
+            launch_primal<K, ST>(fast, nb, s, g, xi, V, Vb, d_u, pp, dq ? dq + it : nullptr, it);
             ctx->loop_launches += 2;
             ctx->total_launches += 2;
             if (ge > 0 && (it + 1) % ge == 0) POTTS_TRY(run_energy<K>(ctx, g, xi, V, d_u, pp, energy + 3 * ((it + 1) / ge - 1)));
@@ -717,7 +724,7 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
         ctx->total_launches += 1;
         POTTS_CUDA(cudaMemsetAsync(st.xi[0], 0, xi_bytes, s));
         if (iters > 0) {
-            potts::dual_kernel<K, ST><<<nb, potts::kPlainThreads, 0, s>>>(g, st.xi[0], st.v[0], tau2, ctx->thr);
+            launch_dual<K, ST>(fast, nb, s, g, st.xi[0], st.v[0], tau2, ctx->thr);
             ctx->total_launches += 1;
         }
         for (int m = 1; m < iters; ++m) {
@@ -725,7 +732,7 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
             POTTS_TRY(seg_begin(ctx));
             ctx->loop_launches += 1;
             ctx->total_launches += 1;
-            POTTS_TRY((launch_tiled<K, ST>)(ctx, fp.tile, (const potts::FusedVolume<K, ST> *)ctx->vols.p,
+            POTTS_TRY((launch_tiled<K, ST>)(ctx, fp.tile, fast, (const potts::FusedVolume<K, ST> *)ctx->vols.p,
                                             (const int4 *)ctx->work.p, nullptr, fp.n_work, cur, m - 1, tau2));
             if (ge > 0 && m % ge == 0) POTTS_TRY(run_energy<K>(ctx, g, st.xi[cur], st.v[nxt], d_u, pp, energy + 3 * (m / ge - 1)));
             if (o.sync_monitor && dq) POTTS_TRY(monitor_sync<K>(ctx, m - 1));
@@ -734,8 +741,8 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
         POTTS_TRY(seg_end(ctx));
         if (iters > 0) {
             ctx->total_launches += 1;
-            potts::primal_kernel<K, ST><<<nb, potts::kPlainThreads, 0, s>>>(
-                g, st.xi[cur], st.v[cur], (ST *)nullptr, d_u, pp, dq ? dq + (iters - 1) : nullptr, iters - 1);
+            launch_primal<K, ST>(fast, nb, s, g, st.xi[cur], st.v[cur], (ST *)nullptr, d_u, pp,
+                                 dq ? dq + (iters - 1) : nullptr, iters - 1);
             if (ge > 0 && iters % ge == 0) POTTS_TRY(run_energy<K>(ctx, g, st.xi[cur], st.v[cur], d_u, pp, energy + 3 * (iters / ge - 1)));
             if (o.sync_monitor && dq) POTTS_TRY(monitor_sync<K>(ctx, iters - 1));
         }
@@ -888,6 +895,8 @@ int check_params(int K, const float *ci, float lam, float tau1, float tau2, int 
     if (o.tile_rows < 0 || o.tile_slices < 0 || o.segment_cols < 0 || o.tile_vpt < 0)
         return fail(POTTS_EINVAL, "tile options must be >= 0");
     if (o.prefetch > 16) return fail(POTTS_EINVAL, "prefetch must be <= 16");
+    if (o.arith != POTTS_ARITH_EXACT && o.arith != POTTS_ARITH_FAST) return fail(POTTS_EINVAL, "unknown arith");
+    if (o.stall_plane < 0) return fail(POTTS_EINVAL, "stall_plane must be >= 0");
     return POTTS_OK;
 }
 
@@ -1119,6 +1128,8 @@ void potts_default_options(potts_options *o)
     o->tile_vpt = 0;
     o->prefetch = 0;
     o->autotune = 0;
+    o->arith = POTTS_ARITH_EXACT;
+    o->stall_plane = 0;
 }
 
 const char *potts_status_string(int s)

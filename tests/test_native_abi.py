@@ -28,10 +28,11 @@ def test_library_exports_every_declared_symbol(native_lib):
 
 
 def test_library_is_built_for_sm100a_only():
-    from segmentctscans_b200.build import NVCC_FLAGS
+    from segmentctscans_b200.build import COMPILE_FLAGS, LINK_FLAGS
 
-    assert "arch=compute_100a,code=sm_100a" in NVCC_FLAGS
-    assert "-fmad=false" in NVCC_FLAGS
+    assert "arch=compute_100a,code=sm_100a" in COMPILE_FLAGS
+    assert "arch=compute_100a,code=sm_100a" in LINK_FLAGS
+    assert "-fmad=false" in COMPILE_FLAGS
 
 
 def test_status_strings(native_lib):
