@@ -29,7 +29,8 @@ is the differentiable solve: 192^3, r = 90, K = 3, 200 unrolled iterations,
 checkpoints every 20, cross-entropy of V against the true labels; value =
 voxel-iterations of forward + backward per second; the gradients of c, lambda
 and --fd-coords random u coordinates are checked against FP64 central
-differences of the oracle (step 1e-6 relative; also 1e-4 for u).
+differences of the FP64 GPU solve (the same bits as the FP64 oracle; step 1e-6
+relative, also 1e-4 for u).
 
 --workload tv is TV-L2 denoising (chambolle(), 768^2 x 1024, 150 iterations).
 --workload fieldio is the field I/O around the solve on the same core: the
@@ -91,7 +92,7 @@ def parse_args():
                    default="config1",
                    help="config1: 768x768x1024 r=370 (the benchmark); config0: 128^3 r=60; "
                         "mid: 384x384x256 r=180 (profiling size, state > L2)")
-    p.add_argument("--fd-coords", type=int, default=4,
+    p.add_argument("--fd-coords", type=int, default=64,
                    help="config4: random u coordinates checked against FP64 central differences")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -746,19 +747,19 @@ def run_adjoint(args, dist_: Dist) -> None:
 
     check = None
     if dist_.rank == 0 and args.fd_coords >= 0:
-        from oracle import oracle
-
-        oracle.set_threads(os.cpu_count() or 1)
+        # FP64 losses through the FP64 GPU solve (the same bits as the FP64 CPU oracle)
         u_h = u.cpu().numpy().copy()
-        t_h = truth.cpu().numpy()
-        mv = m.mask_values
+        idx_t = torch.from_numpy(np.arange(m.span).reshape(m.n_lines, m.nstride)[:, : m.n_images].reshape(-1)).to(dev)
+        t_in = truth.long()[idx_t].clamp(max=len(ci) - 1)
+        V64 = torch.empty((len(ci) - 1, m.span), dtype=torch.float64, device=dev)
 
         def loss64(uu, cc, ll):
-            r = oracle.solve(m, uu, cc, ll, tau, tau, iters, precision="f64")
-            Vm = mv(r.V)
-            Vf = np.concatenate([Vm, 1.0 - Vm.sum(0, keepdims=True)])
-            tt = np.minimum(mv(t_h).astype(np.int64), len(ci) - 1)
-            return float(-np.mean(np.log(np.take_along_axis(Vf, tt[None], 0)[0] + eps)))
+            du = torch.from_numpy(np.ascontiguousarray(uu, np.float32)).to(dev)
+            potts.solve_device_f64(ctx, m, du.data_ptr(), cc, ll, tau, tau, iters, V_ptr=V64.data_ptr(), stats=False)
+            torch.cuda.synchronize(dev)
+            Vm = V64[:, idx_t]
+            Vf = torch.cat([Vm, 1.0 - Vm.sum(0, keepdim=True)])
+            return float(-torch.log(Vf.gather(0, t_in[None])[0] + eps).mean().item())
 
         def cd(fun, x, rel):
             h = rel * max(abs(x), 1e-2)

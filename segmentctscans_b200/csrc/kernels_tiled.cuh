@@ -84,15 +84,22 @@ struct TileShape {
     static constexpr int NV = NT + 4;                   // u and Vbar (FP32): slices n0 .. n0+NT+3
     static constexpr int MAIN = R * Q;
     static constexpr int MAIN_WARPS = MAIN / 32;
-    static constexpr int HALO_WARPS = (Q + 31) / 32;  // the high halo row (and the slice n0+NT)
+    // the high halo row, then (its own warp when POTTS_NHALO_WARP) the slice n0+NT
+#ifdef POTTS_NHALO_WARP
+    static constexpr int NHALO_OWN = 1;
+#else
+    static constexpr int NHALO_OWN = 0;
+#endif
+    static constexpr int HALO_WARPS = (Q + 31) / 32 + NHALO_OWN;
     static constexpr int PRODUCER_WARP = MAIN_WARPS + HALO_WARPS;
     // Dykstra warps run the projection loop of queued voxels; row warp r
     // queues for Dykstra warp r % NW (about 5 % of the voxels need the loop,
-    // 2.5 sweeps on average: a few warps running full batches keep up)
+    // 2.5 sweeps on average; a lane runs one voxel at a time, so the loop's
+    // latency is hidden by many lanes: 6 warps measured faster than 2, 3 or 8)
 #ifdef POTTS_DYKSTRA_WARPS
     static constexpr int NW = MAIN_WARPS >= 2 * POTTS_DYKSTRA_WARPS ? POTTS_DYKSTRA_WARPS : (MAIN_WARPS >= 2 ? MAIN_WARPS / 2 : 1);
 #else
-    static constexpr int NW = MAIN_WARPS >= 12 ? 3 : (MAIN_WARPS >= 4 ? 2 : 1);
+    static constexpr int NW = MAIN_WARPS >= 12 ? 6 : (MAIN_WARPS >= 2 ? MAIN_WARPS / 2 : 1);
 #endif
     static constexpr int DYKSTRA_WARP = PRODUCER_WARP + 1;  // the first one
     static constexpr int THREADS = MAIN + 32 * HALO_WARPS + 32 + 32 * NW;
@@ -450,12 +457,10 @@ __device__ __forceinline__ void stage_a_nhalo(const TiledSmem<K, R, NT, VPT, ST>
 }
 
 // The Dykstra warp: runs the projection loop of the voxels that the row warps
-// queue.  It sleeps until a batch of kBatch voxels has gathered in its queue
-// (or the row warps are done), then each lane takes one voxel, runs it a
-// sweep at a time and, once it is done, stores the result and takes the next
-// waiting ticket, until the queue is empty and every lane has finished.  Work
-// therefore runs in full batches instead of a sweep per arriving voxel, so
-// few warp instructions are issued with one or two lanes active.  It returns
+// queue.  It sleeps until kBatch voxels have gathered in its queue (or the
+// row warps are done), then each lane takes one voxel, runs it a sweep at a
+// time and, once it is done, stores the result and takes the next waiting
+// ticket, until the queue is empty and every lane has finished.  It returns
 // when every row warp has finished and the queue is empty, or when the block
 // aborts.  Every wait is bounded.
 constexpr int kQueueSpin = 1 << 20;   // polls of an entry's publication flag
@@ -463,7 +468,7 @@ constexpr int kIdleRounds = 1 << 23;  // idle polls (~400 ns each) while the row
 #ifdef POTTS_DYKSTRA_BATCH
 constexpr uint32_t kBatch = POTTS_DYKSTRA_BATCH;
 #else
-constexpr uint32_t kBatch = 32;  // queued voxels that start a batch
+constexpr uint32_t kBatch = 1;  // queued voxels that start a batch (larger batches measured no faster)
 #endif
 
 template <int K, int R, int NT, int VPT, typename ST, bool FAST>
@@ -676,79 +681,103 @@ __device__ __forceinline__ void stage_b_chunk(const TiledSmem<K, R, NT, VPT, ST>
         }
     }
 
-    // voxels that need the loop go to the block's queue (the Dykstra warp runs
-    // them); when it is full, the lane runs the loop itself
+    // Every voxel's q is stored at once, whole vectors in every lane (no lane
+    // takes a separate path for its loop voxels).  The voxels that need the
+    // projection loop are stored again, with the loop's result, by the Dykstra
+    // warp that runs them (their queue entries are published behind a block
+    // fence, after this store) or by the lane itself when the queue is full.
+    if (live) {
+        if (nb + VPT <= tp.ns) {
 #pragma unroll
-    for (int j = 0; j < VPT; ++j) {
-        const bool mine = (need >> j) & 1u;
-        const unsigned bal = __ballot_sync(0xffffffffu, mine);
-        if (bal == 0u) continue;
-        const uint32_t n = (uint32_t)__popc(bal);
-        uint32_t base = 0;
-        bool queued = false;
-        const int w = (threadIdx.x >> 5) % S::NW;
-        if (lane == 0) {
-            uint32_t *tail = sm.q_tail(w);
-            uint32_t t = *reinterpret_cast<volatile uint32_t *>(tail);
-            for (int tries = 0; tries < 64; ++tries) {
-                if (t + n - *sm.q_head(w) > (uint32_t)S::QN) break;  // no room
-                const uint32_t prev = atomicCAS(tail, t, t + n);
-                if (prev == t) {
-                    queued = true;
-                    base = t;
-                    break;
+            for (int i = 0; i < K - 1; ++i)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    float w[VPT];
+#pragma unroll
+                    for (int j = 0; j < VPT; ++j) w[j] = qv[j][i][a];
+                    stv<VPT>(Xout + (3 * i + a) * tp.plane_w + o, w);
                 }
-                t = prev;
-            }
-        }
-        queued = __shfl_sync(0xffffffffu, queued, 0);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (mine) {
-            if (queued) {
-                const uint32_t ticket = base + (uint32_t)__popc(bal & ((1u << lane) - 1u));
-                float *e = sm.queue_entry(w, ticket);
+        } else {
 #pragma unroll
-                for (int i = 0; i < K; ++i) {
-                    e[3 * i] = qv[j][i][0];
-                    e[3 * i + 1] = qv[j][i][1];
-                    e[3 * i + 2] = qv[j][i][2];
-                }
-                e[3 * K] = __int_as_float((int)(o + j));
-                __threadfence_block();
-                *sm.queue_seq(w, ticket) = ticket + 1u;
-            } else {
-                if constexpr (FAST)
-                    fast::dual_project<K>(qv[j]);
-                else
-                    dual_project<K>(qv[j], thr);
+            for (int j = 0; j < VPT; ++j)
+                if (nb + j < tp.ns)
 #pragma unroll
-                for (int i = 0; i < K - 1; ++i)
+                    for (int i = 0; i < K - 1; ++i)
 #pragma unroll
-                    for (int a = 0; a < 3; ++a)
-                        Xout[(3 * i + a) * tp.plane_w + o + j] = Store<ST>::st(qv[j][i][a]);
-            }
+                        for (int a = 0; a < 3; ++a)
+                            Xout[(3 * i + a) * tp.plane_w + o + j] = Store<ST>::st(qv[j][i][a]);
         }
     }
-    if (!live) return;
 
-    if (need == 0u && nb + VPT <= tp.ns) {
+    // the loop voxels of the whole warp go to the block's queue in one
+    // reservation (the Dykstra warp runs them); when it is full, each lane
+    // runs the loop of its own voxels
+    unsigned bal[VPT];
+    uint32_t total = 0;
 #pragma unroll
-        for (int i = 0; i < K - 1; ++i)
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                float w[VPT];
-#pragma unroll
-                for (int j = 0; j < VPT; ++j) w[j] = qv[j][i][a];
-                stv<VPT>(Xout + (3 * i + a) * tp.plane_w + o, w);
+    for (int j = 0; j < VPT; ++j) {
+        bal[j] = __ballot_sync(0xffffffffu, (need >> j) & 1u);
+        total += (uint32_t)__popc(bal[j]);
+    }
+    if (total == 0u) return;
+    uint32_t base = 0;
+    bool queued = false;
+    const int w = (threadIdx.x >> 5) % S::NW;
+    if (lane == 0) {
+        uint32_t *tail = sm.q_tail(w);
+        uint32_t t = *reinterpret_cast<volatile uint32_t *>(tail);
+        for (int tries = 0; tries < 64; ++tries) {
+            if (t + total - *sm.q_head(w) > (uint32_t)S::QN) break;  // no room
+            const uint32_t prev = atomicCAS(tail, t, t + total);
+            if (prev == t) {
+                queued = true;
+                base = t;
+                break;
             }
-    } else {
+            t = prev;
+        }
+    }
+    queued = __shfl_sync(0xffffffffu, queued, 0);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (need == 0u) return;
+    const unsigned lower = (1u << lane) - 1u;
+    if (queued) {
+        uint32_t first = base, tickets[VPT];
+#pragma unroll
+        for (int j = 0; j < VPT; ++j) {
+            tickets[j] = first + (uint32_t)__popc(bal[j] & lower);
+            first += (uint32_t)__popc(bal[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < VPT; ++j) {
+            if (!((need >> j) & 1u)) continue;
+            float *e = sm.queue_entry(w, tickets[j]);
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                e[3 * i] = qv[j][i][0];
+                e[3 * i + 1] = qv[j][i][1];
+                e[3 * i + 2] = qv[j][i][2];
+            }
+            e[3 * K] = __int_as_float((int)(o + j));
+        }
+        __threadfence_block();
 #pragma unroll
         for (int j = 0; j < VPT; ++j)
-            if (nb + j < tp.ns && !((need >> j) & 1u))
+            if ((need >> j) & 1u) *sm.queue_seq(w, tickets[j]) = tickets[j] + 1u;
+    } else {
 #pragma unroll
-                for (int i = 0; i < K - 1; ++i)
+        for (int j = 0; j < VPT; ++j) {
+            if (!((need >> j) & 1u)) continue;
+            if constexpr (FAST)
+                fast::dual_project<K>(qv[j]);
+            else
+                dual_project<K>(qv[j], thr);
 #pragma unroll
-                    for (int a = 0; a < 3; ++a) Xout[(3 * i + a) * tp.plane_w + o + j] = Store<ST>::st(qv[j][i][a]);
+            for (int i = 0; i < K - 1; ++i)
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                    Xout[(3 * i + a) * tp.plane_w + o + j] = Store<ST>::st(qv[j][i][a]);
+        }
     }
 }
 
@@ -890,7 +919,9 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
             const int rr = is_main ? tid / S::Q : R;
             const int q = is_main ? tid % S::Q : hq;
             const bool chunk_a = is_main || hq < S::Q;
-            const bool nhalo = !is_main && hq <= R;  // lanes of the first halo warp
+            // lanes of the first halo warp, or of the last one when it has its own
+            const int hn = S::NHALO_OWN ? hq - 32 * (S::HALO_WARPS - 1) : hq;
+            const bool nhalo = !is_main && hn >= 0 && hn <= R;
             bool ok = true;
             // ring slots of positions p-1, p, p+1 and the barrier parities of p-1, p
             int s_prev = S::D - 1, s_cur = 0, s_next = 1;
@@ -903,7 +934,7 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
                     if (chunk_a)
                         stage_a_chunk<K, R, NT, VPT, ST, FAST>(sm, tp, pp, p, s_cur, s_prev, r0, rr, n0, q,
                                                          is_main && ca - 1 + p < cb, Vout, dqmax);
-                    if (nhalo) stage_a_nhalo<K, R, NT, VPT, ST, FAST>(sm, tp, pp, p, s_cur, s_prev, r0, hq, n0);
+                    if (nhalo) stage_a_nhalo<K, R, NT, VPT, ST, FAST>(sm, tp, pp, p, s_cur, s_prev, r0, hn, n0);
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(sm.ready(s_cur));
