@@ -101,6 +101,9 @@ def parse_args():
     p.add_argument("--tile-slices", type=int, default=0, help="fused tile slices (0 = library default)")
     p.add_argument("--segment", type=int, default=0, help="columns per fused work item (0 = library default)")
     p.add_argument("--tile-vpt", type=int, default=0, help="fused slices per thread (0 = library default)")
+    p.add_argument("--persistent", type=int, choices=[0, 1], default=0,
+                   help="fused: 1 = the iterations between energy evaluations in one persistent launch, "
+                        "0 = one launch per iteration")
     p.add_argument("--prefetch", type=int, default=0,
                    help="fused: planes of L2 prefetch ahead of the load ring (0 = library default, -1 = none)")
     args = p.parse_args()
@@ -350,7 +353,8 @@ def run_ours(args, dist_: Dist) -> None:
     lab = torch.empty(span, dtype=torch.uint8, device=dev)
 
     tile_opts = {"tile_rows": args.tile_rows, "tile_slices": args.tile_slices, "segment_cols": args.segment,
-                 "tile_vpt": args.tile_vpt, "prefetch": args.prefetch, "arith": args.arith}
+                 "tile_vpt": args.tile_vpt, "prefetch": args.prefetch, "arith": args.arith,
+                 "persistent": args.persistent}
 
     def step():
         return potts.solve_device(ctx, m, u.data_ptr(), ci, LAMBDA, tau, tau, args.iters, res_ptr=res.data_ptr(),
@@ -381,18 +385,22 @@ def run_ours(args, dist_: Dist) -> None:
     # roofline of the fused iteration kernel: algorithmic bytes / average launch time
     loop_ms = sum(s.loop_ms for s in stats)
     loop_launches = sum(s.loop_launches for s in stats)
+    loop_iters = sum(s.loop_iters for s in stats)
     launch_s = loop_ms / 1000.0 / max(loop_launches, 1)
+    iter_s = loop_ms / 1000.0 / max(loop_iters, 1)
     bpv = bytes_per_voxel_iter(args.variant, k, args.storage)
-    # the split form runs two launches per iteration
-    per_launch_bytes = bpv * vox if args.variant == "fused" else bpv * vox / 2
-    achieved = per_launch_bytes / launch_s / 1e9
+    # bytes of one iteration over its device time (a persistent launch runs many iterations; the
+    # split form runs two launches per iteration)
+    achieved = bpv * vox / iter_s / 1e9
     peaks = measured_peaks()
     tr = profiled_traffic(args.variant if args.storage == "f32" and k == 3 else None)
     traffic = tr["dram_bytes_per_voxel_iter"] * vox if tr else None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
-                "kernel": "potts::fused_tiled_kernel" if args.variant == "fused" else "potts::dual_kernel+primal_kernel",
+                "kernel": ("potts::fused_persistent_kernel" if loop_iters > loop_launches else "potts::fused_tiled_kernel")
+                if args.variant == "fused" else "potts::dual_kernel+primal_kernel",
                 "bytes_per_voxel_iter": bpv, "avg_launch_ms": round(launch_s * 1000, 4),
+                "avg_iter_ms": round(iter_s * 1000, 4), "iters_per_launch": round(loop_iters / max(loop_launches, 1), 2),
                 "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)"}
 
     # quality figures of the last solve
@@ -453,7 +461,7 @@ def run_ours(args, dist_: Dist) -> None:
                        "gap_every": args.gap_every, "variant": args.variant, "storage": args.storage,
                        "arith": args.arith,
                        "tile": [args.tile_rows, args.tile_slices, args.tile_vpt, args.segment],
-                       "prefetch": args.prefetch,
+                       "prefetch": args.prefetch, "persistent": args.persistent,
                        "parallelism": f"replica x{dist_.world}" if dist_.world > 1 else "single",
                        "l2": "inputs larger than L2 (state ~30 GB per GPU)"},
             "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clk, "cpu_baseline": cpu,
@@ -504,7 +512,7 @@ def storage_compare(args, dist_: Dist, ctx, m, u, ci, tau, stream, dev, fused_va
     def solve(storage, variant, arith, iters):
         return potts.solve_device(ctx, m, u.data_ptr(), ci, LAMBDA, tau, tau, iters, labels_ptr=lab.data_ptr(),
                                   V_ptr=v.data_ptr(), stats=True, variant=variant, gap_every=args.gap_every,
-                                  storage=storage, arith=arith)
+                                  storage=storage, arith=arith, persistent=args.persistent)
 
     def timed(storage, variant, arith):
         solve(storage, variant, arith, 2)  # allocations, module load
@@ -517,13 +525,12 @@ def storage_compare(args, dist_: Dist, ctx, m, u, ci, tau, stream, dev, fused_va
         torch.cuda.synchronize(dev)
         t = dist_.reduce(e0.elapsed_time(e1) / 1000.0, "max")
         value = dist_.reduce(float(vox) * args.iters, "sum") / t / 1e9
-        launch_s = st.loop_ms / 1000.0 / max(st.loop_launches, 1)
+        iter_s = st.loop_ms / 1000.0 / max(st.loop_iters, 1)
         bpv = bytes_per_voxel_iter("fused" if variant == 0 else "plain", k, storage)
-        per_launch = bpv * vox if variant == 0 else bpv * vox / 2
         diff = in_mask(lab) != lr
         flips = int(dist_.reduce(float((diff & ~ties).sum().item()), "sum"))
         dv = float(torch.linalg.vector_norm(in_mask(v, k - 1).double() - vr).item())
-        return {"value": round(value, 3), "achieved_gbs": round(per_launch / launch_s / 1e9, 1),
+        return {"value": round(value, 3), "achieved_gbs": round(bpv * vox / iter_s / 1e9, 1),
                 "bytes_per_voxel_iter": bpv, "arith": arith, "label_flips_vs_f64": flips,
                 "flip_rate_vs_f64": flips / n_vox, "v_rel_l2_vs_f64": dv / max(vr_norm, 1e-300),
                 "gap_last": st.energy_trace[-1].tolist() if st.energy_trace is not None else None}
@@ -605,7 +612,8 @@ def run_batch(args, dist_: Dist) -> None:
         keep.append((ph, res, lab))
         vols.append(potts.BatchVolume(m, ph.u.data_ptr(), ph.ci, specs[i].lam, res.data_ptr(), lab.data_ptr()))
     tile_opts = {"tile_rows": args.tile_rows, "tile_slices": args.tile_slices, "segment_cols": args.segment,
-                 "tile_vpt": args.tile_vpt, "prefetch": args.prefetch, "arith": args.arith}
+                 "tile_vpt": args.tile_vpt, "prefetch": args.prefetch, "arith": args.arith,
+                 "persistent": args.persistent}
     autotune = int(not any(v > 0 for k, v in tile_opts.items() if k != "arith"))
     batch = potts.Batch(ctx, vols, tau, tau, iters, storage=args.storage, autotune=autotune, **tile_opts)
     info = batch.info()
@@ -629,13 +637,16 @@ def run_batch(args, dist_: Dist) -> None:
     value = vox_all * iters * args.steps / t_max / 1e9
 
     launch_s = sum(s.loop_ms for s in stats) / 1000.0 / max(sum(s.loop_launches for s in stats), 1)
+    iter_s = sum(s.loop_ms for s in stats) / 1000.0 / max(sum(s.loop_iters for s in stats), 1)
     bpv = bytes_per_voxel_iter("fused", 3, args.storage)
-    achieved = bpv * vox_local / launch_s / 1e9
+    achieved = bpv * vox_local / iter_s / 1e9
     peaks = measured_peaks()
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None,
-                "kernel": "potts::fused_tiled_kernel (all volumes per launch)", "bytes_per_voxel_iter": bpv,
-                "avg_launch_ms": round(launch_s * 1000, 4),
+                "kernel": "potts::fused_persistent_kernel (every iteration of all volumes in one launch)"
+                if all(s.loop_launches == 1 for s in stats)
+                else "potts::fused_tiled_kernel (all volumes per launch)", "bytes_per_voxel_iter": bpv,
+                "avg_launch_ms": round(launch_s * 1000, 4), "avg_iter_ms": round(iter_s * 1000, 4),
                 "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)"}
 
     e2e = None
@@ -860,11 +871,11 @@ def run_tv(args, dist_: Dist) -> None:
     vox = m.data_size
     value = dist_.reduce(float(vox) * iters * args.steps, "sum") / t_max / 1e9
     launch_s = sum(s.loop_ms for s in stats) / 1000.0 / max(sum(s.loop_launches for s in stats), 1)
+    iter_s = sum(s.loop_ms for s in stats) / 1000.0 / max(sum(s.loop_iters for s in stats), 1)
     # tiled: xi (3) and the differences of g (3) in, xi (3) out; per-voxel fused: xi (3) and g in,
-    # xi (3) out; split: div reads xi (3), writes v; grad reads v, g, xi (3), writes xi (3) -- per
-    # launch the average of the two
+    # xi (3) out; split: div reads xi (3), writes v; grad reads v, g, xi (3), writes xi (3)
     bpv = {0: 36, 1: 48, 2: 28}[variant]
-    achieved = (bpv / 2 if variant == 1 else bpv) * vox / launch_s / 1e9
+    achieved = bpv * vox / iter_s / 1e9
     peaks = measured_peaks()
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None,

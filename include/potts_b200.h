@@ -116,6 +116,11 @@ typedef struct potts_options {
                          the loads of that plane of its column march, so every wait for it gives up
                          after its limit (about 2 s) and the solve returns POTTS_ETIMEOUT with the
                          context still usable; 0 = off (default) */
+    int persistent;   /* fused form: 1 = the iterations between two energy evaluations (all of them
+                         without gap_every) run as one persistent cooperative launch that keeps every
+                         block resident and passes a grid-wide barrier between iterations; batches
+                         then capture a single iteration launch; 0 = one launch per iteration
+                         (default 0; sync_monitor implies 0) */
 } potts_options;
 
 typedef struct potts_stats {
@@ -130,6 +135,8 @@ typedef struct potts_stats {
     uint64_t state_bytes; /* out: device bytes held by the solver state */
     float *dq_trace;      /* in, optional: [iters] max |dV|^2 per iteration of the last slab (host) */
     double *energy_trace; /* in, optional: [3 * (iters / gap_every)] (lagrangian, dual, gap) (host) */
+    int loop_iters;       /* out: iterations run inside loop_ms (the fused form's persistent launches run
+                             many iterations each) */
 } potts_stats;
 
 /* Defaults: fused, FP32, no gap, planner-chosen slabs, track_dq = 1, no per-iteration sync. */

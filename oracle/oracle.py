@@ -185,6 +185,44 @@ def div_step(m, K: int, xi, V, u, ci, lam, tau1, precision: str = "f64"):
     return V, Vb, float(dq)
 
 
+def div_step_cols(m, K: int, xi, V, u, ci, lam, tau1, col_lo: int, col_hi: int, precision: str = "f64"):
+    """One primal step over every column; the returned max |dV|^2 covers the columns [col_lo, col_hi)
+    only (the owned columns of a shard)."""
+    dt, ct = _real(precision)
+    xi = np.ascontiguousarray(xi, dtype=dt)
+    V = np.ascontiguousarray(V, dtype=dt).copy()
+    Vb = np.zeros_like(V)
+    u = np.ascontiguousarray(u, dtype=np.float32)
+    c = np.ascontiguousarray(np.asarray(ci, np.float32))
+    f = getattr(lib(), f"oracle_div_step_cols_{precision}")
+    f.restype = ct
+    f.argtypes = [ctypes.POINTER(OCyl), ctypes.c_int, ctypes.POINTER(ct), ctypes.POINTER(ct), ctypes.POINTER(ct),
+                  ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), ctypes.c_float, ctypes.c_float,
+                  ctypes.c_int64, ctypes.c_int64]
+    oc = ocyl(m)
+    dq = f(ctypes.byref(oc), K, _ptr(xi, ct), _ptr(V, ct), _ptr(Vb, ct), _ptr(u, ctypes.c_float),
+           _ptr(c, ctypes.c_float), float(lam), float(tau1), int(col_lo), int(col_hi))
+    return V, Vb, float(dq)
+
+
+def energies_cols(m, K: int, xi, V, u, ci, lam, col_lo: int, col_hi: int, precision: str = "f64") -> np.ndarray:
+    """(lagrangian, dual, gap) in FP64 over the voxels of the columns [col_lo, col_hi)."""
+    dt, ct = _real(precision)
+    xi = np.ascontiguousarray(xi, dtype=dt)
+    V = np.ascontiguousarray(V, dtype=dt)
+    u = np.ascontiguousarray(u, dtype=np.float32)
+    c = np.ascontiguousarray(np.asarray(ci, np.float32))
+    out = np.zeros(3, np.float64)
+    f = getattr(lib(), f"oracle_energies_cols_{precision}")
+    f.argtypes = [ctypes.POINTER(OCyl), ctypes.c_int, ctypes.POINTER(ct), ctypes.POINTER(ct),
+                  ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), ctypes.c_float, ctypes.c_int64,
+                  ctypes.c_int64, ctypes.POINTER(ctypes.c_double)]
+    oc = ocyl(m)
+    f(ctypes.byref(oc), K, _ptr(xi, ct), _ptr(V, ct), _ptr(u, ctypes.c_float), _ptr(c, ctypes.c_float), float(lam),
+      int(col_lo), int(col_hi), _ptr(out, ctypes.c_double))
+    return out
+
+
 def energies(m, K: int, xi, V, u, ci, lam, precision: str = "f64") -> np.ndarray:
     """(lagrangian, dual, gap) in FP64."""
     dt, ct = _real(precision)

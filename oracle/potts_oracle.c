@@ -319,7 +319,10 @@ static void grad_step(ostate *st, REAL tau2, int n_lo, int n_hi, int *sweep_hist
 }
 
 /* div_kernel, potts-min-partition.cpp:349-488.  Returns max_x |V^{k+1}-V^k|^2. */
-static REAL div_step(ostate *st, const float *u, const REAL *c, REAL lam, REAL tau1, int n_lo, int n_hi)
+/* dq_lo/dq_hi: the columns whose voxels enter the returned max |dV|^2 (all
+ * columns are updated). */
+static REAL div_step(ostate *st, const float *u, const REAL *c, REAL lam, REAL tau1, int n_lo, int n_hi,
+                     int64_t dq_lo, int64_t dq_hi)
 {
     const ocyl *m = st->m;
     const int K = st->K;
@@ -386,7 +389,7 @@ static REAL div_step(ostate *st, const float *u, const REAL *c, REAL lam, REAL t
                     st->Vb[i * S + o] = store_round(st->store, (REAL)2 * q[i] - v[i]);
                     st->V[i * S + o] = store_round_v(st, q[i], line, (uint32_t)n, i);
                 }
-                if (dq > dq_max) dq_max = dq;
+                if (dq > dq_max && col >= dq_lo && col < dq_hi) dq_max = dq;
             }
         }
     }
@@ -424,18 +427,20 @@ static void update(const ostate *st, const float *c, int n_lo, int n_hi, float *
  *   dual       = sum_x min_i (G_i - div Xi_i)
  *   gap        = lagrangian - dual  (>= 0 for V on the simplex)
  * with G_i = lam (u - c_i)^2.  The reference computes no energy; this is the
- * diagnostic reported every few iterations.  Sums are per column, then added
- * in column order.
+ * diagnostic reported every few iterations.  Sums are per column over the
+ * columns [col_lo, col_hi) (neighbours outside that range still count in the
+ * divergence), then added in column order.
  * ------------------------------------------------------------------------- */
-static void energies(const ostate *st, const float *u, const REAL *c, REAL lam, int n_lo, int n_hi, double out[3])
+static void energies(const ostate *st, const float *u, const REAL *c, REAL lam, int n_lo, int n_hi, int64_t col_lo,
+                     int64_t col_hi, double out[3])
 {
     const ocyl *m = st->m;
     const int K = st->K;
     const int64_t S = st->span;
-    const int64_t ncol = (int64_t)m->col_end - m->col_begin;
+    const int64_t ncol = col_hi - col_lo;
     double *part = (double *)calloc((size_t)(2 * (ncol > 0 ? ncol : 1)), sizeof(double));
 #pragma omp parallel for schedule(dynamic, 4)
-    for (int64_t col = m->col_begin; col < m->col_end; ++col) {
+    for (int64_t col = col_lo; col < col_hi; ++col) {
         double sl = 0, sd = 0;
         for (int64_t row = row_begin(m, col); row < row_end(m, col); ++row) {
             const int has_r = row_end(m, col) - 1 > row;
@@ -480,8 +485,8 @@ static void energies(const ostate *st, const float *u, const REAL *c, REAL lam, 
                 sd += mn;
             }
         }
-        part[2 * (col - m->col_begin)] = sl;
-        part[2 * (col - m->col_begin) + 1] = sd;
+        part[2 * (col - col_lo)] = sl;
+        part[2 * (col - col_lo) + 1] = sd;
     }
     double L = 0, D = 0;
     for (int64_t i = 0; i < ncol; ++i) { L += part[2 * i]; D += part[2 * i + 1]; }
@@ -548,10 +553,11 @@ int NAME(oracle_solve_store)(const ocyl *m, const float *u, int K, const float *
         for (int it = 0; it < iters; ++it) {
             grad_step(&st, tau2, s0, s1, sweep_hist);
             st.it = it;
-            REAL dq = div_step(&st, u, c, lam, tau1, s0, s1);
+            REAL dq = div_step(&st, u, c, lam, tau1, s0, s1, m->col_begin, m->col_end);
             if (dq_trace) dq_trace[it] = (float)dq;
             if (energy_trace && gap_every > 0 && (it + 1) % gap_every == 0)
-                energies(&st, u, c, lam, s0, s1, energy_trace + 3 * ((it + 1) / gap_every - 1));
+                energies(&st, u, c, lam, s0, s1, m->col_begin, m->col_end,
+                         energy_trace + 3 * ((it + 1) / gap_every - 1));
         }
         const int r0 = (s0 == 0) ? s0 : s0 + halo;
         const int r1 = (s1 == n) ? s1 : s1 - halo;
@@ -589,7 +595,7 @@ REAL NAME(oracle_div_step)(const ocyl *m, int K, const REAL *xi, REAL *V, REAL *
     REAL c[KMAX];
     for (int i = 0; i < K; ++i) c[i] = (REAL)c_f[i];
     ostate st = {m, K, (int64_t)m->base[m->cols], (REAL *)xi, V, Vb, 0, 0};
-    return div_step(&st, u, c, (REAL)lam, (REAL)tau1, 0, (int)m->n_images);
+    return div_step(&st, u, c, (REAL)lam, (REAL)tau1, 0, (int)m->n_images, m->col_begin, m->col_end);
 }
 
 void NAME(oracle_energies)(const ocyl *m, int K, const REAL *xi, const REAL *V, const float *u, const float *c_f,
@@ -598,7 +604,28 @@ void NAME(oracle_energies)(const ocyl *m, int K, const REAL *xi, const REAL *V, 
     REAL c[KMAX];
     for (int i = 0; i < K; ++i) c[i] = (REAL)c_f[i];
     ostate st = {m, K, (int64_t)m->base[m->cols], (REAL *)xi, (REAL *)V, NULL, 0, 0};
-    energies(&st, u, c, (REAL)lam, 0, (int)m->n_images, out);
+    energies(&st, u, c, (REAL)lam, 0, (int)m->n_images, m->col_begin, m->col_end, out);
+}
+
+/* Column-range forms for sharded solves: the primal step updates every column
+ * and returns max |dV|^2 over [col_lo, col_hi); the energies sum over the
+ * voxels of [col_lo, col_hi). */
+REAL NAME(oracle_div_step_cols)(const ocyl *m, int K, const REAL *xi, REAL *V, REAL *Vb, const float *u,
+                                const float *c_f, float lam, float tau1, int64_t col_lo, int64_t col_hi)
+{
+    REAL c[KMAX];
+    for (int i = 0; i < K; ++i) c[i] = (REAL)c_f[i];
+    ostate st = {m, K, (int64_t)m->base[m->cols], (REAL *)xi, V, Vb, 0, 0};
+    return div_step(&st, u, c, (REAL)lam, (REAL)tau1, 0, (int)m->n_images, col_lo, col_hi);
+}
+
+void NAME(oracle_energies_cols)(const ocyl *m, int K, const REAL *xi, const REAL *V, const float *u,
+                                const float *c_f, float lam, int64_t col_lo, int64_t col_hi, double out[3])
+{
+    REAL c[KMAX];
+    for (int i = 0; i < K; ++i) c[i] = (REAL)c_f[i];
+    ostate st = {m, K, (int64_t)m->base[m->cols], (REAL *)xi, (REAL *)V, NULL, 0, 0};
+    energies(&st, u, c, (REAL)lam, 0, (int)m->n_images, col_lo, col_hi, out);
 }
 
 /* ---------------------------------------------------------------------------

@@ -33,7 +33,7 @@ class PottsOptions(ctypes.Structure):
         ("slab_w", ctypes.c_int), ("track_dq", ctypes.c_int), ("sync_monitor", ctypes.c_int),
         ("tile_rows", ctypes.c_int), ("tile_slices", ctypes.c_int), ("segment_cols", ctypes.c_int),
         ("tile_vpt", ctypes.c_int), ("prefetch", ctypes.c_int), ("autotune", ctypes.c_int),
-        ("arith", ctypes.c_int), ("stall_plane", ctypes.c_int),
+        ("arith", ctypes.c_int), ("stall_plane", ctypes.c_int), ("persistent", ctypes.c_int),
     ]
 
 
@@ -43,6 +43,7 @@ class PottsStats(ctypes.Structure):
         ("dq_last", ctypes.c_float), ("solve_ms", ctypes.c_double), ("loop_ms", ctypes.c_double),
         ("loop_launches", ctypes.c_int), ("total_launches", ctypes.c_int), ("state_bytes", ctypes.c_uint64),
         ("dq_trace", ctypes.POINTER(ctypes.c_float)), ("energy_trace", ctypes.POINTER(ctypes.c_double)),
+        ("loop_iters", ctypes.c_int),
     ]
 
 

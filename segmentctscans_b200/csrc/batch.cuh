@@ -1,10 +1,11 @@
 // Batched solves: many independent volumes (own mapping, u, labels and
 // lambda; common K, step sizes, iteration count and storage) planned once and
 // run as captured CUDA graphs: set-up (u staging, init and first dual step of
-// every volume), iterations (each a single launch of the fused kernel over
-// the work items of all volumes, one volume descriptor each) and finish (last
-// primal step and argmax of every volume), replayed back to back so that the
-// iterations can be timed apart.  Included by potts_b200.cu inside its
+// every volume), iterations (one persistent launch of the fused kernel that
+// runs every iteration over the work items of all volumes, one volume
+// descriptor each; or, with persistent = 0, one launch per iteration) and
+// finish (last primal step and argmax of every volume), replayed back to back
+// so that the iterations can be timed apart.  Included by potts_b200.cu inside its
 // internal namespace.
 #pragma once
 
@@ -31,7 +32,7 @@ struct potts_batch {
     float tau1 = 0.0f, tau2 = 0.0f;
     potts_options opts{};
     std::vector<BatchVolume> vols;
-    DevBuf lines, cols, state, desc, work, work_vol, dq, ustage;
+    DevBuf lines, cols, state, desc, work, work_vol, dq, ustage, pctl;
     TileChoice tile{};
     int n_work = 0;
     cudaGraph_t graph[3] = {nullptr, nullptr, nullptr};  // set-up, iterations, finish
@@ -39,6 +40,7 @@ struct potts_batch {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // run start/end, iterations start/end
     uint64_t voxels = 0, state_bytes = 0;
     int graph_launches = 0;
+    int loop_launches = 0;  // launches of the iterations graph
     double autotune_ms = 0.0;
 };
 
@@ -57,7 +59,8 @@ void batch_free(potts_batch *b)
     }
     for (cudaEvent_t e : b->ev)
         if (e) cudaEventDestroy(e);
-    for (DevBuf *d : {&b->lines, &b->cols, &b->state, &b->desc, &b->work, &b->work_vol, &b->dq, &b->ustage})
+    for (DevBuf *d : {&b->lines, &b->cols, &b->state, &b->desc, &b->work, &b->work_vol, &b->dq, &b->ustage,
+                      &b->pctl})
         if (d->p) cudaFree(d->p);
     delete b;
 }
@@ -307,8 +310,12 @@ int batch_build(potts_batch *b)
         POTTS_TRY((choose_tile<K, ST>(o, &tile)));
     }
     POTTS_TRY((batch_plan_tiles<K, ST>(b, tile)));
-    // the kernel's shared-memory attribute is set outside the capture
+    // the kernel's shared-memory attribute is set (and the persistent launch's
+    // control words allocated) outside the capture
     POTTS_TRY((launch_tiled<K, ST>(ctx, tile, b->opts.arith == POTTS_ARITH_FAST, nullptr, nullptr, nullptr, 0, 0, 0, b->tau2)));
+    if (b->opts.persistent && b->iters > 1)
+        POTTS_TRY((launch_tiled_persistent<K, ST>(ctx, b->pctl, tile, b->opts.arith == POTTS_ARITH_FAST, nullptr,
+                                                  nullptr, nullptr, 0, 0, 0, b->iters - 1, b->tau2)));
     POTTS_CUDA(cudaStreamSynchronize(ctx->stream));
 
     for (cudaEvent_t &e : b->ev) POTTS_CUDA(cudaEventCreate(&e));
@@ -335,12 +342,24 @@ int batch_capture(potts_batch *b, const TileChoice &tile)
         if (part == 0) {
             rc = batch_enqueue_head<K, ST>(b);
         } else if (part == 1) {
-            for (int m = 1; m < b->iters && rc == POTTS_OK; ++m) {
-                rc = launch_tiled<K, ST>(ctx, tile, b->opts.arith == POTTS_ARITH_FAST, static_cast<const potts::FusedVolume<K, ST> *>(b->desc.p),
-                                         static_cast<const int4 *>(b->work.p), static_cast<const int *>(b->work_vol.p),
-                                         b->n_work, cur, m - 1, b->tau2);
+            const bool fast = b->opts.arith == POTTS_ARITH_FAST;
+            const auto *vols = static_cast<const potts::FusedVolume<K, ST> *>(b->desc.p);
+            const auto *work = static_cast<const int4 *>(b->work.p);
+            const auto *work_vol = static_cast<const int *>(b->work_vol.p);
+            if (b->opts.persistent && b->iters > 1) {
+                // every iteration of every volume in one launch
+                rc = launch_tiled_persistent<K, ST>(ctx, b->pctl, tile, fast, vols, work, work_vol, b->n_work, 0, 0,
+                                                    b->iters - 1, b->tau2);
                 ctx->total_launches += 1;
-                cur ^= 1;
+                b->loop_launches = 1;
+                cur = (b->iters - 1) & 1;
+            } else {
+                for (int m = 1; m < b->iters && rc == POTTS_OK; ++m) {
+                    rc = launch_tiled<K, ST>(ctx, tile, fast, vols, work, work_vol, b->n_work, cur, m - 1, b->tau2);
+                    ctx->total_launches += 1;
+                    cur ^= 1;
+                }
+                b->loop_launches = b->iters > 1 ? b->iters - 1 : 0;
             }
         } else {
             rc = batch_enqueue_tail<K, ST>(b, cur);

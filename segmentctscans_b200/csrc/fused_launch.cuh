@@ -35,13 +35,55 @@ cudaError_t launch_fused(cudaStream_t stream, const FusedVolume<K, ST> *vols, co
     return cudaGetLastError();
 }
 
-// Instantiates launch_fused for every tile shape of ShapesOf<K, ST>.
+template <int K, int R, int NT, int VPT, typename ST, bool FAST>
+cudaError_t launch_fused_persistent(cudaStream_t stream, const FusedVolume<K, ST> *vols, const int4 *work,
+                                    const int *work_vol, int n_work, int in0, int it0, int n_iters, float tau2,
+                                    DykstraThresholds thr, int *err, uint32_t *ctl)
+{
+    using S = TileShape<K, R, NT, VPT, ST>;
+    constexpr int kMaxDevices = 64;
+    static bool attr_set[kMaxDevices] = {};
+    static int grid_of[kMaxDevices] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    auto kern = fused_persistent_kernel<K, R, NT, VPT, ST, FAST>;
+    if (!attr_set[dev]) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM_ALLOC);
+        if (e != cudaSuccess) return e;
+        int per_sm = 0, sms = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, S::THREADS, S::SMEM_ALLOC);
+        if (e != cudaSuccess) return e;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
+        grid_of[dev] = per_sm * sms;
+        attr_set[dev] = true;
+    }
+    if (n_work == 0 || n_iters <= 0) return cudaSuccess;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(n_work < grid_of[dev] ? n_work : grid_of[dev]));
+    cfg.blockDim = dim3(S::THREADS);
+    cfg.dynamicSmemBytes = S::SMEM_ALLOC;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, vols, work, work_vol, n_work, in0, it0, n_iters, tau2, thr, err, ctl);
+}
+
+// Instantiates launch_fused and launch_fused_persistent for every tile shape
+// of ShapesOf<K, ST>.
 template <int K, typename ST, bool FAST, size_t... I>
 const void *const *fused_instances(std::index_sequence<I...>)
 {
     using TS = ShapesOf<K, ST>;
     static const void *const table[] = {
-        reinterpret_cast<const void *>(&launch_fused<K, TS::r[I], TS::t[I], TS::v[I], ST, FAST>)...};
+        reinterpret_cast<const void *>(&launch_fused<K, TS::r[I], TS::t[I], TS::v[I], ST, FAST>)...,
+        reinterpret_cast<const void *>(&launch_fused_persistent<K, TS::r[I], TS::t[I], TS::v[I], ST, FAST>)...};
     return table;
 }
 

@@ -794,28 +794,29 @@ struct FusedVolume {
     float *dq;  // per-iteration max |dV|^2 of this volume, or null
 };
 
-// One block per work item: a tile row range x slice range marching over up
-// to 64 columns of one volume (work_vol[item], or volume 0 when work_vol is
-// null); the items of every volume of a batch share one launch, and the
-// block scheduler hands them out as blocks finish.  The launch turns
-// (Xi^m, V^{m-1}) in half `in` into (Xi^{m+1}, V^m) in half in ^ 1; it = m - 1.
+// The work of one block on one work item: a tile row range x slice range
+// marching over up to 64 columns of one volume (work_vol[item], or volume 0
+// when work_vol is null).  It turns (Xi^m, V^{m-1}) in half `in` into
+// (Xi^{m+1}, V^m) in half in ^ 1 for the item's voxels; it = m - 1.
+// `reinit`: the block ran an earlier item, so its mbarriers are invalidated
+// before they are initialised again.  Ends with a block-wide barrier.
 template <int K, int R, int NT, int VPT, typename ST, bool FAST>
-__global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
-    fused_tiled_kernel(const FusedVolume<K, ST> *__restrict__ vols, const int4 *__restrict__ work,
-                       const int *__restrict__ work_vol, int in, int it, float tau2, DykstraThresholds thr, int *err)
+__device__ __forceinline__ void tiled_item(const TiledSmem<K, R, NT, VPT, ST> &sm,
+                                           const FusedVolume<K, ST> *__restrict__ vols, const int4 *__restrict__ work,
+                                           const int *__restrict__ work_vol, int item, bool reinit, int in, int it,
+                                           float tau2, DykstraThresholds thr, int *err)
 {
     using S = TileShape<K, R, NT, VPT, ST>;
-    using T = TiledSmem<K, R, NT, VPT, ST>;
-    extern __shared__ __align__(128) uint8_t smem_raw[];
-    T sm;
-    // align to 128 bytes by pointer arithmetic on the shared array itself, so
-    // that the compiler keeps every access a shared-memory access
-    sm.base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     volatile int *abort = sm.abort_flag();
     {
         if (tid == 0) {
             for (int i = 0; i < S::D; ++i) {
+                if (reinit) {
+                    mbar_inval(sm.full(i));
+                    mbar_inval(sm.ready(i));
+                    mbar_inval(sm.empty(i));
+                }
                 mbar_init(sm.full(i), 1);
                 mbar_init(sm.ready(i), S::MAIN_WARPS + S::HALO_WARPS);
                 mbar_init(sm.empty(i), S::MAIN_WARPS + S::HALO_WARPS);
@@ -828,7 +829,6 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
             }
             mbar_fence_init();
         }
-        const int item = blockIdx.x;
         const FusedVolume<K, ST> *vol = vols + (work_vol ? work_vol[item] : 0);
         TiledParams tp = vol->tp;
         tp.it = it;
@@ -864,6 +864,9 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
                 tma_fence_acquire_desc(tm_xi);
                 tma_fence_acquire_desc(tm_v);
                 tma_fence_acquire_desc(tm_u);
+                // the state was written through the generic proxy (an earlier
+                // iteration of a persistent launch); the loads use the async proxy
+                fence_proxy_async_global();
                 tma_prefetch_desc(tm_xi);
                 tma_prefetch_desc(tm_v);
                 tma_prefetch_desc(tm_u);
@@ -877,7 +880,7 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
                     const int c = ca - 1 + p;
                     if (p == 0 && c < tp.col_begin) {  // no plane before the first column
                         mbar_arrive(sm.full(0));
-                    } else if (p == tp.stall_plane && blockIdx.x == 0) {
+                    } else if (p == tp.stall_plane && item == 0) {
                         // testing: this plane never arrives, so the waits for it run out
                     } else {
                         const int4 ci = sm.cols()[p];
@@ -969,9 +972,124 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
                 }
             }
         }
+        // this item's stores (generic proxy) before any later TMA load of them
+        // (the next iteration of a persistent launch)
+        fence_proxy_async_global();
         __syncthreads();
         if (tid == 0 && *abort) atomicExch(err, 1);
         if (vol->dq) block_max_to(dqmax, vol->dq + it);
+    }
+}
+
+// 128-byte aligned view of the dynamic shared memory of a fused launch.
+template <int K, int R, int NT, int VPT, typename ST>
+__device__ __forceinline__ TiledSmem<K, R, NT, VPT, ST> tiled_smem()
+{
+    extern __shared__ __align__(128) uint8_t smem_raw[];
+    TiledSmem<K, R, NT, VPT, ST> sm;
+    // align by pointer arithmetic on the shared array itself, so that the
+    // compiler keeps every access a shared-memory access
+    sm.base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+    return sm;
+}
+
+// One block per work item; the items of every volume of a batch share one
+// launch, and the block scheduler hands them out as blocks finish.  The launch
+// turns (Xi^m, V^{m-1}) in half `in` into (Xi^{m+1}, V^m) in half in ^ 1;
+// it = m - 1.
+template <int K, int R, int NT, int VPT, typename ST, bool FAST>
+__global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
+    fused_tiled_kernel(const FusedVolume<K, ST> *__restrict__ vols, const int4 *__restrict__ work,
+                       const int *__restrict__ work_vol, int in, int it, float tau2, DykstraThresholds thr, int *err)
+{
+    const auto sm = tiled_smem<K, R, NT, VPT, ST>();
+    tiled_item<K, R, NT, VPT, ST, FAST>(sm, vols, work, work_vol, (int)blockIdx.x, false, in, it, tau2, thr, err);
+}
+
+// Control words of a persistent launch (device memory, zeroed before it):
+// ctl[0] counts the blocks that finished an iteration, ctl[1] is set when a
+// block gave up (every block then leaves), ctl[2 + m] hands out the work items
+// of the launch's iteration m.
+constexpr int kPersistentCtlHead = 2;
+// Polls (each followed by a ~256 ns sleep) of the grid barrier before a block
+// gives up: about 2 s.
+constexpr int kGridWaitTries = 1 << 23;
+
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t *p)
+{
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier of a persistent launch, called by thread 0 of every block
+// after a block-wide barrier: waits (bounded) until `target` block arrivals
+// have been counted.  False when the launch is aborting or the wait ran out
+// (which then aborts the launch).
+__device__ __forceinline__ bool grid_barrier(uint32_t *ctl, uint32_t target)
+{
+    volatile int *gabort = reinterpret_cast<volatile int *>(ctl + 1);
+    __threadfence();
+    atomicAdd(ctl, 1u);
+    for (int i = 0; i < kGridWaitTries; ++i) {
+        if (ld_acquire_gpu(ctl) >= target) return true;
+        if (*gabort) return false;
+        __nanosleep(256);
+    }
+    atomicExch(reinterpret_cast<int *>(ctl + 1), 1);
+    return false;
+}
+
+// The iterations it0 .. it0 + n_iters - 1 of the fused form in one launch:
+// every block of the grid is resident (cooperative launch), takes the work
+// items of an iteration one at a time from a counter, and waits at a grid-wide
+// barrier before the next iteration (whose items read the halos that other
+// blocks wrote).  Iteration m of the launch turns state half (in0 + m) & 1
+// into the other half, like fused_tiled_kernel.  The result does not depend on
+// the grid size or the order in which blocks take items.
+template <int K, int R, int NT, int VPT, typename ST, bool FAST>
+__global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
+    fused_persistent_kernel(const FusedVolume<K, ST> *__restrict__ vols, const int4 *__restrict__ work,
+                            const int *__restrict__ work_vol, int n_work, int in0, int it0, int n_iters, float tau2,
+                            DykstraThresholds thr, int *err, uint32_t *ctl)
+{
+    const auto sm = tiled_smem<K, R, NT, VPT, ST>();
+    // The schedule lives in shared memory and only thread 0 changes it, so no
+    // register carries state across an item (the item body needs them all).
+    // s_m: the block's current iteration; s_item: its next item, or -1 when
+    // the block is done; s_items: items the block has run.
+    __shared__ int s_m, s_item, s_items;
+    if (threadIdx.x == 0) s_m = 0, s_items = 0;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            int m = s_m, item = -1;
+            while (m < n_iters) {
+                if (*reinterpret_cast<volatile int *>(ctl + 1)) break;  // aborting
+                item = (int)atomicAdd(ctl + kPersistentCtlHead + m, 1u);
+                if (item < n_work) break;
+                item = -1;
+                // every item of iteration m is taken: wait for the grid before
+                // the next iteration reads the halos that other blocks write
+                if (m + 1 == n_iters) break;
+                if (!grid_barrier(ctl, (uint32_t)(m + 1) * gridDim.x)) {
+                    atomicExch(err, 1);
+                    break;
+                }
+                ++m;
+            }
+            s_m = m;
+            s_item = item;
+        }
+        __syncthreads();
+        const int item = s_item;
+        if (item < 0) break;
+        const int m = s_m;
+        tiled_item<K, R, NT, VPT, ST, FAST>(sm, vols, work, work_vol, item, s_items > 0, (in0 + m) & 1, it0 + m,
+                                            tau2, thr, err);
+        if (threadIdx.x == 0) {
+            s_items += 1;
+            if (*sm.abort_flag()) atomicExch(reinterpret_cast<int *>(ctl + 1), 1);
+        }
     }
 }
 
@@ -981,6 +1099,16 @@ __global__ void __launch_bounds__(TileShape<K, R, NT, VPT, ST>::THREADS, 1)
 template <int K, int R, int NT, int VPT, typename ST, bool FAST>
 cudaError_t launch_fused(cudaStream_t stream, const FusedVolume<K, ST> *vols, const int4 *work, const int *work_vol,
                          int n_work, int in, int it, float tau2, DykstraThresholds thr, int *err);
+
+// One persistent launch of fused_persistent_kernel<K, R, NT, VPT, ST, FAST>
+// running n_iters iterations (state half in0, iteration it0 first) over
+// n_work items, on `stream`; ctl holds 2 + n_iters zeroed words.  The grid
+// is one block per SM times the blocks an SM holds (at most n_work), launched
+// cooperatively so that every block is resident.
+template <int K, int R, int NT, int VPT, typename ST, bool FAST>
+cudaError_t launch_fused_persistent(cudaStream_t stream, const FusedVolume<K, ST> *vols, const int4 *work,
+                                    const int *work_vol, int n_work, int in0, int it0, int n_iters, float tau2,
+                                    DykstraThresholds thr, int *err, uint32_t *ctl);
 
 // Copies the slab's part of u into a buffer with the state's stride, so that
 // every TMA box of u starts on a 16-byte boundary.

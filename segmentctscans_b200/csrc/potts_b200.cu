@@ -216,6 +216,9 @@ struct potts_context {
     int seg_used = 0;
     bool seg_open = false;
     int loop_launches = 0, total_launches = 0;
+    int loop_iters = 0;  // iterations inside the event pairs
+    // control words of persistent fused launches (item counters per iteration, grid barrier)
+    DevBuf pctl;
 };
 
 struct potts_field {
@@ -558,6 +561,41 @@ int launch_tiled(potts_context *ctx, const TileChoice &tile, bool fast, const po
     }
 }
 
+// One persistent launch of the fused kernel: n_iters iterations (state half
+// in0, iteration it0 first) over n_work items; zeroes the launch's control
+// words in `ctl` (grown as needed) on the stream first.
+template <int K, typename ST, int I = 0>
+int launch_tiled_persistent(potts_context *ctx, DevBuf &ctl, const TileChoice &tile, bool fast,
+                            const potts::FusedVolume<K, ST> *vols, const int4 *work, const int *work_vol, int n_work,
+                            int in0, int it0, int n_iters, float tau2)
+{
+    using TS = ShapesOf<K, ST>;
+    if constexpr (I < TS::n) {
+        constexpr int R = TS::r[I], NT = TS::t[I], VPT = TS::v[I];
+        if (tile.rows == R && tile.slices == NT && tile.vpt == VPT) {
+            const size_t words = (size_t)potts::kPersistentCtlHead + (size_t)std::max(n_iters, 1);
+            POTTS_TRY(ensure(ctx, ctl, sizeof(uint32_t) * words));
+            POTTS_CUDA(cudaMemsetAsync(ctl.p, 0, sizeof(uint32_t) * words, ctx->stream));
+            uint32_t *cw = static_cast<uint32_t *>(ctl.p);
+            const cudaError_t e =
+                fast ? potts::launch_fused_persistent<K, R, NT, VPT, ST, true>(
+                           ctx->stream, vols, work, work_vol, n_work, in0, it0, n_iters, tau2, ctx->thr,
+                           (int *)ctx->err.p, cw)
+                     : potts::launch_fused_persistent<K, R, NT, VPT, ST, false>(
+                           ctx->stream, vols, work, work_vol, n_work, in0, it0, n_iters, tau2, ctx->thr,
+                           (int *)ctx->err.p, cw);
+            if (e != cudaSuccess)
+                return fail(e == cudaErrorMemoryAllocation ? POTTS_ENOMEM : POTTS_ECUDA,
+                            std::string("persistent fused kernel launch: ") + cudaGetErrorString(e));
+            return POTTS_OK;
+        }
+        return launch_tiled_persistent<K, ST, I + 1>(ctx, ctl, tile, fast, vols, work, work_vol, n_work, in0, it0,
+                                                     n_iters, tau2);
+    } else {
+        return fail(POTTS_EINVAL, "no compiled tile shape matches");
+    }
+}
+
 // Descriptor of one volume for the fused kernel: tensor maps of both halves
 // of the state and of u (read from ubase with row stride ustride, slice ux0 =
 // slice 0 of the volume), its column table and phase parameters.
@@ -701,6 +739,7 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
             launch_primal<K, ST>(fast, nb, s, g, xi, V, Vb, d_u, pp, dq ? dq + it : nullptr, it);
             ctx->loop_launches += 2;
             ctx->total_launches += 2;
+            ctx->loop_iters += 1;
             if (ge > 0 && (it + 1) % ge == 0) POTTS_TRY(run_energy<K>(ctx, g, xi, V, d_u, pp, energy + 3 * ((it + 1) / ge - 1)));
             if (o.sync_monitor && dq) POTTS_TRY(monitor_sync<K>(ctx, it));
         }
@@ -727,16 +766,31 @@ int run_slab(potts_context *ctx, const Geometry &g, const float *d_u, const Phas
             launch_dual<K, ST>(fast, nb, s, g, st.xi[0], st.v[0], tau2, ctx->thr);
             ctx->total_launches += 1;
         }
-        for (int m = 1; m < iters; ++m) {
-            const int nxt = cur ^ 1;
+        const bool persistent = o.persistent && !o.sync_monitor;
+        for (int m = 1; m < iters;) {
+            // launches m .. last: one persistent launch up to the next energy
+            // evaluation, or a single iteration
+            int last = m;
+            if (persistent) last = ge > 0 ? std::min(iters - 1, (m + ge - 1) / ge * ge) : iters - 1;
+            const int n_it = last - m + 1;
             POTTS_TRY(seg_begin(ctx));
             ctx->loop_launches += 1;
             ctx->total_launches += 1;
-            POTTS_TRY((launch_tiled<K, ST>)(ctx, fp.tile, fast, (const potts::FusedVolume<K, ST> *)ctx->vols.p,
-                                            (const int4 *)ctx->work.p, nullptr, fp.n_work, cur, m - 1, tau2));
-            if (ge > 0 && m % ge == 0) POTTS_TRY(run_energy<K>(ctx, g, st.xi[cur], st.v[nxt], d_u, pp, energy + 3 * (m / ge - 1)));
+            ctx->loop_iters += n_it;
+            const auto *vols = (const potts::FusedVolume<K, ST> *)ctx->vols.p;
+            if (persistent)
+                POTTS_TRY((launch_tiled_persistent<K, ST>)(ctx, ctx->pctl, fp.tile, fast, vols,
+                                                           (const int4 *)ctx->work.p, nullptr, fp.n_work, cur, m - 1,
+                                                           n_it, tau2));
+            else
+                POTTS_TRY((launch_tiled<K, ST>)(ctx, fp.tile, fast, vols, (const int4 *)ctx->work.p, nullptr,
+                                                fp.n_work, cur, m - 1, tau2));
+            cur ^= n_it & 1;
+            // launch `last` read Xi^last from half cur ^ 1 and wrote V^last to half cur
+            if (ge > 0 && last % ge == 0)
+                POTTS_TRY(run_energy<K>(ctx, g, st.xi[cur ^ 1], st.v[cur], d_u, pp, energy + 3 * (last / ge - 1)));
             if (o.sync_monitor && dq) POTTS_TRY(monitor_sync<K>(ctx, m - 1));
-            cur = nxt;
+            m = last + 1;
         }
         POTTS_TRY(seg_end(ctx));
         if (iters > 0) {
@@ -835,7 +889,7 @@ int solve_k(potts_context *ctx, const float *d_u, const float *ci, float lam, fl
 
     ctx->seg_used = 0;
     ctx->seg_open = false;
-    ctx->loop_launches = ctx->total_launches = 0;
+    ctx->loop_launches = ctx->total_launches = ctx->loop_iters = 0;
     POTTS_TRY(ensure(ctx, ctx->err, sizeof(int)));
     POTTS_CUDA(cudaMemsetAsync(ctx->err.p, 0, sizeof(int), ctx->stream));
     POTTS_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
@@ -861,6 +915,7 @@ int solve_k(potts_context *ctx, const float *d_u, const float *ci, float lam, fl
         stats->solve_ms = ms;
         POTTS_TRY(seg_total_ms(ctx, &stats->loop_ms));
         stats->loop_launches = ctx->loop_launches;
+        stats->loop_iters = ctx->loop_iters;
         stats->total_launches = ctx->total_launches;
         stats->state_bytes = state_bytes;
         stats->dq_last = 0.0f;
@@ -897,6 +952,7 @@ int check_params(int K, const float *ci, float lam, float tau1, float tau2, int 
     if (o.prefetch > 16) return fail(POTTS_EINVAL, "prefetch must be <= 16");
     if (o.arith != POTTS_ARITH_EXACT && o.arith != POTTS_ARITH_FAST) return fail(POTTS_EINVAL, "unknown arith");
     if (o.stall_plane < 0) return fail(POTTS_EINVAL, "stall_plane must be >= 0");
+    if (o.persistent != 0 && o.persistent != 1) return fail(POTTS_EINVAL, "persistent must be 0 or 1");
     return POTTS_OK;
 }
 
@@ -1034,7 +1090,7 @@ int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int 
     float *dq = static_cast<float *>(ctx->dq.p);
     ctx->seg_used = 0;
     ctx->seg_open = false;
-    ctx->loop_launches = ctx->total_launches = 0;
+    ctx->loop_launches = ctx->total_launches = ctx->loop_iters = 0;
     POTTS_CUDA(cudaEventRecord(ctx->ev0, s));
     // xi starts at zero; every other plane is written at the voxels it is read at before it is read
     POTTS_CUDA(cudaMemsetAsync(ctx->state.p, 0, sizeof(float) * 3 * (size_t)std::max<int64_t>(g.plane_w, 1), s));
@@ -1059,16 +1115,19 @@ int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int 
                 map_in ^= 1;
                 ctx->loop_launches += 1;
                 ctx->total_launches += 1;
+                ctx->loop_iters += 1;
             } else if (variant == POTTS_VARIANT_PLAIN) {
                 potts::tv_div_kernel<<<nb, potts::kPlainThreads, 0, s>>>(g, xi, v);
                 potts::tv_grad_kernel<<<nb, potts::kPlainThreads, 0, s>>>(g, d_g, xi, v, lam, tau, dq + it);
                 ctx->loop_launches += 2;
                 ctx->total_launches += 2;
+                ctx->loop_iters += 1;
             } else {
                 potts::tv_fused_kernel<<<nb, potts::kPlainThreads, 0, s>>>(g, d_g, xi, xi_b, lam, tau, dq + it);
                 std::swap(xi, xi_b);
                 ctx->loop_launches += 1;
                 ctx->total_launches += 1;
+                ctx->loop_iters += 1;
             }
         }
         POTTS_TRY(seg_end(ctx));
@@ -1087,6 +1146,7 @@ int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int 
         stats->solve_ms = ms;
         POTTS_TRY(seg_total_ms(ctx, &stats->loop_ms));
         stats->loop_launches = ctx->loop_launches;
+        stats->loop_iters = ctx->loop_iters;
         stats->total_launches = ctx->total_launches;
         stats->state_bytes = sizeof(float) * planes * (uint64_t)std::max<int64_t>(g.plane_w, 1);
         stats->dq_last = 0.0f;
@@ -1130,6 +1190,7 @@ void potts_default_options(potts_options *o)
     o->autotune = 0;
     o->arith = POTTS_ARITH_EXACT;
     o->stall_plane = 0;
+    o->persistent = 0;
 }
 
 const char *potts_status_string(int s)
@@ -1161,7 +1222,7 @@ void potts_context_destroy(potts_context *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (DevBuf *b : {&ctx->lines, &ctx->state, &ctx->dq, &ctx->energy, &ctx->partial, &ctx->host_u,
                       &ctx->host_res, &ctx->host_labels, &ctx->ustage, &ctx->err, &ctx->cols, &ctx->work, &ctx->vols,
-                      &ctx->hist, &ctx->io, &ctx->io_tables})
+                      &ctx->hist, &ctx->io, &ctx->io_tables, &ctx->pctl})
         if (b->p) cudaFree(b->p);
     if (ctx->pinned_dq) cudaFreeHost(ctx->pinned_dq);
     for (cudaEvent_t e : ctx->seg_ev) cudaEventDestroy(e);
@@ -1431,7 +1492,8 @@ int potts_batch_run(potts_batch *b, potts_stats *stats)
     stats->iters = b->iters;
     stats->solve_ms = ms;
     stats->loop_ms = lms;
-    stats->loop_launches = b->iters > 1 ? b->iters - 1 : 0;
+    stats->loop_launches = b->loop_launches;
+    stats->loop_iters = b->iters > 1 ? b->iters - 1 : 0;
     stats->total_launches = b->graph_launches;
     stats->state_bytes = b->state_bytes;
     stats->dq_last = 0.0f;

@@ -159,6 +159,7 @@ class SolveStats:
     state_bytes: int
     dq_trace: Optional[np.ndarray] = None       # [iters] max |dV|^2 per iteration (last slab)
     energy_trace: Optional[np.ndarray] = None   # [iters // gap_every, 3] (lagrangian, dual, gap)
+    loop_iters: int = 0                         # iterations inside loop_ms
 
 
 def _make_stats(iters: int, gap_every: int, want_traces: bool):
@@ -175,7 +176,8 @@ def _make_stats(iters: int, gap_every: int, want_traces: bool):
 
 def _stats_out(st, dq, en) -> SolveStats:
     return SolveStats(st.n_slabs, st.slab_w, st.iters, float(st.dq_last), float(st.solve_ms), float(st.loop_ms),
-                      int(st.loop_launches), int(st.total_launches), int(st.state_bytes), dq, en)
+                      int(st.loop_launches), int(st.total_launches), int(st.state_bytes), dq, en,
+                      int(st.loop_iters))
 
 
 def potts_min_partition(ctx: CudaContext, g: DeviceField, cpu_map: CylinderMapping, ci: Sequence[float],

@@ -1,6 +1,7 @@
 """Batched solves (potts_batch_create / potts_batch_run): every volume of a batch gives
-the bits of its own single-volume solve, for each storage format, with the default tile
-and with the autotuner's; replays reread u."""
+the bits of its own single-volume solve, for each storage format, with the iterations as one
+persistent launch (the default) or one launch each, with the default tile and with the
+autotuner's; replays reread u."""
 import numpy as np
 import pytest
 
@@ -49,17 +50,21 @@ def _check_against_single(vols, iters, **opts):
         assert np.array_equal(mv(v["V"].cpu().numpy().reshape(K - 1, -1)), mv(g.V))
 
 
+@pytest.mark.parametrize("persistent", [1, 0])
 @pytest.mark.parametrize("store", ["f32", "bf16", "f16"])
 @pytest.mark.parametrize("K", [3, 4])
-def test_batch_equals_single_volume_solves(cuda_device, store, K):
+def test_batch_equals_single_volume_solves(cuda_device, store, K, persistent):
     iters = 14
     vols = _batch_inputs(K)
     with potts.make_context(0) as ctx:
-        with _make(ctx, vols, iters, storage=store) as b:
+        with _make(ctx, vols, iters, storage=store, persistent=persistent) as b:
             st = b.run()
             info = b.info()
-            assert info.n_volumes == len(vols) and info.n_work > 0 and info.graph_launches > iters - 1
-            assert st.loop_launches == iters - 1 and st.solve_ms > 0 and st.loop_ms > 0
+            assert info.n_volumes == len(vols) and info.n_work > 0
+            # set-up and finish launches per volume, plus the iterations: one persistent launch, or one each
+            assert info.graph_launches >= (1 if persistent else iters - 1) + len(vols)
+            assert st.loop_launches == (1 if persistent else iters - 1)
+            assert st.loop_iters == iters - 1 and st.solve_ms > 0 and st.loop_ms > 0
             _check_against_single(vols, iters, storage=store)
             dq = b.dq()
             for i, v in enumerate(vols):
