@@ -66,7 +66,7 @@ METRIC = "Potts PD Gvox-iter/s at k=3, %HBM peak; BF16-store vs FP32 at ≤1e-4 
 UNIT = "Gvox-iter/s"
 K_LABELS = 3
 LAMBDA = 30.0
-RADIUS = {"config1": 370.0, "config2": 370.0, "config0": 60.0, "mid": 180.0, "mid4": 180.0}
+RADIUS = {"config1": 370.0, "config2": 370.0, "config0": 60.0, "mid": 180.0, "mid4": 180.0, "prof": 246.0}
 STORE_BYTES = {"f32": 4, "bf16": 2, "f16": 2}
 
 
@@ -82,18 +82,22 @@ def parse_args():
                    help="voxel: TV workloads only, the per-voxel fused TV kernel")
     p.add_argument("--storage", choices=["f32", "bf16", "f16"], default="f32",
                    help="state storage of the timed solves")
-    p.add_argument("--arith", choices=["exact", "fast"], default="exact",
-                   help="FP32 arithmetic of the solves: exact (the reference's operations, bit-identical to the "
-                        "FP32 oracle) or fast (fewer operations, held to the FP64 oracle)")
+    p.add_argument("--arith", choices=["exact", "fast"], default="fast",
+                   help="FP32 arithmetic of the solves: fast (the default: fewer operations, held to the FP64 "
+                        "oracle within 1e-5 relative on V) or exact (the reference's operations, bit-identical to "
+                        "the FP32 oracle)")
     p.add_argument("--no-storage-compare", action="store_true",
                    help="skip the FP32-plain / BF16 / FP16 comparison solves")
-    p.add_argument("--workload", choices=["config1", "config2", "config3", "config4", "config0", "mid", "mid4", "tv", "tvmid",
+    p.add_argument("--workload", choices=["config1", "config2", "config3", "config4", "config0", "mid", "mid4", "prof", "tv", "tvmid",
                             "fieldio", "fieldiomid", "labels", "labelsmid"],
                    default="config1",
                    help="config1: 768x768x1024 r=370 (the benchmark); config0: 128^3 r=60; "
-                        "mid: 384x384x256 r=180 (profiling size, state > L2)")
+                        "mid: 384x384x256 r=180 (profiling size, state > L2); "
+                        "prof: 512x512x256 r=246 (profiling size with 5 waves of work items, 3.3 GB)")
     p.add_argument("--fd-coords", type=int, default=64,
                    help="config4: random u coordinates checked against FP64 central differences")
+    p.add_argument("--shard", action="store_true",
+                   help="config1 as one volume split by columns over the ranks (NCCL halo exchange, strong scaling)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
@@ -336,6 +340,8 @@ def run_ours(args, dist_: Dist) -> None:
         ph = config2_phantom(seed=dist_.rank, device=dev)
     elif args.workload == "config0":
         ph = config0_phantom(seed=dist_.rank, device=dev)
+    elif args.workload == "prof":
+        ph = make_phantom(256, 512, 512, 246.0, seed=dist_.rank, radius_range=(6.0, 30.0), noise=7e-3, device=dev)
     else:
         ph = make_phantom(256, 384, 384, 180.0, seed=dist_.rank, radius_range=(6.0, 30.0), noise=7e-3, device=dev,
                           k=4 if args.workload == "mid4" else 3)
@@ -543,6 +549,8 @@ def storage_compare(args, dist_: Dist, ctx, m, u, ci, tau, stream, dev, fused_va
     plain_value = out["f32_plain"]["value"]
     out["f32_fused"] = timed("f32", 0, args.arith)
     out["f32_fused"]["timed_line_value"] = round(fused_value, 3)
+    if args.arith == "fast":
+        out["f32_fused_exact"] = timed("f32", 0, "exact")
     for storage in ("bf16", "f16"):
         r = timed(storage, 0, args.arith)
         r["speedup_vs_f32_plain"] = round(r["value"] / plain_value, 3)
@@ -1204,11 +1212,92 @@ def run_labels(args, dist_: Dist) -> None:
     dist_.close()
 
 
+def run_shard(args, dist_: Dist) -> None:
+    """One volume (768 x 768 x 1024, r = 370, K = 3) split by columns over the ranks, one shard per
+    GPU, halos over NCCL (potts_shard_*): strong scaling, value = the volume's voxel-iterations per
+    second over the slowest rank's device time."""
+    import torch
+
+    from segmentctscans_b200 import potts
+    from segmentctscans_b200.phantom import config1_phantom
+    from segmentctscans_b200.sharding import Shard, destroy_comm, native_bounds, native_cuts, nccl_comm, run_shards
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    dev = torch.device("cuda", dist_.local)
+    torch.cuda.set_device(dev)
+    dist_.init("nccl")
+    ph = config1_phantom(seed=0, device=dev)  # the same volume on every rank
+    m, u, ci = ph.mapping, ph.u, ph.ci
+    del ph
+    torch.cuda.empty_cache()
+    tau = tau_baseline()
+    stream = torch.cuda.current_stream(dev)
+    ctx = potts.make_context(dev.index, stream=stream.cuda_stream)
+    cuts = native_cuts(m, dist_.world)
+    cols, span = native_bounds(m, cuts, dist_.rank)
+    comm = nccl_comm(dist_.rank, dist_.world, dev.index) if dist_.world > 1 else None
+    opts = {"arith": args.arith, "storage": args.storage, "gap_every": args.gap_every, "prefetch": args.prefetch}
+    shard = Shard(ctx, m, cuts, dist_.rank, u.data_ptr() + 4 * span[0], ci, LAMBDA, tau, tau, **opts)
+    if comm is not None:
+        shard.use_nccl(comm)
+    lab = torch.empty(shard.local_span, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        run_shards([shard], args.iters, label_ptrs=[lab.data_ptr()])
+    torch.cuda.synchronize(dev)
+    dist_.barrier()
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    stats = [run_shards([shard], args.iters, label_ptrs=[lab.data_ptr()]) for _ in range(args.steps)]
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    dist_.barrier()
+    clk = clocks.stop()
+    t_max = dist_.reduce(e0.elapsed_time(e1) / 1000.0, "max")
+    vox = m.data_size
+    value = float(vox) * args.iters * args.steps / t_max / 1e9
+    own_vox = int(m.base[cols[3]] - m.base[cols[2]]) // m.nstride * m.n_images
+    iter_s = sum(s.loop_ms for s in stats) / 1000.0 / max(sum(s.loop_iters for s in stats), 1)
+    bpv = bytes_per_voxel_iter("fused", 3, args.storage)
+    achieved = dist_.reduce(bpv * own_vox / iter_s / 1e9, "sum")
+    peaks = measured_peaks()
+    shard.close()
+    destroy_comm(comm)
+    if dist_.rank == 0:
+        out = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist_.world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": round(1000 * t_max / args.steps, 2), "higher_is_better": True,
+               "scaling": "strong", "vs_baseline": None,
+               "dtype": "f32" if args.storage == "f32" else f"f32 math, {args.storage} state", "data": "synthetic",
+               "config": {"workload": "potts_k3_768x768x1024_r370_column_shards", "in_mask_voxels": vox,
+                          "iters": args.iters, "gap_every": args.gap_every, "arith": args.arith,
+                          "storage": args.storage, "parallelism": f"column shards x{dist_.world} (NCCL halos)",
+                          "cuts": cuts, "l2": "inputs larger than L2"},
+               "roofline": {"bound": "hbm", "achieved": round(achieved, 1),
+                            "peak": peaks["hbm_gbs"] * dist_.world, "unit": "GB/s",
+                            "frac": round(achieved / (peaks["hbm_gbs"] * dist_.world), 4), "traffic": None,
+                            "kernel": "potts::fused_tiled_kernel (per shard)", "bytes_per_voxel_iter": bpv,
+                            "avg_iter_ms_rank0": round(iter_s * 1000, 4),
+                            "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs) x ranks"},
+               "e2e": None, "gpu_launches": sum(s.total_launches for s in stats), "clocks": clk,
+               "cpu_baseline": None,
+               "quality": {"final_sqrt_max_dV2": stats[-1].dq_last,
+                           "energy_last": stats[-1].energy_trace[-1].tolist()
+                           if stats[-1].energy_trace is not None else None}}
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    dist_.close()
+
+
 def main():
     args = parse_args()
     d = Dist()
     if args.impl == "reference":
         run_reference(args, d)
+        return
+    if args.shard:
+        run_shard(args, d)
         return
     if args.workload == "config3":
         run_batch(args, d)

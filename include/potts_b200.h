@@ -103,14 +103,15 @@ typedef struct potts_options {
     int slab_w;       /* 0: plan slabs from free memory like the reference; > 0: force this slab width */
     int track_dq;     /* 1: record max_x |V^{k+1} - V^k|^2 of every iteration on the device */
     int sync_monitor; /* 1: reference behaviour, read the monitor back and sync after every iteration */
-    int tile_rows;    /* fused form: rows per tile (0 = default for K) */
+    int tile_rows;    /* fused form: rows per tile (0 = default for K and arith) */
     int tile_slices;  /* fused form: slices (n) per tile (0 = default for K) */
     int segment_cols; /* fused form: columns one tile marches over (0 = 64, at most 64) */
     int tile_vpt;     /* fused form: consecutive slices per thread, 2 or 4 (0 = default for K) */
     int prefetch;     /* fused form: planes the load ring prefetches into L2 ahead of its loads
-                         (0 = default, < 0 = none, at most 16) */
-    int autotune;     /* batches: 1 = time every compiled tile shape and segment length on the batch
-                         and keep the fastest (used when no tile option is set); 0 = default tile */
+                         (0 = default: none, < 0 = none, at most 16) */
+    int autotune;     /* batches: 1 = time every compiled tile shape and segment length, each as one
+                         launch per iteration and as the persistent launch, on the batch and keep the
+                         fastest (used when no tile option is set); 0 = default tile and launch form */
     int arith;        /* enum potts_arith (default EXACT) */
     int stall_plane;  /* testing the bounded waits: > 0 makes the fused kernel's first work item skip
                          the loads of that plane of its column march, so every wait for it gives up
@@ -279,6 +280,7 @@ typedef struct potts_batch_info {
     uint64_t state_bytes;
     int graph_launches; /* kernel launches in the captured graph */
     double autotune_ms; /* device time spent autotuning (0 without) */
+    int persistent;     /* 1: the iterations run as one persistent launch, 0: one launch each */
 } potts_batch_info;
 
 int potts_batch_create(potts_context *ctx, int n_volumes, const potts_batch_volume *volumes, int K, float tau1,
@@ -316,23 +318,52 @@ int potts_backward(potts_tape *tape, float *d_grad_u, double *grad_ci, double *g
 void potts_tape_destroy(potts_tape *tape);
 
 /* ---------------------------------------------------------------------------
- * Step-by-step split solve (no counterpart in the reference), for column
- * sharding over several GPUs: the caller exchanges halo columns between the
- * steps.  FP32 state, laid out with the mapping's own stride (component i of
- * xi / v / vb starts at the returned pointer + i * plane_w, voxel (n, row, col)
- * at the mapping's offset), so that a column's lines are the same span range
- * in the state as in the mapping.  Create runs the nearest-label init; each
- * call enqueues on the context's stream.
+ * Column sharding of one volume: the iteration loop of potts_min_partition
+ * (potts-model/potts-min-partition.cpp:625-660) over several GPUs, one shard
+ * per GPU (a rank of an NCCL communicator), or over several shards that one
+ * process holds on one context (their halos move by device copies).
+ *
+ * The active columns are split into contiguous ranges (potts_shard_partition:
+ * about equal in-mask voxels).  Shard r owns the columns [cuts[r], cuts[r+1])
+ * and holds the global columns [first, last) = one column before and two
+ * after (where the volume has them).  Its u is the global u's span range
+ * [base[first], base[last]) (potts_shard_bounds gives both).  Each iteration
+ * is one fused launch per shard and an exchange of the Xi planes of one column
+ * with each neighbour; at the end the convergence trace is reduced by max and
+ * the FP64 energies by sum over all shards.  The owned voxels get the bits of
+ * potts_solve_device with the same options (fused form; FP32, bfloat16 or
+ * binary16 state).  Every rank must call potts_shard_solve with the same
+ * iters and options.
  * ------------------------------------------------------------------------- */
-typedef struct potts_stepper potts_stepper;
+typedef struct potts_shard potts_shard;
 
-int potts_stepper_create(potts_context *ctx, const potts_mapping *map, const float *d_u, int K, const float *ci,
-                         float lambda, float tau1, float tau2, potts_stepper **out);
-int potts_stepper_dual(potts_stepper *stepper);            /* Xi <- Pi_K(Xi + tau2 grad+ Vbar) */
-int potts_stepper_primal(potts_stepper *stepper, int it);  /* V, Vbar of iteration it (0-based) */
-int potts_stepper_state(potts_stepper *stepper, float **xi, float **v, float **vb, int64_t *plane_w);
-int potts_stepper_finish(potts_stepper *stepper, float *d_res, uint8_t *d_labels, float *d_V);
-void potts_stepper_destroy(potts_stepper *stepper);
+/* cuts[0 .. world]: cuts[0] = col_begin < cuts[1] < ... < cuts[world] = col_end. */
+int potts_shard_partition(const potts_mapping *map, int world, uint32_t *cuts);
+/* cols (optional, 4 values): first, last, own_begin, own_end (global columns);
+   span (optional, 2 values): base[first], base[last] (the shard's span range in the global arrays). */
+int potts_shard_bounds(const potts_mapping *map, const uint32_t *cuts, int world, int rank, uint32_t *cols,
+                       uint64_t *span);
+/* d_u: the shard's u (the global u + span[0]); not copied, must stay valid.  opts: as for
+   potts_solve_device (fused form only; tile, arith, storage, gap_every, prefetch are used). */
+int potts_shard_create(potts_context *ctx, const potts_mapping *map, const uint32_t *cuts, int world, int rank,
+                       const float *d_u, int K, const float *ci, float lambda, float tau1, float tau2,
+                       const potts_options *opts, potts_shard **out);
+/* Shards of neighbouring ranks held by this process (one context). */
+int potts_shard_link(potts_shard *left, potts_shard *right);
+/* NCCL: the library loads libnccl.so.2 (the one already in the process, else the system's).
+   id: 128 bytes, made on one rank and passed to every rank by the caller. */
+int potts_nccl_unique_id(void *id);
+int potts_nccl_comm_create(const void *id, int world, int rank, int device, void **comm);
+int potts_nccl_comm_destroy(void *comm);
+/* The shard exchanges with ranks rank - 1 and rank + 1 of comm (size world, this shard's rank). */
+int potts_shard_set_nccl(potts_shard *shard, void *comm);
+/* Solves: shards = every shard of this process (all ranks in order and linked, or one NCCL shard);
+   d_res / d_labels / d_V (arrays of n pointers, or NULL; entries may be NULL): ci[argmax], the
+   argmax and V (K-1 planes of the shard's span) for the owned voxels, in the shard's span layout.
+   stats: dq_trace and energy_trace of the whole volume; timing of this process.  Blocks until done. */
+int potts_shard_solve(potts_shard *const *shards, int n, int iters, float *const *d_res, uint8_t *const *d_labels,
+                      float *const *d_V, potts_stats *stats);
+void potts_shard_destroy(potts_shard *shard);
 
 /* TV-L2 (ROF) denoising of a field in place: chambolle() of
  * totalvarmin/chambolle.cpp:220-276 (Chambolle's projection algorithm, xi and

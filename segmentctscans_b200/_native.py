@@ -60,7 +60,7 @@ class PottsBatchInfo(ctypes.Structure):
         ("n_volumes", ctypes.c_int), ("n_work", ctypes.c_int), ("tile_rows", ctypes.c_int),
         ("tile_slices", ctypes.c_int), ("tile_vpt", ctypes.c_int), ("segment_cols", ctypes.c_int),
         ("voxels", ctypes.c_uint64), ("state_bytes", ctypes.c_uint64), ("graph_launches", ctypes.c_int),
-        ("autotune_ms", ctypes.c_double),
+        ("autotune_ms", ctypes.c_double), ("persistent", ctypes.c_int),
     ]
 
 
@@ -124,13 +124,18 @@ SIGNATURES = {
                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_P)]),
     "potts_backward": (_I, [_P, _P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "potts_tape_destroy": (None, [_P]),
-    "potts_stepper_create": (_I, [_P, _MP, _P, _I, _FP, _F, _F, _F, ctypes.POINTER(_P)]),
-    "potts_stepper_dual": (_I, [_P]),
-    "potts_stepper_primal": (_I, [_P, _I]),
-    "potts_stepper_state": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),
-                                 ctypes.POINTER(ctypes.c_int64)]),
-    "potts_stepper_finish": (_I, [_P, _P, _P, _P]),
-    "potts_stepper_destroy": (None, [_P]),
+    "potts_shard_partition": (_I, [_MP, _I, ctypes.POINTER(_U32)]),
+    "potts_shard_bounds": (_I, [_MP, ctypes.POINTER(_U32), _I, _I, ctypes.POINTER(_U32), ctypes.POINTER(_U64)]),
+    "potts_shard_create": (_I, [_P, _MP, ctypes.POINTER(_U32), _I, _I, _P, _I, _FP, _F, _F, _F, _OP,
+                                ctypes.POINTER(_P)]),
+    "potts_shard_link": (_I, [_P, _P]),
+    "potts_nccl_unique_id": (_I, [_P]),
+    "potts_nccl_comm_create": (_I, [_P, _I, _I, _I, ctypes.POINTER(_P)]),
+    "potts_nccl_comm_destroy": (_I, [_P]),
+    "potts_shard_set_nccl": (_I, [_P, _P]),
+    "potts_shard_solve": (_I, [ctypes.POINTER(_P), _I, _I, ctypes.POINTER(_P), ctypes.POINTER(_P),
+                               ctypes.POINTER(_P), _SP]),
+    "potts_shard_destroy": (None, [_P]),
     "potts_tv_denoise": (_I, [_P, _MP, _P, _F, _F, _I, _I, _SP]),
     "potts_min_max": (_I, [_P, _MP, _P, _FP, _FP]),
     "potts_min_max_positive": (_I, [_P, _MP, _P, _FP, _FP]),

@@ -184,11 +184,12 @@ int batch_enqueue_tail(potts_batch *b, int cur)
     return POTTS_OK;
 }
 
-// Tile autotuner: time a few iteration launches of every compiled tile shape
-// (and three segment lengths) on the batch itself; keep the fastest.  The
-// solution does not depend on the tile, so the choice only changes speed.
+// Tile autotuner: time a few iterations of every compiled tile shape (and
+// three segment lengths), as one launch per iteration and as the persistent
+// launch, on the batch itself; keep the fastest.  The solution depends on
+// neither, so the choice only changes speed.
 template <int K, typename ST>
-int batch_autotune(potts_batch *b, TileChoice *best)
+int batch_autotune(potts_batch *b, TileChoice *best, int *best_persistent)
 {
     potts_context *ctx = b->ctx;
     using TS = ShapesOf<K, ST>;
@@ -210,25 +211,40 @@ int batch_autotune(potts_batch *b, TileChoice *best)
             if (rc != POTTS_OK) break;
             rc = batch_enqueue_head<K, ST>(b);
             if (rc != POTTS_OK) break;
-            // one untimed launch, then kTrials timed ones
-            for (int m = 0; m <= kTrials && rc == POTTS_OK; ++m) {
-                if (m == 1) cudaEventRecord(e0, ctx->stream);
-                rc = launch_tiled<K, ST>(ctx, tc, b->opts.arith == POTTS_ARITH_FAST, static_cast<const potts::FusedVolume<K, ST> *>(b->desc.p),
-                                         static_cast<const int4 *>(b->work.p), static_cast<const int *>(b->work_vol.p),
-                                         b->n_work, m & 1, m, b->tau2);
-            }
-            if (rc != POTTS_OK) break;
-            cudaEventRecord(e1, ctx->stream);
-            if (cudaEventSynchronize(e1) != cudaSuccess) {
-                rc = fail(POTTS_ECUDA, "autotune timing failed");
-                break;
-            }
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (!have || ms < best_ms) {
-                best_ms = ms;
-                *best = tc;
-                have = true;
+            const bool fast = b->opts.arith == POTTS_ARITH_FAST;
+            const auto *vols = static_cast<const potts::FusedVolume<K, ST> *>(b->desc.p);
+            const auto *work = static_cast<const int4 *>(b->work.p);
+            const auto *work_vol = static_cast<const int *>(b->work_vol.p);
+            // form 0: one launch per iteration (one untimed, then kTrials timed);
+            // form 1: the persistent launch (one iteration untimed, then kTrials in one launch)
+            for (int form = 0; form < 2 && rc == POTTS_OK; ++form) {
+                if (form == 0) {
+                    for (int m = 0; m <= kTrials && rc == POTTS_OK; ++m) {
+                        if (m == 1) cudaEventRecord(e0, ctx->stream);
+                        rc = launch_tiled<K, ST>(ctx, tc, fast, vols, work, work_vol, b->n_work, m & 1, m, b->tau2);
+                    }
+                } else {
+                    rc = launch_tiled_persistent<K, ST>(ctx, b->pctl, tc, fast, vols, work, work_vol, b->n_work, 0, 0,
+                                                        1, b->tau2);
+                    cudaEventRecord(e0, ctx->stream);
+                    if (rc == POTTS_OK)
+                        rc = launch_tiled_persistent<K, ST>(ctx, b->pctl, tc, fast, vols, work, work_vol, b->n_work,
+                                                            1, 1, kTrials, b->tau2);
+                }
+                if (rc != POTTS_OK) break;
+                cudaEventRecord(e1, ctx->stream);
+                if (cudaEventSynchronize(e1) != cudaSuccess) {
+                    rc = fail(POTTS_ECUDA, "autotune timing failed");
+                    break;
+                }
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (!have || ms < best_ms) {
+                    best_ms = ms;
+                    *best = tc;
+                    *best_persistent = form;
+                    have = true;
+                }
             }
         }
     cudaEventRecord(t1, ctx->stream);
@@ -305,7 +321,7 @@ int batch_build(potts_batch *b)
     const potts_options &o = b->opts;
     if (o.autotune && o.tile_rows <= 0 && o.tile_slices <= 0 && o.tile_vpt <= 0 && o.segment_cols <= 0 &&
         b->iters > 1) {
-        POTTS_TRY((batch_autotune<K, ST>(b, &tile)));
+        POTTS_TRY((batch_autotune<K, ST>(b, &tile, &b->opts.persistent)));
     } else {
         POTTS_TRY((choose_tile<K, ST>(o, &tile)));
     }

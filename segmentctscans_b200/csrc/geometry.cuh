@@ -32,6 +32,11 @@ struct Geometry {
     int ns;             // n-extent of the slab: n in [0, ns)
     int nstride_in;     // stride of n in u and in the outputs
     int slab_start;     // n of the slab's first slice in u
+    // The plain kernels run over the lines [line_begin, n_lines) (a shard's
+    // owned lines; 0 = all).  line_base: the line number of line 0 in the
+    // whole volume (keys the stochastic rounding of a shard's bfloat16 V).
+    int64_t line_begin = 0;
+    int64_t line_base = 0;
 };
 
 template <int K>

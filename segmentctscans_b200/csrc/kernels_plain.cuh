@@ -30,7 +30,7 @@ __device__ __forceinline__ PlainIndex plain_index(const Geometry &g, int n_begin
 {
     const int chunks = (n_end - n_begin + kPlainThreads - 1) / kPlainThreads;
     PlainIndex p;
-    p.line = (int64_t)blockIdx.x / chunks;
+    p.line = g.line_begin + (int64_t)blockIdx.x / chunks;
     p.n = n_begin + (int)(blockIdx.x % chunks) * kPlainThreads + (int)threadIdx.x;
     p.valid = p.line < g.n_lines && p.n < n_end;
     return p;
@@ -163,7 +163,8 @@ __global__ void __launch_bounds__(kPlainThreads) primal_kernel(Geometry g, const
         if constexpr (Store<ST>::kStochasticV) {
 #pragma unroll
             for (int k = 0; k < (K - 1 + 1) / 2; ++k)
-                h[k] = sr_hash((uint32_t)p.line, (uint32_t)(g.slab_start + p.n), (uint32_t)it, (uint32_t)k);
+                h[k] = sr_hash((uint32_t)(g.line_base + p.line), (uint32_t)(g.slab_start + p.n), (uint32_t)it,
+                               (uint32_t)k);
         }
 #pragma unroll
         for (int i = 0; i < K - 1; ++i) {

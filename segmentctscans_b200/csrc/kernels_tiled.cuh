@@ -71,6 +71,7 @@ struct TiledParams {
     int it;         // 0-based iteration of the launch's primal step (keys stochastic rounding)
     int prefetch;   // planes ahead of the load ring prefetched into L2 (0: none)
     int stall_plane;  // testing: > 0 = the first work item never loads that ring position (0: off)
+    int64_t line_base;  // line number of line 0 in the whole volume (keys stochastic rounding)
 };
 
 template <int K, int R, int NT, int VPT, typename ST>
@@ -378,7 +379,7 @@ __device__ __forceinline__ void stage_a_chunk(const TiledSmem<K, R, NT, VPT, ST>
     if (store_v) {
         const int64_t o = (int64_t)(ci.x + row - ci.y) * tp.nstride_w + nb;
         if constexpr (Store<ST>::kStochasticV) {
-            const uint32_t line = (uint32_t)(ci.x + row - ci.y);
+            const uint32_t line = (uint32_t)(tp.line_base + ci.x + row - ci.y);
             ST sv[K - 1][VPT];
 #pragma unroll
             for (int j = 0; j < VPT; ++j) {
@@ -880,7 +881,7 @@ __device__ __forceinline__ void tiled_item(const TiledSmem<K, R, NT, VPT, ST> &s
                     const int c = ca - 1 + p;
                     if (p == 0 && c < tp.col_begin) {  // no plane before the first column
                         mbar_arrive(sm.full(0));
-                    } else if (p == tp.stall_plane && item == 0) {
+                    } else if (tp.stall_plane > 0 && p == tp.stall_plane && item == 0) {
                         // testing: this plane never arrives, so the waits for it run out
                     } else {
                         const int4 ci = sm.cols()[p];

@@ -2,8 +2,12 @@
 // slab planner and the iteration driver (potts-model/potts-min-partition.cpp:540-679).
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <dlfcn.h>
+#include <nccl.h>
 
 #include <algorithm>
+#include <memory>
+#include <mutex>
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
@@ -343,7 +347,7 @@ struct Outputs {
 inline unsigned plain_blocks(const Geometry &g, int n_begin, int n_end)
 {
     const int chunks = (n_end - n_begin + potts::kPlainThreads - 1) / potts::kPlainThreads;
-    return (unsigned)(g.n_lines * chunks);
+    return (unsigned)((g.n_lines - g.line_begin) * chunks);
 }
 
 template <int K, typename ST>
@@ -352,6 +356,10 @@ int run_energy(potts_context *ctx, const Geometry &g, const ST *xi, const ST *V,
 {
     POTTS_TRY(seg_end(ctx));
     const unsigned nb = plain_blocks(g, 0, g.ns);
+    if (nb == 0) return POTTS_OK;
+    // one pair of partial sums per block (the buffer is grown outside the iteration loops by the
+    // solvers; this keeps every caller safe)
+    POTTS_TRY(ensure(ctx, ctx->partial, sizeof(double2) * (size_t)nb));
     ctx->total_launches += 2;
     potts::energy_kernel<K, ST><<<nb, potts::kPlainThreads, 0, ctx->stream>>>(g, xi, V, d_u, pp,
                                                                           (double2 *)ctx->partial.p);
@@ -419,8 +427,9 @@ int encode_map(CUtensorMap *m, CUtensorMapDataType dt, const void *base, int ran
     return POTTS_OK;
 }
 
-// Planes of L2 prefetch ahead of the fused kernel's load ring.
-constexpr int kDefaultPrefetch = 2;
+// Planes of L2 prefetch ahead of the fused kernel's load ring by default
+// (none: prefetching 2 or 4 planes measured 0.5-3 % slower at 768^2 x 1024).
+constexpr int kDefaultPrefetch = 0;
 
 struct TileChoice {
     int rows, slices, vpt, segment;
@@ -430,9 +439,10 @@ template <int K, typename ST>
 int choose_tile(const potts_options &o, TileChoice *tc)
 {
     using TS = ShapesOf<K, ST>;
-    tc->rows = TS::r[0];
-    tc->slices = TS::t[0];
-    tc->vpt = TS::v[0];
+    const int d = o.arith == POTTS_ARITH_FAST ? TS::fast : 0;
+    tc->rows = TS::r[d];
+    tc->slices = TS::t[d];
+    tc->vpt = TS::v[d];
     tc->segment = o.segment_cols > 0 ? o.segment_cols : 64;
     if (tc->segment > 64) return fail(POTTS_EINVAL, "segment_cols must be <= 64");
     if (o.tile_rows > 0 || o.tile_slices > 0 || o.tile_vpt > 0) {
@@ -467,10 +477,13 @@ std::vector<int4> column_table(const potts_mapping &m)
 // column range), ordered so that items sharing columns run together (halo
 // rows of neighbouring tiles meet in L2), the slice tiles of the same rows side
 // by side.
-std::vector<int4> work_items(const potts_mapping &m, int ns, const TileChoice &tc)
+std::vector<int4> work_items(const potts_mapping &m, int ns, const TileChoice &tc, int c_begin = -1, int c_end = -1)
 {
+    // the columns [c_begin, c_end) (default: all active columns)
+    const uint32_t cb0 = c_begin < 0 ? m.col_begin : (uint32_t)c_begin;
+    const uint32_t ce0 = c_end < 0 ? m.col_end : (uint32_t)c_end;
     int row_lo = INT32_MAX, row_hi = 0;
-    for (uint32_t c = m.col_begin; c < m.col_end; ++c) {
+    for (uint32_t c = cb0; c < ce0; ++c) {
         const int64_t cnt = (int64_t)(m.base[c + 1] - m.base[c]) / m.nstride;
         if (cnt <= 0) continue;
         row_lo = std::min<int>(row_lo, (int)m.start_row[c]);
@@ -483,9 +496,9 @@ std::vector<int4> work_items(const potts_mapping &m, int ns, const TileChoice &t
     const int tiles = (ns + tc.slices - 1) / tc.slices;
     for (int r0 = row_lo; r0 < row_hi; r0 += tc.rows) {
         int run = -1;
-        for (int c = (int)m.col_begin; c <= (int)m.col_end; ++c) {
+        for (int c = (int)cb0; c <= (int)ce0; ++c) {
             bool active = false;
-            if (c < (int)m.col_end) {
+            if (c < (int)ce0) {
                 const int64_t cnt = (int64_t)(m.base[c + 1] - m.base[c]) / m.nstride;
                 active = cnt > 0 && (int)m.start_row[c] < r0 + tc.rows && (int)(m.start_row[c] + cnt) > r0;
             }
@@ -1029,7 +1042,7 @@ int context_init(int device, void *stream, bool use_stream, potts_context **out)
 #include "batch.cuh"
 #include "label_inputs.cuh"
 #include "field_io.cuh"
-#include "stepper.cuh"
+#include "shard.cuh"
 
 // Work items, shared-memory size and the tensor maps of the two xi buffers (3 planes each,
 // boxes of XS slices x XR lines x 3 components) of the tiled TV kernel for TR x TN tiles.
@@ -1522,6 +1535,7 @@ int potts_batch_get_info(const potts_batch *b, potts_batch_info *info)
     info->state_bytes = b->state_bytes;
     info->graph_launches = b->graph_launches;
     info->autotune_ms = b->autotune_ms;
+    info->persistent = b->opts.persistent;
     return POTTS_OK;
 }
 
@@ -1626,74 +1640,6 @@ int potts_backward(potts_tape *t, float *d_grad_u, double *grad_ci, double *grad
 
 void potts_tape_destroy(potts_tape *t) { tape_free(t); }
 
-int potts_stepper_create(potts_context *ctx, const potts_mapping *map, const float *d_u, int K, const float *ci,
-                         float lambda, float tau1, float tau2, potts_stepper **out)
-{
-    if (!out) return fail(POTTS_EINVAL, "out is NULL");
-    *out = nullptr;
-    if (!ctx) return fail(POTTS_EINVAL, "context is NULL");
-    potts_options o;
-    potts_default_options(&o);
-    POTTS_TRY(check_params(K, ci, lambda, tau1, tau2, 0, o));
-    if (!d_u) return fail(POTTS_EINVAL, "u is NULL");
-    POTTS_CUDA(cudaSetDevice(ctx->device));
-    auto *st = new potts_stepper();
-    st->ctx = ctx;
-    int rc = copy_mapping(map, st->mc);
-    if (rc == POTTS_OK) {
-        st->K = K;
-        st->tau1 = tau1;
-        st->tau2 = tau2;
-        st->lambda = lambda;
-        for (int i = 0; i < K; ++i) st->c[i] = ci[i];
-        st->d_u = d_u;
-        const potts_mapping &m = st->mc.m;
-        st->g.n_lines = st->mc.n_lines;
-        st->g.nstride_w = (int)m.nstride;  // the mapping's layout
-        st->g.plane_w = st->mc.n_lines * (int64_t)m.nstride;
-        st->g.nstride_in = (int)m.nstride;
-        st->g.ns = (int)m.n_images;
-        st->g.slab_start = 0;
-        rc = ensure(ctx, st->lines, sizeof(int4) * (size_t)std::max<int64_t>(st->mc.n_lines, 1));
-        if (rc == POTTS_OK && st->mc.n_lines > 0 &&
-            cudaMemcpy(st->lines.p, st->mc.lines.data(), sizeof(int4) * st->mc.n_lines, cudaMemcpyHostToDevice) !=
-                cudaSuccess)
-            rc = fail(POTTS_ECUDA, "copying the line table failed");
-        st->g.lines = static_cast<const int4 *>(st->lines.p);
-        if (rc == POTTS_OK)
-            rc = ensure(ctx, st->state, sizeof(float) * 5 * (size_t)(K - 1) * (size_t)std::max<int64_t>(st->g.plane_w, 1));
-    }
-    if (rc == POTTS_OK) rc = stepper_dispatch(st, 0, 0, nullptr, nullptr, nullptr);
-    if (rc != POTTS_OK) {
-        const std::string msg = g_last_error;
-        stepper_free(st);
-        g_last_error = msg;
-        return rc;
-    }
-    *out = st;
-    return POTTS_OK;
-}
-
-int potts_stepper_dual(potts_stepper *s) { return stepper_dispatch(s, 1, 0, nullptr, nullptr, nullptr); }
-
-int potts_stepper_primal(potts_stepper *s, int it) { return stepper_dispatch(s, 2, it, nullptr, nullptr, nullptr); }
-
-int potts_stepper_state(potts_stepper *s, float **xi, float **v, float **vb, int64_t *plane_w)
-{
-    if (!s) return fail(POTTS_EINVAL, "stepper is NULL");
-    if (xi) *xi = stepper_xi(s);
-    if (v) *v = stepper_v(s);
-    if (vb) *vb = stepper_vb(s);
-    if (plane_w) *plane_w = s->g.plane_w;
-    return POTTS_OK;
-}
-
-int potts_stepper_finish(potts_stepper *s, float *d_res, uint8_t *d_labels, float *d_V)
-{
-    return stepper_dispatch(s, 3, 0, d_res, d_labels, d_V);
-}
-
-void potts_stepper_destroy(potts_stepper *s) { stepper_free(s); }
 
 int potts_tv_denoise(potts_context *ctx, const potts_mapping *map, float *d_g, float lambda, float tau, int iters,
                      int variant, potts_stats *stats)
@@ -1902,5 +1848,121 @@ int potts_png_slice(potts_context *ctx, const potts_mapping *map, const float *d
     POTTS_CUDA(cudaSetDevice(ctx->device));
     return png_slice_run(ctx, map, d_field, col, out, capacity, out_bytes);
 }
+
+int potts_shard_partition(const potts_mapping *map, int world, uint32_t *cuts)
+{
+    if (!cuts) return fail(POTTS_EINVAL, "cuts is NULL");
+    POTTS_TRY(validate_mapping(map));
+    return shard_partition(*map, world, cuts);
+}
+
+int potts_shard_bounds(const potts_mapping *map, const uint32_t *cuts, int world, int rank, uint32_t *cols,
+                       uint64_t *span)
+{
+    POTTS_TRY(validate_mapping(map));
+    ShardColumns sc;
+    POTTS_TRY(shard_columns(*map, cuts, world, rank, &sc));
+    if (cols) {
+        cols[0] = sc.first;
+        cols[1] = sc.last;
+        cols[2] = sc.own_begin;
+        cols[3] = sc.own_end;
+    }
+    if (span) {
+        span[0] = map->base[sc.first];
+        span[1] = map->base[sc.last];
+    }
+    return POTTS_OK;
+}
+
+int potts_shard_create(potts_context *ctx, const potts_mapping *map, const uint32_t *cuts, int world, int rank,
+                       const float *d_u, int K, const float *ci, float lambda, float tau1, float tau2,
+                       const potts_options *opts, potts_shard **out)
+{
+    if (!out) return fail(POTTS_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (!ctx) return fail(POTTS_EINVAL, "context is NULL");
+    potts_options o;
+    potts_default_options(&o);
+    if (opts) o = *opts;
+    return shard_create(ctx, map, cuts, world, rank, d_u, K, ci, lambda, tau1, tau2, o, out);
+}
+
+int potts_shard_link(potts_shard *left, potts_shard *right)
+{
+    if (!left || !right) return fail(POTTS_EINVAL, "shard is NULL");
+    if (left->ctx != right->ctx) return fail(POTTS_EINVAL, "linked shards share one context");
+    if (left->world != right->world || right->rank != left->rank + 1)
+        return fail(POTTS_EINVAL, "only neighbouring ranks are linked");
+    if (left->nccl || right->nccl) return fail(POTTS_EINVAL, "a shard on NCCL is not linked");
+    left->right = right;
+    right->left = left;
+    return POTTS_OK;
+}
+
+int potts_nccl_unique_id(void *id)
+{
+    if (!id) return fail(POTTS_EINVAL, "id is NULL");
+    const NcclApi *api;
+    POTTS_TRY(nccl_api(&api));
+    ncclUniqueId u;
+    POTTS_NCCL(api, api->GetUniqueId(&u));
+    std::memcpy(id, &u, sizeof(u));
+    return POTTS_OK;
+}
+
+int potts_nccl_comm_create(const void *id, int world, int rank, int device, void **comm)
+{
+    if (!id || !comm) return fail(POTTS_EINVAL, "id or comm is NULL");
+    *comm = nullptr;
+    if (world < 1 || rank < 0 || rank >= world) return fail(POTTS_EINVAL, "rank must be in [0, world)");
+    const NcclApi *api;
+    POTTS_TRY(nccl_api(&api));
+    POTTS_CUDA(cudaSetDevice(device));
+    ncclUniqueId u;
+    std::memcpy(&u, id, sizeof(u));
+    ncclComm_t c = nullptr;
+    POTTS_NCCL(api, api->CommInitRank(&c, world, u, rank));
+    *comm = c;
+    return POTTS_OK;
+}
+
+int potts_nccl_comm_destroy(void *comm)
+{
+    if (!comm) return POTTS_OK;
+    const NcclApi *api;
+    POTTS_TRY(nccl_api(&api));
+    POTTS_NCCL(api, api->CommDestroy(static_cast<ncclComm_t>(comm)));
+    return POTTS_OK;
+}
+
+int potts_shard_set_nccl(potts_shard *s, void *comm)
+{
+    if (!s || !comm) return fail(POTTS_EINVAL, "shard or comm is NULL");
+    if (s->left || s->right) return fail(POTTS_EINVAL, "a linked shard does not use NCCL");
+    const NcclApi *api;
+    POTTS_TRY(nccl_api(&api));
+    int count = 0, rank = -1;
+    POTTS_NCCL(api, api->CommCount(static_cast<ncclComm_t>(comm), &count));
+    POTTS_NCCL(api, api->CommUserRank(static_cast<ncclComm_t>(comm), &rank));
+    if (count != s->world || rank != s->rank)
+        return fail(POTTS_EINVAL, "the communicator's size and rank differ from the shard's");
+    s->nccl = static_cast<ncclComm_t>(comm);
+    return POTTS_OK;
+}
+
+int potts_shard_solve(potts_shard *const *shards, int n, int iters, float *const *d_res, uint8_t *const *d_labels,
+                      float *const *d_V, potts_stats *stats)
+{
+    POTTS_TRY(shard_check(shards, n, iters));
+    POTTS_CUDA(cudaSetDevice(shards[0]->ctx->device));
+    switch (shards[0]->opts.storage) {
+    case POTTS_STORE_BF16: return shard_solve_store<__nv_bfloat16>(shards, n, iters, d_res, d_labels, d_V, stats);
+    case POTTS_STORE_F16: return shard_solve_store<__half>(shards, n, iters, d_res, d_labels, d_V, stats);
+    default: return shard_solve_store<float>(shards, n, iters, d_res, d_labels, d_V, stats);
+    }
+}
+
+void potts_shard_destroy(potts_shard *s) { shard_free(s); }
 
 }  // extern "C"

@@ -313,6 +313,7 @@ class BatchInfo:
     state_bytes: int
     graph_launches: int
     autotune_ms: float
+    persistent: int = 0          # 1: the iterations run as one persistent launch
 
 
 class Batch:
@@ -358,7 +359,8 @@ class Batch:
         i = _native.PottsBatchInfo()
         check(_native.host_lib().potts_batch_get_info(self._h, ctypes.byref(i)))
         return BatchInfo(i.n_volumes, i.n_work, (i.tile_rows, i.tile_slices, i.tile_vpt, i.segment_cols),
-                         int(i.voxels), int(i.state_bytes), i.graph_launches, float(i.autotune_ms))
+                         int(i.voxels), int(i.state_bytes), i.graph_launches, float(i.autotune_ms),
+                         int(i.persistent))
 
     def dq(self) -> np.ndarray:
         """[n_volumes, iters] max |dV|^2 of every volume and iteration of the last run."""
