@@ -399,7 +399,8 @@ def run_ours(args, dist_: Dist) -> None:
     # split form runs two launches per iteration)
     achieved = bpv * vox / iter_s / 1e9
     peaks = measured_peaks()
-    tr = profiled_traffic(args.variant if args.storage == "f32" and k == 3 else None)
+    tr = profiled_traffic((args.variant + ("_fast" if args.arith == "fast" else ""))
+                          if args.storage == "f32" and k == 3 and args.tile_rows == 0 else None)
     traffic = tr["dram_bytes_per_voxel_iter"] * vox if tr else None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
