@@ -705,7 +705,8 @@ def run_batch(args, dist_: Dist) -> None:
             "config": {"workload": "potts_k3_batch48_sides64-256", "volumes": len(specs),
                        "volumes_this_rank": len(mine), "in_mask_voxels": int(vox_all), "k": 3,
                        "lambda_range": [round(min(lams), 3), round(max(lams), 3)], "tau": tau, "iters": iters,
-                       "storage": args.storage, "tile": list(info.tile), "autotuned": bool(autotune),
+                       "storage": args.storage, "arith": args.arith, "tile": list(info.tile),
+                       "persistent": info.persistent, "autotuned": bool(autotune),
                        "autotune_ms": round(info.autotune_ms, 1), "work_items": info.n_work,
                        "graph_launches": info.graph_launches,
                        "parallelism": f"volumes bin-packed over {dist_.world} ranks" if dist_.world > 1 else "single",
@@ -786,16 +787,40 @@ def run_adjoint(args, dist_: Dist) -> None:
             xp, xm = np.float32(x + h), np.float32(x - h)
             return (fun(float(xp)) - fun(float(xm))) / (float(xp) - float(xm))
 
+        def init_flips(c2):
+            # in-mask voxels whose nearest label (the initial state) changes between ci and c2
+            a = np.argmin(np.abs(np.asarray(ci, np.float32)[:, None] - u_in[None]), 0)
+            b = np.argmin(np.abs(np.asarray(c2, np.float32)[:, None] - u_in[None]), 0)
+            return int(np.sum(a != b))
+
         t0 = time.perf_counter()
+        u_in = u_h.reshape(m.n_lines, m.nstride)[:, : m.n_images].reshape(-1)
         rows = []
         for i in range(len(ci)):
             def fc(v, i=i):
                 c2 = list(ci)
                 c2[i] = v
                 return loss64(u_h, c2, lam)
-            g = cd(fc, ci[i], 1e-6)
-            rows.append({"param": f"c{i + 1}", "adjoint": float(gc[i]), "fd": float(g),
-                         "rel": float(abs(gc[i] - g) / abs(g))})
+            # the step starts at 1e-6 relative and shrinks while it would move a voxel's nearest
+            # label (the initial state is piecewise constant in c: that is a jump, not the derivative)
+            def steps(rel):
+                h = rel * abs(ci[i])
+                return float(np.float32(ci[i] + h)), float(np.float32(ci[i] - h))
+
+            rel = 1e-6
+            while True:
+                cp, cm = steps(rel)
+                flips = init_flips([cp if k == i else c for k, c in enumerate(ci)]) + \
+                    init_flips([cm if k == i else c for k, c in enumerate(ci)])
+                if flips == 0:
+                    break
+                nxt = steps(rel / 4.0)
+                if nxt[0] == nxt[1]:  # FP32 cannot take a smaller step: keep this one
+                    break
+                rel /= 4.0
+            g = (fc(cp) - fc(cm)) / (cp - cm)
+            rows.append({"param": f"c{i + 1}", "step": rel, "init_label_flips": flips, "adjoint": float(gc[i]),
+                         "fd": float(g), "rel": float(abs(gc[i] - g) / abs(g))})
         g = cd(lambda v: loss64(u_h, ci, v), lam, 1e-6)
         rows.append({"param": "lambda", "adjoint": float(gl), "fd": float(g), "rel": float(abs(gl - g) / abs(g))})
         gu_h = gu.cpu().numpy()

@@ -11,8 +11,6 @@
 // privatised histograms, so no two runs differ.
 #pragma once
 
-#include <cooperative_groups.h>
-
 #include <cstdint>
 
 #include "geometry.cuh"
@@ -144,6 +142,76 @@ __global__ void __launch_bounds__(kHistThreads) grad_magn_kernel(Geometry g, con
     }
 }
 
+// The same with one warp per line and 16-byte loads and stores (lines of a multiple of 4 values
+// and stride, 16-byte aligned fields): lane l of a pass takes slices 4q .. 4q+3, q = pass * 32 + l,
+// from the line and its four neighbour lines; the in-line neighbours 4q-1 and 4q+4 come from the
+// neighbouring lanes (or a load at the ends of the pass).  Same operations per voxel as
+// grad_magn_kernel, so the same bits.
+__global__ void __launch_bounds__(kHistThreads) grad_magn_vec_kernel(Geometry g, const float *__restrict__ u,
+                                                                     float *__restrict__ v)
+{
+    const int lane = threadIdx.x & 31;
+    constexpr int kWarps = kHistThreads / 32;
+    const int nq = g.ns / 4;
+    for (int64_t L = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5); L < g.n_lines; L += (int64_t)gridDim.x * kWarps) {
+        const LineInfo li = load_line(g, L);
+        const bool inner = (li.flags & kHasNextRow) && (li.flags & kHasPrevRow) && li.next_col >= 0 &&
+                           li.prev_col >= 0;
+        const float4 *c4 = reinterpret_cast<const float4 *>(u + L * g.nstride_w);
+        float4 *o4 = reinterpret_cast<float4 *>(v + L * g.nstride_w);
+        if (!inner) {
+            for (int q = lane; q < nq; q += 32) o4[q] = make_float4(-1.0f, -1.0f, -1.0f, -1.0f);
+            continue;
+        }
+        const float4 *rn = reinterpret_cast<const float4 *>(u + (L + 1) * g.nstride_w);
+        const float4 *rp = reinterpret_cast<const float4 *>(u + (L - 1) * g.nstride_w);
+        const float4 *cn = reinterpret_cast<const float4 *>(u + (int64_t)li.next_col * g.nstride_w);
+        const float4 *cp = reinterpret_cast<const float4 *>(u + (int64_t)li.prev_col * g.nstride_w);
+        const float *line = u + L * g.nstride_w;
+        for (int q0 = 0; q0 < nq; q0 += 32) {
+            const int q = q0 + lane;
+            const bool live = q < nq;
+            float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b = a, c = a, d = a, e = a;
+            if (live) {
+                a = __ldg(c4 + q);
+                b = __ldg(rn + q);
+                c = __ldg(rp + q);
+                d = __ldg(cn + q);
+                e = __ldg(cp + q);
+            }
+            // slice 4q-1 and 4q+4 of the line
+            float before = __shfl_up_sync(0xffffffffu, a.w, 1);
+            float after = __shfl_down_sync(0xffffffffu, a.x, 1);
+            if (live && lane == 0 && q > 0) before = __ldg(line + 4 * q - 1);
+            if (live && (lane == 31 || q + 1 >= nq) && 4 * q + 4 < g.ns) after = __ldg(line + 4 * q + 4);
+            if (!live) continue;
+            const float xs[6] = {before, a.x, a.y, a.z, a.w, after};
+            const float rnv[4] = {b.x, b.y, b.z, b.w}, rpv[4] = {c.x, c.y, c.z, c.w};
+            const float cnv[4] = {d.x, d.y, d.z, d.w}, cpv[4] = {e.x, e.y, e.z, e.w};
+            float r[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int n = 4 * q + j;
+                r[j] = -1.0f;
+                if (n > 0 && n + 1 < g.ns) {
+                    float q1 = 0.0f, q2 = 0.0f, q3 = 0.0f;
+                    q1 += xs[j + 2];
+                    q2 += rnv[j];
+                    q3 += cnv[j];
+                    q1 -= xs[j];
+                    q2 -= rpv[j];
+                    q3 -= cpv[j];
+                    float s = q1 * q1;
+                    s = fmaf(q2, q2, s);
+                    s = fmaf(q3, q3, s);
+                    r[j] = 0.5f * __fsqrt_rn(s);
+                }
+            }
+            o4[q] = make_float4(r[0], r[1], r[2], r[3]);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Histogram bins (calc_hist.cpp:62-66, uv-hist-kernel.cpp:139-149): t = (x - start) / (end -
 // start), bin = round(nb t - 0.5) (the multiply-add contracted as the reference's clang build
@@ -176,46 +244,110 @@ __device__ __forceinline__ float hist_jitter(uint64_t seed, uint64_t idx, float 
     return __fadd_rn(-0.5f * delta, __fmul_rn(delta, u01));
 }
 
-// Adds 1 to counter `id` (>= 0) for every lane whose id it is, one atomic per distinct id of the
-// warp (lanes of a line often share a bin).  add(ptr_of(id), count) does the atomic.
+// Adds 1 to counter `id` (>= 0) for every lane whose id it is.  The lanes that share the first
+// active lane's id add together with one atomic (a warp inside one bin, the common case of a
+// concentrated histogram), every other lane adds its own 1.  A shuffle and two ballots: grouping
+// every distinct id (match.any) cost more than it saved on spread intensities, where a warp's
+// ids are mostly distinct.  add(id, count) does the atomic.
 template <typename Add>
 __device__ __forceinline__ void warp_count(int id, Add add)
 {
     const unsigned active = __ballot_sync(0xffffffffu, id >= 0);
+    if (active == 0u) return;
+    const int leader = __ffs(active) - 1;
+    const int first = __shfl_sync(0xffffffffu, id, leader);
+    const unsigned same = __ballot_sync(0xffffffffu, id == first);
     if (id < 0) return;
-    const unsigned same = __match_any_sync(active, id);
-    if ((threadIdx.x & 31) == __ffs(same) - 1) add(id, (uint32_t)__popc(same));
+    if (id != first)
+        add(id, 1u);
+    else if ((int)(threadIdx.x & 31) == leader)
+        add(first, (uint32_t)__popc(same));
 }
 
-// 1-D histogram (calc_hist.cpp:23-80) into a shared-memory copy per block, flushed with one
-// global atomic per non-zero bin.  nb * 4 bytes of dynamic shared memory.
-template <bool kJitter>
-__global__ void __launch_bounds__(kHistThreads) hist1d_kernel(Geometry g, const float *__restrict__ f, float rs,
-                                                              float re, int nb, float delta, uint64_t seed,
-                                                              uint32_t *__restrict__ ghist)
+// Eight values of one line for one lane of a warp that walks the line in steps of 256 values
+// (slices base .. base+255): with kVec two 16-byte loads (quads base/4 + lane and + 32; lines of
+// a multiple of 4 values and stride, 16-byte aligned field), else eight coalesced 4-byte loads
+// (slices base + lane + 32 j).  Bit j of the result: value j exists.  Several loads in flight
+// per lane keep enough bytes moving to cover the memory latency.
+template <bool kVec>
+__device__ __forceinline__ unsigned load8(const float *__restrict__ line, int ns, int base, int lane, float (&x)[8])
 {
-    extern __shared__ uint32_t sh_hist[];
-    for (int i = threadIdx.x; i < nb; i += blockDim.x) sh_hist[i] = 0u;
+    unsigned valid = 0u;
+    if constexpr (kVec) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int q = (base >> 2) + lane + 32 * h;
+            if (4 * q < ns) {
+                const float4 t = __ldg(reinterpret_cast<const float4 *>(line) + q);
+                x[4 * h] = t.x, x[4 * h + 1] = t.y, x[4 * h + 2] = t.z, x[4 * h + 3] = t.w;
+                valid |= 0xfu << (4 * h);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int n = base + lane + 32 * j;
+            if (n < ns) {
+                x[j] = __ldg(line + n);
+                valid |= 1u << j;
+            }
+        }
+    }
+    return valid;
+}
+
+// The slice of value j of load8.
+template <bool kVec>
+__device__ __forceinline__ int slice8(int base, int lane, int j)
+{
+    if constexpr (kVec)
+        return 4 * ((base >> 2) + lane + 32 * (j >> 2)) + (j & 3);
+    else
+        return base + lane + 32 * j;
+}
+
+// 1-D histogram (calc_hist.cpp:23-80) into shared-memory copies, flushed with one global atomic
+// per non-zero bin.  `copies` = 1 (one copy per block) or kHistThreads / 32 (one per warp: when a
+// few bins hold most voxels, warps then never contend for the same counter); copies * nb * 4
+// bytes of dynamic shared memory.
+template <bool kJitter, bool kVec>
+__global__ void __launch_bounds__(kHistThreads) hist1d_kernel(Geometry g, const float *__restrict__ f, float rs,
+                                                              float re, int nb, int copies, float delta,
+                                                              uint64_t seed, uint32_t *__restrict__ ghist)
+{
+    extern __shared__ uint32_t sh_all[];
+    for (int i = threadIdx.x; i < nb * copies; i += blockDim.x) sh_all[i] = 0u;
     __syncthreads();
+    uint32_t *sh_hist = sh_all + (copies > 1 ? (int)(threadIdx.x >> 5) * nb : 0);
     const float hd = delta * 0.5f;  // delta / 2, exact
     const float lo = rs - hd;
-    for (int64_t L = blockIdx.x; L < g.n_lines; L += gridDim.x) {
+    const int lane = threadIdx.x & 31;
+    constexpr int kWarps = kHistThreads / 32;
+    // one warp per line
+    for (int64_t L = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5); L < g.n_lines; L += (int64_t)gridDim.x * kWarps) {
         const float *line = f + L * g.nstride_w;
-        // whole warps walk the line so that the warp-level combining sees full warps
-        for (int n0 = 0; n0 < g.ns; n0 += blockDim.x) {
-            const int n = n0 + threadIdx.x;
-            int id = -1;
-            if (n < g.ns) {
-                float x = __ldg(line + n);
-                if (kJitter) x = __fadd_rn(x, hist_jitter(seed, (uint64_t)L * g.ns + n, delta));
-                if (lo <= x && __fadd_rn(x, hd) <= re) id = hist_bin(x, rs, re, nb);
+        for (int base = 0; base < g.ns; base += 256) {
+            float x[8];
+            const unsigned valid = load8<kVec>(line, g.ns, base, lane, x);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                int id = -1;
+                if ((valid >> j) & 1u) {
+                    float xv = x[j];
+                    if (kJitter)
+                        xv = __fadd_rn(xv, hist_jitter(seed, (uint64_t)L * g.ns + slice8<kVec>(base, lane, j), delta));
+                    if (lo <= xv && __fadd_rn(xv, hd) <= re) id = hist_bin(xv, rs, re, nb);
+                }
+                warp_count(id, [&](int b, uint32_t c) { atomicAdd(sh_hist + b, c); });
             }
-            warp_count(id, [&](int b, uint32_t c) { atomicAdd(sh_hist + b, c); });
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < nb; i += blockDim.x)
-        if (sh_hist[i]) atomicAdd(ghist + i, sh_hist[i]);
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        uint32_t t = 0;
+        for (int c = 0; c < copies; ++c) t += sh_all[c * nb + i];
+        if (t) atomicAdd(ghist + i, t);
+    }
 }
 
 // The same with global atomics only (bin counts too large for shared memory).
@@ -253,54 +385,100 @@ __device__ __forceinline__ int uv_bin(float x, float y, const UvRange &r)
     return hist_bin(y, r.vs, r.ve, r.nb) * r.stride + hist_bin(x, r.us, r.ue, r.nb);
 }
 
-// 2-D histogram held in the distributed shared memory of a cluster of kUvCluster blocks:
-// block rank k of the cluster owns bins [k kUvSlice, (k+1) kUvSlice), and every block of the
-// cluster adds into whichever block owns a bin.  Each cluster flushes its non-zero bins to the
-// global histogram once.  1 MB of 32-bit counters: 512 x 512 bins fit.
-constexpr int kUvCluster = 8;
-constexpr int kUvSlice = 32768;   // counters per block (128 KB)
-constexpr int kUvThreads = 1024;  // one block per multiprocessor: as many warps as it holds
-
-__global__ void __cluster_dims__(kUvCluster, 1, 1) __launch_bounds__(kUvThreads, 1)
-    uv_hist_cluster_kernel(Geometry g, const float *__restrict__ u, const float *__restrict__ v, UvRange r,
-                           int total_bins, uint32_t *__restrict__ ghist)
+// Both bins of the pair, or false outside [u_start, u_end] x [v_start, v_end] (as uv_bin).
+__device__ __forceinline__ bool uv_bins(float x, float y, const UvRange &r, int &xb, int &yb)
 {
-    namespace cg = cooperative_groups;
-    cg::cluster_group cluster = cg::this_cluster();
-    extern __shared__ uint32_t sh_uv[];
-    for (int i = threadIdx.x; i < kUvSlice; i += blockDim.x) sh_uv[i] = 0u;
-    cluster.sync();
-    for (int64_t L = blockIdx.x; L < g.n_lines; L += gridDim.x) {
-        const int64_t o0 = L * g.nstride_w;
-        for (int n0 = 0; n0 < g.ns; n0 += blockDim.x) {
-            const int n = n0 + threadIdx.x;
-            int id = -1;
-            if (n < g.ns) id = uv_bin(__ldg(u + o0 + n), __ldg(v + o0 + n), r);
-            warp_count(id, [&](int b, uint32_t c) {
-                uint32_t *dst = cluster.map_shared_rank(sh_uv, (unsigned)(b / kUvSlice));
-                atomicAdd(dst + (b % kUvSlice), c);
-            });
-        }
-    }
-    cluster.sync();
-    const int base = (int)cluster.block_rank() * kUvSlice;
-    for (int i = threadIdx.x; i < kUvSlice && base + i < total_bins; i += blockDim.x)
-        if (sh_uv[i]) atomicAdd(ghist + base + i, sh_uv[i]);
+    if (!(r.us <= x && x <= r.ue && r.vs <= y && y <= r.ve)) return false;
+    xb = hist_bin(x, r.us, r.ue, r.nb);
+    yb = hist_bin(y, r.vs, r.ve, r.nb);
+    return true;
 }
 
-// The same with global atomics only (histograms larger than a cluster's shared memory).
-__global__ void __launch_bounds__(kHistThreads) uv_hist_global_kernel(Geometry g, const float *__restrict__ u,
-                                                                      const float *__restrict__ v, UvRange r,
-                                                                      uint32_t *__restrict__ ghist)
+// The 2-D histogram with its densest bins in every block's own shared memory.  The bins are
+// grouped into coarse cells of 2^cs x 2^cs bins (cdim cells per axis, at most kUvCoarseMax);
+// uv_coarse_kernel counts the cells over a sample of the lines, the host gives the densest
+// cells (up to kUvHotBins bins) a slot, and uv_hist_hot_kernel counts a voxel in its block's
+// slot counters when its cell has one, else with a global atomic.  Counts are exact either
+// way; the choice of cells only changes speed.
+constexpr int kUvCoarseMax = 64;    // coarse cells per axis
+constexpr int kUvHotBins = 32768;   // bins counted in a block's shared memory (128 KB)
+constexpr int kUvThreads = 1024;    // one block per multiprocessor: as many warps as it holds
+
+template <bool kVec>
+__global__ void __launch_bounds__(kHistThreads) uv_coarse_kernel(Geometry g, const float *__restrict__ u,
+                                                                 const float *__restrict__ v, UvRange r, int cs,
+                                                                 int cdim, int step, uint32_t *__restrict__ gcoarse)
 {
-    for (int64_t L = blockIdx.x; L < g.n_lines; L += gridDim.x) {
-        const int64_t o0 = L * g.nstride_w;
-        for (int n0 = 0; n0 < g.ns; n0 += blockDim.x) {
-            const int n = n0 + threadIdx.x;
-            int id = -1;
-            if (n < g.ns) id = uv_bin(__ldg(u + o0 + n), __ldg(v + o0 + n), r);
-            warp_count(id, [&](int b, uint32_t c) { atomicAdd(ghist + b, c); });
+    __shared__ uint32_t sh[kUvCoarseMax * kUvCoarseMax];
+    const int cells = cdim * cdim;
+    for (int i = threadIdx.x; i < cells; i += blockDim.x) sh[i] = 0u;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    constexpr int kWarps = kHistThreads / 32;
+    for (int64_t k = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5); k * step < g.n_lines;
+         k += (int64_t)gridDim.x * kWarps) {
+        const int64_t o0 = k * step * g.nstride_w;
+        for (int base = 0; base < g.ns; base += 256) {
+            float x[8], y[8];
+            const unsigned valid = load8<kVec>(u + o0, g.ns, base, lane, x) & load8<kVec>(v + o0, g.ns, base, lane, y);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                int id = -1, xb, yb;
+                if (((valid >> j) & 1u) && uv_bins(x[j], y[j], r, xb, yb)) id = (yb >> cs) * cdim + (xb >> cs);
+                warp_count(id, [&](int b, uint32_t c) { atomicAdd(sh + b, c); });
+            }
         }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < cells; i += blockDim.x)
+        if (sh[i]) atomicAdd(gcoarse + i, sh[i]);
+}
+
+// Dynamic shared memory: n_slots << 2cs counters, then the cell -> slot table (cdim^2 int16).
+template <bool kVec>
+__global__ void __launch_bounds__(kUvThreads, 1)
+    uv_hist_hot_kernel(Geometry g, const float *__restrict__ u, const float *__restrict__ v, UvRange r, int cs,
+                       int cdim, const int16_t *__restrict__ table, const int16_t *__restrict__ slot_cell,
+                       int n_slots, uint32_t *__restrict__ ghist)
+{
+    extern __shared__ uint32_t sh_hot[];
+    const int n_hot = n_slots << (2 * cs);
+    int16_t *stab = reinterpret_cast<int16_t *>(sh_hot + n_hot);
+    for (int i = threadIdx.x; i < n_hot; i += blockDim.x) sh_hot[i] = 0u;
+    for (int i = threadIdx.x; i < cdim * cdim; i += blockDim.x) stab[i] = table[i];
+    __syncthreads();
+    const int mask = (1 << cs) - 1;
+    const int lane = threadIdx.x & 31;
+    constexpr int kWarps = kUvThreads / 32;
+    // one warp per line
+    for (int64_t L = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5); L < g.n_lines; L += (int64_t)gridDim.x * kWarps) {
+        const int64_t o0 = L * g.nstride_w;
+        for (int base = 0; base < g.ns; base += 256) {
+            float x[8], y[8];
+            const unsigned valid = load8<kVec>(u + o0, g.ns, base, lane, x) & load8<kVec>(v + o0, g.ns, base, lane, y);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                int lid = -1, gid = -1, xb, yb;
+                if (((valid >> j) & 1u) && uv_bins(x[j], y[j], r, xb, yb)) {
+                    const int slot = stab[(yb >> cs) * cdim + (xb >> cs)];
+                    if (slot >= 0)
+                        lid = (slot << (2 * cs)) | ((yb & mask) << cs) | (xb & mask);
+                    else
+                        gid = yb * r.stride + xb;
+                }
+                warp_count(lid, [&](int b, uint32_t c) { atomicAdd(sh_hot + b, c); });
+                warp_count(gid, [&](int b, uint32_t c) { atomicAdd(ghist + b, c); });
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n_hot; i += blockDim.x) {
+        const uint32_t c = sh_hot[i];
+        if (!c) continue;
+        const int cell = slot_cell[i >> (2 * cs)];
+        const int yb = ((cell / cdim) << cs) | ((i >> cs) & mask);
+        const int xb = ((cell % cdim) << cs) | (i & mask);
+        atomicAdd(ghist + yb * r.stride + xb, c);
     }
 }
 

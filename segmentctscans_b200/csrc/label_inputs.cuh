@@ -27,6 +27,12 @@ unsigned field_blocks(const potts_context *ctx, int64_t n_lines, int per_sm)
 
 bool field_empty(const Geometry &g) { return g.n_lines == 0 || g.ns == 0; }
 
+// 16-byte loads along a line: lines of a multiple of 4 values and stride, aligned field.
+bool field_vec(const Geometry &g, const float *d_f)
+{
+    return ((uintptr_t)d_f & 15u) == 0 && g.ns % 4 == 0 && g.nstride_w % 4 == 0;
+}
+
 // min_max (min_max/min_max.cpp:56-81) and, with positive, the min/max of the strictly positive
 // values (uv-hist-kernel.cpp:70-92).  FLT_MAX / -FLT_MAX when there is no such value.
 int minmax_run(potts_context *ctx, const float *d_f, bool positive, float *out_min, float *out_max)
@@ -63,13 +69,19 @@ int grad_magn_run(potts_context *ctx, const float *d_u, float *d_v)
 {
     const Geometry g = field_geometry(ctx);
     if (field_empty(g)) return POTTS_OK;
-    potts::grad_magn_kernel<<<field_blocks(ctx, g.n_lines, 8), potts::kHistThreads, 0, ctx->stream>>>(g, d_u, d_v);
+    if (field_vec(g, d_u) && field_vec(g, d_v))  // one warp per line
+        potts::grad_magn_vec_kernel<<<field_blocks(ctx, (g.n_lines + 7) / 8, 8), potts::kHistThreads, 0,
+                                      ctx->stream>>>(g, d_u, d_v);
+    else
+        potts::grad_magn_kernel<<<field_blocks(ctx, g.n_lines, 8), potts::kHistThreads, 0, ctx->stream>>>(g, d_u,
+                                                                                                         d_v);
     ctx->total_launches += 1;
     POTTS_CUDA(cudaGetLastError());
     return POTTS_OK;
 }
 
 constexpr int kHist1dSharedMax = 50 * 1024;  // bins kept in shared memory (200 KB)
+constexpr int kHist1dPerWarpMax = 100 * 1024;  // shared bytes of per-warp copies (two blocks per SM)
 
 // calc_hist (calc_hist/calc_hist.cpp:93-138): counts of nb bins over [rs, re] to the host.
 int hist1d_run(potts_context *ctx, const float *d_f, float rs, float re, int nb, float delta, uint64_t seed,
@@ -82,20 +94,24 @@ int hist1d_run(potts_context *ctx, const float *d_f, float rs, float re, int nb,
     if (!field_empty(g)) {
         const bool jitter = delta != 0.0f;
         if (nb <= kHist1dSharedMax) {
-            const int smem = (int)sizeof(uint32_t) * nb;
+            // a copy per warp while the copies fit 100 KB (at most 3200 bins), else one per block
+            const int warps = potts::kHistThreads / 32;
+            const int copies = (size_t)sizeof(uint32_t) * nb * warps <= (size_t)kHist1dPerWarpMax ? warps : 1;
+            const int smem = (int)sizeof(uint32_t) * nb * copies;
             const int per_sm = std::max(1, std::min(8, (200 * 1024) / std::max(smem, 1)));
-            const unsigned blocks = field_blocks(ctx, g.n_lines, per_sm);
-            if (jitter) {
-                POTTS_CUDA(cudaFuncSetAttribute(potts::hist1d_kernel<true>,
-                                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-                potts::hist1d_kernel<true><<<blocks, potts::kHistThreads, smem, ctx->stream>>>(g, d_f, rs, re, nb,
-                                                                                             delta, seed, d_counts);
-            } else {
-                POTTS_CUDA(cudaFuncSetAttribute(potts::hist1d_kernel<false>,
-                                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-                potts::hist1d_kernel<false><<<blocks, potts::kHistThreads, smem, ctx->stream>>>(g, d_f, rs, re, nb,
-                                                                                              delta, seed, d_counts);
-            }
+            // one warp per line
+            const unsigned blocks = field_blocks(ctx, (g.n_lines + 7) / 8, per_sm);
+            const bool vec = field_vec(g, d_f);
+            auto launch = [&](auto kern) -> int {
+                POTTS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+                kern<<<blocks, potts::kHistThreads, smem, ctx->stream>>>(g, d_f, rs, re, nb, copies, delta, seed,
+                                                                         d_counts);
+                return POTTS_OK;
+            };
+            if (jitter)
+                POTTS_TRY(vec ? launch(potts::hist1d_kernel<true, true>) : launch(potts::hist1d_kernel<true, false>));
+            else
+                POTTS_TRY(vec ? launch(potts::hist1d_kernel<false, true>) : launch(potts::hist1d_kernel<false, false>));
         } else {
             const unsigned blocks = field_blocks(ctx, g.n_lines, 8);
             if (jitter)
@@ -117,6 +133,63 @@ int hist1d_run(potts_context *ctx, const float *d_f, float rs, float re, int nb,
 uint32_t uv_stride(int nb) { return (uint32_t)((nb + 31) / 32 * 32); }
 uint64_t uv_span(int nb) { return (uint64_t)(nb - 1) * uv_stride(nb) + (uint64_t)nb; }
 
+// The 2-D histogram through the hot-cell kernels (kernels_hist.cuh): a coarse pass over every
+// 8th line, the densest cells to shared memory, the rest to global atomics.
+int uv_hist_hot(potts_context *ctx, const Geometry &g, const float *d_u, const float *d_v, const potts::UvRange &r,
+                uint32_t *d_hist)
+{
+    int cs = 0;
+    while (((r.nb + (1 << cs) - 1) >> cs) > potts::kUvCoarseMax) ++cs;
+    const int cdim = (r.nb + (1 << cs) - 1) >> cs;
+    const int cells = cdim * cdim;
+    const int n_slots = std::min(cells, potts::kUvHotBins >> (2 * cs));
+    // device: coarse counts (cells uint32), cell -> slot table (cells int16), slot -> cell (n_slots int16)
+    const size_t bytes = sizeof(uint32_t) * cells + sizeof(int16_t) * (cells + n_slots) + 16;
+    POTTS_TRY(ensure(ctx, ctx->hist_aux, bytes));
+    uint32_t *d_coarse = static_cast<uint32_t *>(ctx->hist_aux.p);
+    int16_t *d_table = reinterpret_cast<int16_t *>(d_coarse + cells);
+    int16_t *d_cells = d_table + cells;
+    POTTS_CUDA(cudaMemsetAsync(d_coarse, 0, sizeof(uint32_t) * cells, ctx->stream));
+    constexpr int kSampleStep = 8;
+    const bool vec = field_vec(g, d_u) && field_vec(g, d_v);
+    const unsigned cblocks = field_blocks(ctx, ((g.n_lines + kSampleStep - 1) / kSampleStep + 7) / 8, 8);
+    if (vec)
+        potts::uv_coarse_kernel<true><<<cblocks, potts::kHistThreads, 0, ctx->stream>>>(g, d_u, d_v, r, cs, cdim,
+                                                                                       kSampleStep, d_coarse);
+    else
+        potts::uv_coarse_kernel<false><<<cblocks, potts::kHistThreads, 0, ctx->stream>>>(g, d_u, d_v, r, cs, cdim,
+                                                                                        kSampleStep, d_coarse);
+    ctx->total_launches += 1;
+    POTTS_CUDA(cudaGetLastError());
+    std::vector<uint32_t> counts((size_t)cells);
+    POTTS_CUDA(cudaMemcpyAsync(counts.data(), d_coarse, sizeof(uint32_t) * cells, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+    POTTS_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::vector<int> order((size_t)cells);
+    for (int i = 0; i < cells; ++i) order[(size_t)i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return counts[(size_t)a] > counts[(size_t)b]; });
+    std::vector<int16_t> table((size_t)cells, (int16_t)-1), slot_cell((size_t)std::max(n_slots, 1), (int16_t)0);
+    for (int s = 0; s < n_slots; ++s) {
+        table[(size_t)order[(size_t)s]] = (int16_t)s;
+        slot_cell[(size_t)s] = (int16_t)order[(size_t)s];
+    }
+    POTTS_CUDA(cudaMemcpyAsync(d_table, table.data(), sizeof(int16_t) * cells, cudaMemcpyHostToDevice, ctx->stream));
+    POTTS_CUDA(cudaMemcpyAsync(d_cells, slot_cell.data(), sizeof(int16_t) * n_slots, cudaMemcpyHostToDevice,
+                               ctx->stream));
+    const int smem = (int)(sizeof(uint32_t) * ((size_t)n_slots << (2 * cs)) + sizeof(int16_t) * cells);
+    auto hot = vec ? potts::uv_hist_hot_kernel<true> : potts::uv_hist_hot_kernel<false>;
+    POTTS_CUDA(cudaFuncSetAttribute(hot, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const unsigned hblocks = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>(std::max(ctx->n_sm, 1), (g.n_lines + potts::kUvThreads / 32 - 1) / (potts::kUvThreads / 32)));
+    hot<<<hblocks, potts::kUvThreads, smem, ctx->stream>>>(g, d_u, d_v, r, cs, cdim, d_table, d_cells, n_slots,
+                                                           d_hist);
+    ctx->total_launches += 1;
+    POTTS_CUDA(cudaGetLastError());
+    // the host vectors above are pageable: wait for the copies before they go out of scope
+    POTTS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return POTTS_OK;
+}
+
 // uv_hist (uv-hist-kernel.cpp:100-197): the 2-D histogram of (u, v) to the host.
 int uv_hist_run(potts_context *ctx, const float *d_u, const float *d_v, const potts::UvRange &r, uint32_t *h_hist)
 {
@@ -125,33 +198,7 @@ int uv_hist_run(potts_context *ctx, const float *d_u, const float *d_v, const po
     POTTS_TRY(ensure(ctx, ctx->hist, sizeof(uint32_t) * span));
     uint32_t *d_hist = static_cast<uint32_t *>(ctx->hist.p);
     POTTS_CUDA(cudaMemsetAsync(d_hist, 0, sizeof(uint32_t) * span, ctx->stream));
-    if (!field_empty(g)) {
-        if (span <= (uint64_t)potts::kUvCluster * potts::kUvSlice) {
-            const int smem = (int)sizeof(uint32_t) * potts::kUvSlice;
-            POTTS_CUDA(cudaFuncSetAttribute(potts::uv_hist_cluster_kernel,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            // one block per multiprocessor: as many whole clusters as fit at once
-            cudaLaunchConfig_t cfg{};
-            cfg.gridDim = dim3((unsigned)(std::max(ctx->n_sm, 1) / potts::kUvCluster * potts::kUvCluster));
-            cfg.blockDim = dim3(potts::kUvThreads);
-            cfg.dynamicSmemBytes = (size_t)smem;
-            cfg.stream = ctx->stream;
-            int clusters = 0;
-            if (cudaOccupancyMaxActiveClusters(&clusters, (void *)potts::uv_hist_cluster_kernel, &cfg) != cudaSuccess ||
-                clusters < 1) {
-                cudaGetLastError();
-                clusters = 1;
-            }
-            const unsigned blocks = (unsigned)(clusters * potts::kUvCluster);
-            potts::uv_hist_cluster_kernel<<<blocks, potts::kUvThreads, smem, ctx->stream>>>(g, d_u, d_v, r, (int)span,
-                                                                                           d_hist);
-        } else {
-            potts::uv_hist_global_kernel<<<field_blocks(ctx, g.n_lines, 8), potts::kHistThreads, 0, ctx->stream>>>(
-                g, d_u, d_v, r, d_hist);
-        }
-        ctx->total_launches += 1;
-        POTTS_CUDA(cudaGetLastError());
-    }
+    if (!field_empty(g)) POTTS_TRY(uv_hist_hot(ctx, g, d_u, d_v, r, d_hist));
     POTTS_CUDA(cudaMemcpyAsync(h_hist, d_hist, sizeof(uint32_t) * span, cudaMemcpyDeviceToHost, ctx->stream));
     POTTS_CUDA(cudaStreamSynchronize(ctx->stream));
     return POTTS_OK;

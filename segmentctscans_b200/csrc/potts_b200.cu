@@ -204,7 +204,8 @@ struct potts_context {
     MappingCopy mapping;  // last mapping whose line table is on the device
     bool mapping_valid = false;
     DevBuf lines, state, dq, energy, partial, host_u, host_res, host_labels, ustage, err;
-    DevBuf hist;  // min/max partials and histogram counters of the label-finding inputs
+    DevBuf hist;      // min/max partials and histogram counters of the label-finding inputs
+    DevBuf hist_aux;  // coarse cell counts and cell tables of the 2-D histogram
     DevBuf io, io_tables;  // archive payload / raw label box staging, mask tables of the box kernel
     float *pinned_dq = nullptr;
     // tiled-kernel tables: per column (depends on the mapping) and the work
@@ -1235,7 +1236,7 @@ void potts_context_destroy(potts_context *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (DevBuf *b : {&ctx->lines, &ctx->state, &ctx->dq, &ctx->energy, &ctx->partial, &ctx->host_u,
                       &ctx->host_res, &ctx->host_labels, &ctx->ustage, &ctx->err, &ctx->cols, &ctx->work, &ctx->vols,
-                      &ctx->hist, &ctx->io, &ctx->io_tables, &ctx->pctl})
+                      &ctx->hist, &ctx->hist_aux, &ctx->io, &ctx->io_tables, &ctx->pctl})
         if (b->p) cudaFree(b->p);
     if (ctx->pinned_dq) cudaFreeHost(ctx->pinned_dq);
     for (cudaEvent_t e : ctx->seg_ev) cudaEventDestroy(e);

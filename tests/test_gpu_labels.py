@@ -57,7 +57,7 @@ def test_calc_hist_bitwise(cuda_device, oracle_mod, nb, jitter):
     np.testing.assert_allclose(dens, counts / (m.data_size * bw), rtol=1e-15)
 
 
-@pytest.mark.parametrize("nb", [512, 7, 1, 600], ids=["512-cluster", "7", "1", "600-global"])
+@pytest.mark.parametrize("nb", [512, 7, 1, 600])
 def test_uv_hist_bitwise(cuda_device, oracle_mod, nb):
     m, u, _, _ = phantom_volume(48, 21.0, seed=5, radius_range=(3.0, 8.0))
     with potts.make_context(0) as ctx:
@@ -78,6 +78,24 @@ def test_uv_hist_bitwise(cuda_device, oracle_mod, nb):
     assert np.array_equal(h2, oracle_mod.uv_hist(m, u, v, 0.2, 0.8, 0.0, 0.05, nb))
     mat = potts.uv_hist_matrix(h, nb)
     assert mat.shape == (nb, nb) and int(mat.sum()) == int(h.sum())
+
+
+@pytest.mark.parametrize("nb", [512, 129, 1000, 64])
+def test_uv_hist_spread_values(cuda_device, oracle_mod, nb):
+    """Uniform values spread the counts over every coarse cell, so the cells held in shared memory
+    take only part of them and the rest go to global counters; nb = 129 and 1000 leave the last
+    coarse cells partly outside the histogram."""
+    m, _, _ = random_volume(70, 40, 38, 18.1, 3, seed=9)
+    rng = np.random.default_rng(nb)
+    u = rng.uniform(0.0, 1.0, m.span).astype(np.float32)
+    v = rng.uniform(0.0, 1.0, m.span).astype(np.float32)
+    with potts.make_context(0) as ctx:
+        du, dv = _dev(ctx, m, u), _dev(ctx, m, v)
+        h = potts.uv_hist(ctx, m, du.data_ptr(), dv.data_ptr(), 0.05, 0.95, 0.1, 0.9, nb)
+        for f in (du, dv):
+            f.free()
+    ref = oracle_mod.uv_hist(m, u, v, 0.05, 0.95, 0.1, 0.9, nb)
+    assert np.array_equal(h, ref) and int(h.sum()) > 0
 
 
 def test_empty_range_and_constant_field(cuda_device, oracle_mod):
