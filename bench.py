@@ -807,19 +807,31 @@ def run_adjoint(args, dist_: Dist) -> None:
                 h = rel * abs(ci[i])
                 return float(np.float32(ci[i] + h)), float(np.float32(ci[i] - h))
 
-            rel = 1e-6
+            # central where neither side moves a nearest label, else one-sided on the side that moves
+            # none (a voxel within FP32 spacing of a tie makes every central step a jump)
+            rel, kind = 1e-6, "central"
             while True:
                 cp, cm = steps(rel)
-                flips = init_flips([cp if k == i else c for k, c in enumerate(ci)]) + \
-                    init_flips([cm if k == i else c for k, c in enumerate(ci)])
-                if flips == 0:
+                fp = init_flips([cp if k == i else c for k, c in enumerate(ci)])
+                fm = init_flips([cm if k == i else c for k, c in enumerate(ci)])
+                if fp + fm == 0:
+                    g = (fc(cp) - fc(cm)) / (cp - cm)
                     break
                 nxt = steps(rel / 4.0)
-                if nxt[0] == nxt[1]:  # FP32 cannot take a smaller step: keep this one
+                if nxt[0] == nxt[1]:  # FP32 cannot take a smaller step
+                    cp, cm = steps(1e-6)
+                    fp = init_flips([cp if k == i else c for k, c in enumerate(ci)])
+                    fm = init_flips([cm if k == i else c for k, c in enumerate(ci)])
+                    rel = 1e-6
+                    if fp == 0:
+                        kind, g = "forward", (fc(cp) - fc(ci[i])) / (cp - ci[i])
+                    elif fm == 0:
+                        kind, g = "backward", (fc(ci[i]) - fc(cm)) / (ci[i] - cm)
+                    else:
+                        kind, g = "central (jumps on both sides)", (fc(cp) - fc(cm)) / (cp - cm)
                     break
                 rel /= 4.0
-            g = (fc(cp) - fc(cm)) / (cp - cm)
-            rows.append({"param": f"c{i + 1}", "step": rel, "init_label_flips": flips, "adjoint": float(gc[i]),
+            rows.append({"param": f"c{i + 1}", "step": rel, "difference": kind, "adjoint": float(gc[i]),
                          "fd": float(g), "rel": float(abs(gc[i] - g) / abs(g))})
         g = cd(lambda v: loss64(u_h, ci, v), lam, 1e-6)
         rows.append({"param": "lambda", "adjoint": float(gl), "fd": float(g), "rel": float(abs(gl - g) / abs(g))})
