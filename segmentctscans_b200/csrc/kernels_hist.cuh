@@ -227,6 +227,27 @@ __device__ __forceinline__ int hist_bin(float x, float start, float end, int nb)
     return (int)r;
 }
 
+// hist_bin without its division where that cannot change the bin.  rinv = __frcp_rn(end - start),
+// the correctly rounded reciprocal.  For |t| <= 1 the product RN((x - start) rinv) differs from
+// the quotient t = RN((x - start) / (end - start)) by at most 1.5 ulp(1) (relative errors of
+// 2^-24 in rinv, in the product and in t), so y' = fma(nb, product, -0.5) differs from
+// hist_bin's fma(nb, t, -0.5) by less than nb 4.2e-7.  The bin is round(y) (halves away from
+// zero, then clamped), which can only differ between y and y' when y' lies within that distance
+// of a half-integer: then, and for a non-finite y', the division decides.  The bins are the same
+// as hist_bin's for every input (one division in about 2 nb 1e-6 of the cases).
+__device__ __forceinline__ int hist_bin_r(float x, float start, float end, float rinv, int nb)
+{
+    const float y = fmaf((float)nb, __fmul_rn(__fsub_rn(x, start), rinv), -0.5f);
+    const float f = y - floorf(y);
+    if (fabsf(f - 0.5f) > fmaf((float)nb, 1e-6f, 1e-6f)) {  // false for a NaN or infinite y
+        const float r = roundf(y);
+        if (!(r >= 0.0f)) return 0;
+        if (r >= (float)(nb - 1)) return nb - 1;
+        return (int)r;
+    }
+    return hist_bin(x, start, end, nb);
+}
+
 // Jitter of voxel `idx` (in-mask index L * n_images + n) for calc_hist's smoothing: uniform in
 // [-delta/2, delta/2) from SplitMix64 (Steele, Lea and Flood, 2014; public domain) of
 // (seed, idx).  The reference draws from a randomly seeded Philox stream, so its jittered
@@ -321,6 +342,7 @@ __global__ void __launch_bounds__(kHistThreads) hist1d_kernel(Geometry g, const 
     uint32_t *sh_hist = sh_all + (copies > 1 ? (int)(threadIdx.x >> 5) * nb : 0);
     const float hd = delta * 0.5f;  // delta / 2, exact
     const float lo = rs - hd;
+    const float rinv = __frcp_rn(__fsub_rn(re, rs));
     const int lane = threadIdx.x & 31;
     constexpr int kWarps = kHistThreads / 32;
     // one warp per line
@@ -336,7 +358,7 @@ __global__ void __launch_bounds__(kHistThreads) hist1d_kernel(Geometry g, const 
                     float xv = x[j];
                     if (kJitter)
                         xv = __fadd_rn(xv, hist_jitter(seed, (uint64_t)L * g.ns + slice8<kVec>(base, lane, j), delta));
-                    if (lo <= xv && __fadd_rn(xv, hd) <= re) id = hist_bin(xv, rs, re, nb);
+                    if (lo <= xv && __fadd_rn(xv, hd) <= re) id = hist_bin_r(xv, rs, re, rinv, nb);
                 }
                 warp_count(id, [&](int b, uint32_t c) { atomicAdd(sh_hist + b, c); });
             }
@@ -373,24 +395,20 @@ __global__ void __launch_bounds__(kHistThreads) hist1d_global_kernel(Geometry g,
     }
 }
 
-// Bin of the pair (x = u, y = grad magnitude) in the 2-D histogram (uv-hist-kernel.cpp:133-150):
-// ybin * stride + xbin, or -1 outside [u_start, u_end] x [v_start, v_end].
+// Ranges and layout of the 2-D histogram (uv-hist-kernel.cpp:133-150): the pair (x = u, y = grad
+// magnitude) counts at ybin * stride + xbin when it lies in [u_start, u_end] x [v_start, v_end].
 struct UvRange {
     float us, ue, vs, ve;
     int nb, stride;
 };
-__device__ __forceinline__ int uv_bin(float x, float y, const UvRange &r)
-{
-    if (!(r.us <= x && x <= r.ue && r.vs <= y && y <= r.ve)) return -1;
-    return hist_bin(y, r.vs, r.ve, r.nb) * r.stride + hist_bin(x, r.us, r.ue, r.nb);
-}
 
-// Both bins of the pair, or false outside [u_start, u_end] x [v_start, v_end] (as uv_bin).
-__device__ __forceinline__ bool uv_bins(float x, float y, const UvRange &r, int &xb, int &yb)
+// Both bins of the pair, or false outside the ranges.  ru / rv: __frcp_rn(ue - us) and
+// __frcp_rn(ve - vs) (hist_bin_r).
+__device__ __forceinline__ bool uv_bins(float x, float y, const UvRange &r, float ru, float rv, int &xb, int &yb)
 {
     if (!(r.us <= x && x <= r.ue && r.vs <= y && y <= r.ve)) return false;
-    xb = hist_bin(x, r.us, r.ue, r.nb);
-    yb = hist_bin(y, r.vs, r.ve, r.nb);
+    xb = hist_bin_r(x, r.us, r.ue, ru, r.nb);
+    yb = hist_bin_r(y, r.vs, r.ve, rv, r.nb);
     return true;
 }
 
@@ -413,6 +431,7 @@ __global__ void __launch_bounds__(kHistThreads) uv_coarse_kernel(Geometry g, con
     const int cells = cdim * cdim;
     for (int i = threadIdx.x; i < cells; i += blockDim.x) sh[i] = 0u;
     __syncthreads();
+    const float ru = __frcp_rn(__fsub_rn(r.ue, r.us)), rv = __frcp_rn(__fsub_rn(r.ve, r.vs));
     const int lane = threadIdx.x & 31;
     constexpr int kWarps = kHistThreads / 32;
     for (int64_t k = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5); k * step < g.n_lines;
@@ -424,7 +443,7 @@ __global__ void __launch_bounds__(kHistThreads) uv_coarse_kernel(Geometry g, con
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
                 int id = -1, xb, yb;
-                if (((valid >> j) & 1u) && uv_bins(x[j], y[j], r, xb, yb)) id = (yb >> cs) * cdim + (xb >> cs);
+                if (((valid >> j) & 1u) && uv_bins(x[j], y[j], r, ru, rv, xb, yb)) id = (yb >> cs) * cdim + (xb >> cs);
                 warp_count(id, [&](int b, uint32_t c) { atomicAdd(sh + b, c); });
             }
         }
@@ -448,6 +467,7 @@ __global__ void __launch_bounds__(kUvThreads, 1)
     for (int i = threadIdx.x; i < cdim * cdim; i += blockDim.x) stab[i] = table[i];
     __syncthreads();
     const int mask = (1 << cs) - 1;
+    const float ru = __frcp_rn(__fsub_rn(r.ue, r.us)), rv = __frcp_rn(__fsub_rn(r.ve, r.vs));
     const int lane = threadIdx.x & 31;
     constexpr int kWarps = kUvThreads / 32;
     // one warp per line
@@ -459,7 +479,7 @@ __global__ void __launch_bounds__(kUvThreads, 1)
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
                 int lid = -1, gid = -1, xb, yb;
-                if (((valid >> j) & 1u) && uv_bins(x[j], y[j], r, xb, yb)) {
+                if (((valid >> j) & 1u) && uv_bins(x[j], y[j], r, ru, rv, xb, yb)) {
                     const int slot = stab[(yb >> cs) * cdim + (xb >> cs)];
                     if (slot >= 0)
                         lid = (slot << (2 * cs)) | ((yb & mask) << cs) | (xb & mask);
