@@ -234,13 +234,16 @@ __device__ __forceinline__ int hist_bin(float x, float start, float end, int nb)
 // hist_bin's fma(nb, t, -0.5) by less than nb 4.2e-7.  The bin is round(y) (halves away from
 // zero, then clamped), which can only differ between y and y' when y' lies within that distance
 // of a half-integer: then, and for a non-finite y', the division decides.  The bins are the same
-// as hist_bin's for every input (one division in about 2 nb 1e-6 of the cases).
+// as hist_bin's for every input (one division in about 2 nb 1e-6 of the cases).  Away from a
+// half-integer, round(y) is the nearer of floor(y) and floor(y) + 1, which the fraction
+// f = y - floor(y) (exact for every finite y) picks: f > 1/2 rounds up.
 __device__ __forceinline__ int hist_bin_r(float x, float start, float end, float rinv, int nb)
 {
     const float y = fmaf((float)nb, __fmul_rn(__fsub_rn(x, start), rinv), -0.5f);
-    const float f = y - floorf(y);
-    if (fabsf(f - 0.5f) > fmaf((float)nb, 1e-6f, 1e-6f)) {  // false for a NaN or infinite y
-        const float r = roundf(y);
+    const float fl = floorf(y);
+    const float f = __fsub_rn(y, fl);
+    if (fabsf(__fsub_rn(f, 0.5f)) > fmaf((float)nb, 1e-6f, 1e-6f)) {  // false for a NaN or infinite y
+        const float r = f > 0.5f ? __fadd_rn(fl, 1.0f) : fl;  // f > 1/2 only where |y| < 2^23: exact
         if (!(r >= 0.0f)) return 0;
         if (r >= (float)(nb - 1)) return nb - 1;
         return (int)r;
@@ -269,20 +272,19 @@ __device__ __forceinline__ float hist_jitter(uint64_t seed, uint64_t idx, float 
 // active lane's id add together with one atomic (a warp inside one bin, the common case of a
 // concentrated histogram), every other lane adds its own 1.  A shuffle and two ballots: grouping
 // every distinct id (match.any) cost more than it saved on spread intensities, where a warp's
-// ids are mostly distinct.  add(id, count) does the atomic.
+// ids are mostly distinct.  add(id, count) does the atomic; every lane that adds reaches the
+// same call, so the warp issues it once.  kNoBin (and -1 converted): the lane adds nothing.
+constexpr uint32_t kNoBin = 0xffffffffu;
 template <typename Add>
-__device__ __forceinline__ void warp_count(int id, Add add)
+__device__ __forceinline__ void warp_count(uint32_t id, Add add)
 {
-    const unsigned active = __ballot_sync(0xffffffffu, id >= 0);
+    const unsigned active = __ballot_sync(0xffffffffu, id != kNoBin);
     if (active == 0u) return;
     const int leader = __ffs(active) - 1;
-    const int first = __shfl_sync(0xffffffffu, id, leader);
+    const uint32_t first = __shfl_sync(0xffffffffu, id, leader);
     const unsigned same = __ballot_sync(0xffffffffu, id == first);
-    if (id < 0) return;
-    if (id != first)
-        add(id, 1u);
-    else if ((int)(threadIdx.x & 31) == leader)
-        add(first, (uint32_t)__popc(same));
+    const bool other = id != first;
+    if (id != kNoBin && (other || (int)(threadIdx.x & 31) == leader)) add(id, other ? 1u : (uint32_t)__popc(same));
 }
 
 // Eight values of one line for one lane of a warp that walks the line in steps of 256 values
@@ -360,7 +362,7 @@ __global__ void __launch_bounds__(kHistThreads) hist1d_kernel(Geometry g, const 
                         xv = __fadd_rn(xv, hist_jitter(seed, (uint64_t)L * g.ns + slice8<kVec>(base, lane, j), delta));
                     if (lo <= xv && __fadd_rn(xv, hd) <= re) id = hist_bin_r(xv, rs, re, rinv, nb);
                 }
-                warp_count(id, [&](int b, uint32_t c) { atomicAdd(sh_hist + b, c); });
+                warp_count(id, [&](uint32_t b, uint32_t c) { atomicAdd(sh_hist + b, c); });
             }
         }
     }
@@ -390,7 +392,7 @@ __global__ void __launch_bounds__(kHistThreads) hist1d_global_kernel(Geometry g,
                 if (kJitter) x = __fadd_rn(x, hist_jitter(seed, (uint64_t)L * g.ns + n, delta));
                 if (lo <= x && __fadd_rn(x, hd) <= re) id = hist_bin(x, rs, re, nb);
             }
-            warp_count(id, [&](int b, uint32_t c) { atomicAdd(ghist + b, c); });
+            warp_count(id, [&](uint32_t b, uint32_t c) { atomicAdd(ghist + b, c); });
         }
     }
 }
@@ -444,7 +446,7 @@ __global__ void __launch_bounds__(kHistThreads) uv_coarse_kernel(Geometry g, con
             for (int j = 0; j < 8; ++j) {
                 int id = -1, xb, yb;
                 if (((valid >> j) & 1u) && uv_bins(x[j], y[j], r, ru, rv, xb, yb)) id = (yb >> cs) * cdim + (xb >> cs);
-                warp_count(id, [&](int b, uint32_t c) { atomicAdd(sh + b, c); });
+                warp_count(id, [&](uint32_t b, uint32_t c) { atomicAdd(sh + b, c); });
             }
         }
     }
@@ -478,16 +480,21 @@ __global__ void __launch_bounds__(kUvThreads, 1)
             const unsigned valid = load8<kVec>(u + o0, g.ns, base, lane, x) & load8<kVec>(v + o0, g.ns, base, lane, y);
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                int lid = -1, gid = -1, xb, yb;
+                // id < n_hot: a slot counter; else n_hot + the global bin (below 2^32 - 2^15 for
+                // every nb <= 65535, so no id is kNoBin)
+                uint32_t id = kNoBin;
+                int xb, yb;
                 if (((valid >> j) & 1u) && uv_bins(x[j], y[j], r, ru, rv, xb, yb)) {
                     const int slot = stab[(yb >> cs) * cdim + (xb >> cs)];
-                    if (slot >= 0)
-                        lid = (slot << (2 * cs)) | ((yb & mask) << cs) | (xb & mask);
-                    else
-                        gid = yb * r.stride + xb;
+                    id = slot >= 0 ? (uint32_t)((slot << (2 * cs)) | ((yb & mask) << cs) | (xb & mask))
+                                   : (uint32_t)n_hot + (uint32_t)yb * (uint32_t)r.stride + (uint32_t)xb;
                 }
-                warp_count(lid, [&](int b, uint32_t c) { atomicAdd(sh_hot + b, c); });
-                warp_count(gid, [&](int b, uint32_t c) { atomicAdd(ghist + b, c); });
+                warp_count(id, [&](uint32_t b, uint32_t c) {
+                    if (b < (uint32_t)n_hot)
+                        atomicAdd(sh_hot + b, c);
+                    else
+                        atomicAdd(ghist + (b - (uint32_t)n_hot), c);
+                });
             }
         }
     }
@@ -498,7 +505,7 @@ __global__ void __launch_bounds__(kUvThreads, 1)
         const int cell = slot_cell[i >> (2 * cs)];
         const int yb = ((cell / cdim) << cs) | ((i >> cs) & mask);
         const int xb = ((cell % cdim) << cs) | (i & mask);
-        atomicAdd(ghist + yb * r.stride + xb, c);
+        atomicAdd(ghist + (size_t)yb * r.stride + xb, c);
     }
 }
 
