@@ -73,7 +73,8 @@ STORE_BYTES = {"f32": 4, "bf16": 2, "f16": 2}
 def parse_args():
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--steps", type=int, default=None,
+                   help="timed steps (default 3; 40 for the label-input workloads, whose step is a few ms)")
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--iters", type=int, default=1000)
@@ -111,6 +112,8 @@ def parse_args():
     p.add_argument("--prefetch", type=int, default=0,
                    help="fused: planes of L2 prefetch ahead of the load ring (0 = library default, -1 = none)")
     args = p.parse_args()
+    if args.steps is None:
+        args.steps = 40 if args.workload in ("labels", "labelsmid") else 3
     if args.variant == "voxel" and args.workload not in ("tv", "tvmid"):
         p.error("--variant voxel applies to the TV workloads only")
     return args

@@ -106,6 +106,86 @@ __global__ void __launch_bounds__(kHistThreads) minmax_final_kernel(const float2
     }
 }
 
+// The ranges of the 2-D histogram in one pass over both fields (uv-hist-kernel.cpp:70-98): per
+// block (min u, max u, min v, max v) over every u and the strictly positive v; kVec: 16-byte
+// loads of both.  minmax_pair_final_kernel folds the blocks into out[0..3].
+__device__ __forceinline__ void fold_minmax4(float4 &a)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a.x = fminf(a.x, __shfl_xor_sync(0xffffffffu, a.x, o));
+        a.y = fmaxf(a.y, __shfl_xor_sync(0xffffffffu, a.y, o));
+        a.z = fminf(a.z, __shfl_xor_sync(0xffffffffu, a.z, o));
+        a.w = fmaxf(a.w, __shfl_xor_sync(0xffffffffu, a.w, o));
+    }
+    __shared__ float4 sw[kHistThreads / 32];
+    if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int i = 1; i < kHistThreads / 32; ++i) {
+            a.x = fminf(a.x, sw[i].x);
+            a.y = fmaxf(a.y, sw[i].y);
+            a.z = fminf(a.z, sw[i].z);
+            a.w = fmaxf(a.w, sw[i].w);
+        }
+}
+
+template <bool kVec>
+__global__ void __launch_bounds__(kHistThreads) minmax_pair_partial_kernel(Geometry g, const float *__restrict__ u,
+                                                                           const float *__restrict__ v,
+                                                                           float4 *__restrict__ partial)
+{
+    float4 a = make_float4(3.402823466e38f, -3.402823466e38f, 3.402823466e38f, -3.402823466e38f);
+    auto see = [&](float x, float y) {
+        a.x = fminf(a.x, x);
+        a.y = fmaxf(a.y, x);
+        if (y > 0.0f) {
+            a.z = fminf(a.z, y);
+            a.w = fmaxf(a.w, y);
+        }
+    };
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (kHistThreads / 32);
+    for (int64_t L = (int64_t)blockIdx.x * (kHistThreads / 32) + (threadIdx.x >> 5); L < g.n_lines; L += warps) {
+        const float *lu = u + L * g.nstride_w, *lv = v + L * g.nstride_w;
+        if constexpr (kVec) {
+#pragma unroll 2
+            for (int q = lane; q < g.ns / 4; q += 32) {
+                const float4 x = __ldg(reinterpret_cast<const float4 *>(lu) + q);
+                const float4 y = __ldg(reinterpret_cast<const float4 *>(lv) + q);
+                see(x.x, y.x);
+                see(x.y, y.y);
+                see(x.z, y.z);
+                see(x.w, y.w);
+            }
+        } else {
+            for (int n = lane; n < g.ns; n += 32) see(__ldg(lu + n), __ldg(lv + n));
+        }
+    }
+    fold_minmax4(a);
+    if (threadIdx.x == 0) partial[blockIdx.x] = a;
+}
+
+__global__ void __launch_bounds__(kHistThreads) minmax_pair_final_kernel(const float4 *__restrict__ partial, int n,
+                                                                         float *__restrict__ out)
+{
+    float4 a = make_float4(3.402823466e38f, -3.402823466e38f, 3.402823466e38f, -3.402823466e38f);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float4 p = partial[i];
+        a.x = fminf(a.x, p.x);
+        a.y = fmaxf(a.y, p.y);
+        a.z = fminf(a.z, p.z);
+        a.w = fmaxf(a.w, p.w);
+    }
+    fold_minmax4(a);
+    if (threadIdx.x == 0) {
+        out[0] = a.x;
+        out[1] = a.y;
+        out[2] = a.z;
+        out[3] = a.w;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Gradient magnitude (grad_magn.cpp:27-55): v = 0.5 sqrt(q_n^2 + q_r^2 + q_c^2) with central
 // differences q = u(x + e) - u(x - e), each accumulated from 0 as the reference does; -1 where
@@ -244,10 +324,11 @@ __device__ __forceinline__ int hist_bin_r(float x, float start, float end, float
     const float f = __fsub_rn(y, fl);
     if (fabsf(__fsub_rn(f, 0.5f)) > fmaf((float)nb, 1e-6f, 1e-6f)) {  // false for a NaN or infinite y
         const float r = f > 0.5f ? __fadd_rn(fl, 1.0f) : fl;  // f > 1/2 only where |y| < 2^23: exact
-        if (!(r >= 0.0f)) return 0;
-        if (r >= (float)(nb - 1)) return nb - 1;
-        return (int)r;
+        return (int)fminf(fmaxf(r, 0.0f), (float)(nb - 1));     // r is finite here
     }
+    // near a half-integer: the bin is floor(y) or floor(y) + 1, clamped, which are the same at
+    // both ends (x at start or end, e.g. a field saturated there)
+    if (f == f && (__fadd_rn(fl, 1.0f) <= 0.0f || fl >= (float)(nb - 1))) return fl >= 0.0f ? nb - 1 : 0;
     return hist_bin(x, start, end, nb);
 }
 
@@ -268,23 +349,22 @@ __device__ __forceinline__ float hist_jitter(uint64_t seed, uint64_t idx, float 
     return __fadd_rn(-0.5f * delta, __fmul_rn(delta, u01));
 }
 
-// Adds 1 to counter `id` (>= 0) for every lane whose id it is.  The lanes that share the first
-// active lane's id add together with one atomic (a warp inside one bin, the common case of a
-// concentrated histogram), every other lane adds its own 1.  A shuffle and two ballots: grouping
-// every distinct id (match.any) cost more than it saved on spread intensities, where a warp's
-// ids are mostly distinct.  add(id, count) does the atomic; every lane that adds reaches the
-// same call, so the warp issues it once.  kNoBin (and -1 converted): the lane adds nothing.
+// Adds 1 to counter `id` for every lane whose id it is (kNoBin, and -1 converted: the lane adds
+// nothing).  The lanes that share lane 0's id add together with one atomic from lane 0 (a warp
+// inside one bin: a saturated or constant region, where 32 atomics on one counter would queue);
+// every other lane adds its own 1.  One shuffle and one ballot: grouping every distinct id
+// (match.any) or the first active lane's (a ballot, a find-first and a shuffle more) cost more
+// than they saved on spread intensities, where a warp's ids are mostly distinct and lanes that
+// share a counter only serialise in the atomic unit.  add(id, count) does the atomic; every
+// lane that adds reaches the same call, so the warp issues it once.
 constexpr uint32_t kNoBin = 0xffffffffu;
 template <typename Add>
 __device__ __forceinline__ void warp_count(uint32_t id, Add add)
 {
-    const unsigned active = __ballot_sync(0xffffffffu, id != kNoBin);
-    if (active == 0u) return;
-    const int leader = __ffs(active) - 1;
-    const uint32_t first = __shfl_sync(0xffffffffu, id, leader);
+    const uint32_t first = __shfl_sync(0xffffffffu, id, 0);
     const unsigned same = __ballot_sync(0xffffffffu, id == first);
     const bool other = id != first;
-    if (id != kNoBin && (other || (int)(threadIdx.x & 31) == leader)) add(id, other ? 1u : (uint32_t)__popc(same));
+    if (id != kNoBin && (other || (threadIdx.x & 31) == 0)) add(id, other ? 1u : (uint32_t)__popc(same));
 }
 
 // Eight values of one line for one lane of a warp that walks the line in steps of 256 values
@@ -355,14 +435,16 @@ __global__ void __launch_bounds__(kHistThreads) hist1d_kernel(Geometry g, const 
             const unsigned valid = load8<kVec>(line, g.ns, base, lane, x);
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                int id = -1;
+                uint32_t id = kNoBin;
                 if ((valid >> j) & 1u) {
                     float xv = x[j];
                     if (kJitter)
                         xv = __fadd_rn(xv, hist_jitter(seed, (uint64_t)L * g.ns + slice8<kVec>(base, lane, j), delta));
-                    if (lo <= xv && __fadd_rn(xv, hd) <= re) id = hist_bin_r(xv, rs, re, rinv, nb);
+                    if (lo <= xv && __fadd_rn(xv, hd) <= re) id = (uint32_t)hist_bin_r(xv, rs, re, rinv, nb);
                 }
-                warp_count(id, [&](uint32_t b, uint32_t c) { atomicAdd(sh_hist + b, c); });
+                // each lane adds its own 1 to its warp's copy (or the block's): grouping the lanes
+                // of one bin measured slower even where half the field sits in one bin
+                if (id != kNoBin) atomicAdd(sh_hist + id, 1u);
             }
         }
     }
@@ -444,8 +526,10 @@ __global__ void __launch_bounds__(kHistThreads) uv_coarse_kernel(Geometry g, con
             const unsigned valid = load8<kVec>(u + o0, g.ns, base, lane, x) & load8<kVec>(v + o0, g.ns, base, lane, y);
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                int id = -1, xb, yb;
-                if (((valid >> j) & 1u) && uv_bins(x[j], y[j], r, ru, rv, xb, yb)) id = (yb >> cs) * cdim + (xb >> cs);
+                uint32_t id = kNoBin;
+                int xb, yb;
+                if (((valid >> j) & 1u) && uv_bins(x[j], y[j], r, ru, rv, xb, yb))
+                    id = (uint32_t)((yb >> cs) * cdim + (xb >> cs));
                 warp_count(id, [&](uint32_t b, uint32_t c) { atomicAdd(sh + b, c); });
             }
         }
@@ -478,23 +562,19 @@ __global__ void __launch_bounds__(kUvThreads, 1)
         for (int base = 0; base < g.ns; base += 256) {
             float x[8], y[8];
             const unsigned valid = load8<kVec>(u + o0, g.ns, base, lane, x) & load8<kVec>(v + o0, g.ns, base, lane, y);
+            // each lane adds its own 1: the 2-D bins of a warp are mostly distinct, and lanes that
+            // do share a counter only serialise in the atomic unit (a warp of one bin is at worst
+            // one voxel per clock per multiprocessor), which costs less than grouping them
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                // id < n_hot: a slot counter; else n_hot + the global bin (below 2^32 - 2^15 for
-                // every nb <= 65535, so no id is kNoBin)
-                uint32_t id = kNoBin;
                 int xb, yb;
                 if (((valid >> j) & 1u) && uv_bins(x[j], y[j], r, ru, rv, xb, yb)) {
                     const int slot = stab[(yb >> cs) * cdim + (xb >> cs)];
-                    id = slot >= 0 ? (uint32_t)((slot << (2 * cs)) | ((yb & mask) << cs) | (xb & mask))
-                                   : (uint32_t)n_hot + (uint32_t)yb * (uint32_t)r.stride + (uint32_t)xb;
-                }
-                warp_count(id, [&](uint32_t b, uint32_t c) {
-                    if (b < (uint32_t)n_hot)
-                        atomicAdd(sh_hot + b, c);
+                    if (slot >= 0)
+                        atomicAdd(sh_hot + ((slot << (2 * cs)) | ((yb & mask) << cs) | (xb & mask)), 1u);
                     else
-                        atomicAdd(ghist + (b - (uint32_t)n_hot), c);
-                });
+                        atomicAdd(ghist + (size_t)yb * r.stride + xb, 1u);
+                }
             }
         }
     }

@@ -64,6 +64,31 @@ int minmax_run(potts_context *ctx, const float *d_f, bool positive, float *out_m
     return POTTS_OK;
 }
 
+// The ranges of uv_hist_auto in one pass: out = (min u, max u, min v, max v) over every u and the
+// strictly positive v (uv-hist-kernel.cpp:70-98); FLT_MAX / -FLT_MAX where there is no value.
+int minmax_pair_run(potts_context *ctx, const float *d_u, const float *d_v, float *out)
+{
+    const Geometry g = field_geometry(ctx);
+    float res[4] = {FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX};
+    if (!field_empty(g)) {
+        const unsigned nb = field_blocks(ctx, g.n_lines, 8);
+        POTTS_TRY(ensure(ctx, ctx->hist, sizeof(float4) * nb + 4 * sizeof(float)));
+        float4 *part = static_cast<float4 *>(ctx->hist.p);
+        float *d_res = reinterpret_cast<float *>(part + nb);
+        if (field_vec(g, d_u) && field_vec(g, d_v))
+            potts::minmax_pair_partial_kernel<true><<<nb, potts::kHistThreads, 0, ctx->stream>>>(g, d_u, d_v, part);
+        else
+            potts::minmax_pair_partial_kernel<false><<<nb, potts::kHistThreads, 0, ctx->stream>>>(g, d_u, d_v, part);
+        potts::minmax_pair_final_kernel<<<1, potts::kHistThreads, 0, ctx->stream>>>(part, (int)nb, d_res);
+        ctx->total_launches += 2;
+        POTTS_CUDA(cudaGetLastError());
+        POTTS_CUDA(cudaMemcpyAsync(res, d_res, sizeof(res), cudaMemcpyDeviceToHost, ctx->stream));
+        POTTS_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    std::copy(res, res + 4, out);
+    return POTTS_OK;
+}
+
 // grad_magn (grad-magn/grad_magn.cpp:60-79): v at every in-mask voxel.
 int grad_magn_run(potts_context *ctx, const float *d_u, float *d_v)
 {

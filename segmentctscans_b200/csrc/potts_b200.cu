@@ -1732,9 +1732,10 @@ int potts_uv_hist_auto(potts_context *ctx, const potts_mapping *map, const float
 {
     if (!ctx || !map || !d_u || !d_v || !out_hist || !out_ranges) return fail(POTTS_EINVAL, "NULL argument");
     POTTS_TRY(check_nbins(nbins));
-    // uv-hist-kernel.cpp:70-98: v over its strictly positive values, u over all
-    POTTS_TRY(potts_min_max_positive(ctx, map, d_v, &out_ranges[2], &out_ranges[3]));
-    POTTS_TRY(potts_min_max(ctx, map, d_u, &out_ranges[0], &out_ranges[1]));
+    // uv-hist-kernel.cpp:70-98: v over its strictly positive values, u over all (one pass)
+    POTTS_CUDA(cudaSetDevice(ctx->device));
+    POTTS_TRY(upload_lines(ctx, map));
+    POTTS_TRY(minmax_pair_run(ctx, d_u, d_v, out_ranges));
     return potts_uv_hist(ctx, map, d_u, d_v, out_ranges[0], out_ranges[1], out_ranges[2], out_ranges[3], nbins,
                          out_hist);
 }

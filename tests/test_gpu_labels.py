@@ -98,6 +98,31 @@ def test_uv_hist_spread_values(cuda_device, oracle_mod, nb):
     assert np.array_equal(h, ref) and int(h.sum()) > 0
 
 
+@pytest.mark.parametrize("nb", [1024, 1, 2, 333])
+def test_histograms_of_saturated_fields(cuda_device, oracle_mod, nb):
+    """A field clamped to its range: about a quarter of the values sit exactly at each end, where the
+    bin formula lands on the half-integers -1/2 and nb - 1/2 (the first and the last bin take them
+    without the division).  Also with jitter, and in the 2-D histogram."""
+    m, u, _ = random_volume(40, 26, 25, 11.7, 3, seed=nb + 3)
+    q1, q3 = np.quantile(m.mask_values(u), [0.25, 0.75])
+    s = np.clip((u - np.float32(q1)) / np.float32(q3 - q1), 0.0, 1.0).astype(np.float32)
+    with potts.make_context(0) as ctx:
+        ds = _dev(ctx, m, s)
+        counts, _, lo, hi = potts.calc_hist_auto(ctx, m, ds.data_ptr(), nb)
+        cj, _ = potts.calc_hist(ctx, m, ds.data_ptr(), 0.0, 1.0, nb, jitter=0.01, seed=5)
+        dv = _dev(ctx, m, np.zeros_like(s))
+        potts.grad_magn(ctx, m, ds.data_ptr(), dv.data_ptr())
+        v = potts.download(ctx, dv)
+        h, rng = potts.uv_hist_auto(ctx, m, ds.data_ptr(), dv.data_ptr(), max(nb // 2, 1))
+        for f in (ds, dv):
+            f.free()
+    assert (lo, hi) == (0.0, 1.0)
+    assert np.array_equal(counts, oracle_mod.calc_hist(m, s, 0.0, 1.0, nb))
+    assert counts[0] >= m.data_size // 5 and counts[-1] >= m.data_size // 5
+    assert np.array_equal(cj, oracle_mod.calc_hist(m, s, 0.0, 1.0, nb, jitter=0.01, seed=5))
+    assert np.array_equal(h, oracle_mod.uv_hist(m, s, v, *rng, max(nb // 2, 1)))
+
+
 def test_empty_range_and_constant_field(cuda_device, oracle_mod):
     """start == end: every in-range value goes to bin 0 (the quotient is NaN), as on the reference's GPU."""
     m, u, _ = random_volume(9, 11, 11, 4.6, 3, seed=2)
