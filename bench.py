@@ -1203,9 +1203,13 @@ def run_labels(args, dist_: Dist) -> None:
     kernels = {k: {"avg_ms": round(avg[k], 4), "gbs": round(algo[k] / (avg[k] / 1000.0) / 1e9, 1),
                    "frac": round(algo[k] / (avg[k] / 1000.0) / 1e9 / peaks["hbm_gbs"], 4),
                    "bytes_per_call": algo[k]} for k in avg}
-    roofline = {"bound": "hbm", "achieved": kernels["grad_magn"]["gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": kernels["grad_magn"]["frac"], "traffic": None, "kernel": "potts::grad_magn_kernel",
-                "bytes_per_voxel": 8, "avg_launch_ms": kernels["grad_magn"]["avg_ms"],
+    # the dominant call: uv_hist_auto (its ranges in one pass over u and v, the coarse cell count
+    # over every 8th line, the hot-cell histogram), against its 16 B per voxel
+    roofline = {"bound": "hbm", "achieved": kernels["uv_hist_auto"]["gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": kernels["uv_hist_auto"]["frac"], "traffic": None,
+                "kernel": "uv_hist_auto: potts::minmax_pair_partial_kernel, potts::uv_coarse_kernel, "
+                          "potts::uv_hist_hot_kernel",
+                "bytes_per_voxel": 16, "avg_launch_ms": kernels["uv_hist_auto"]["avg_ms"],
                 "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)"}
     e2e = None
     if not args.no_e2e:

@@ -14,6 +14,7 @@
 #include <cstdint>
 
 #include "geometry.cuh"
+#include "tma.cuh"
 
 namespace potts {
 
@@ -222,73 +223,132 @@ __global__ void __launch_bounds__(kHistThreads) grad_magn_kernel(Geometry g, con
     }
 }
 
-// The same with one warp per line and 16-byte loads and stores (lines of a multiple of 4 values
-// and stride, 16-byte aligned fields): lane l of a pass takes slices 4q .. 4q+3, q = pass * 32 + l,
-// from the line and its four neighbour lines; the in-line neighbours 4q-1 and 4q+4 come from the
-// neighbouring lanes (or a load at the ends of the pass).  Same operations per voxel as
-// grad_magn_kernel, so the same bits.
-__global__ void __launch_bounds__(kHistThreads) grad_magn_vec_kernel(Geometry g, const float *__restrict__ u,
-                                                                     float *__restrict__ v)
+// Gradient magnitude as a column march (fields of 16-byte lines, 16-byte line stride): a block owns
+// GmTile::TR rows x GmTile::TN slices of a work item's columns [ca, cb) (the work items of the
+// Potts kernel: x = first row, y = first slice, z/w = column range) and walks along the columns
+// with a ring of SLOTS column planes of u in shared memory (rows r0-1 .. r0+TR, slices n0-4 ..
+// n0+TN+3: one TMA box, issued SLOTS-3 planes ahead of the plane after the one being computed).
+// Every u value then comes from DRAM once per tile and its six neighbours from shared memory, with
+// several planes in flight per block.  Thread t takes the slices n0+4(t%32) .. +3 of rows t/32
+// and t/32+8.  The operations per voxel are grad_magn_kernel's, so the bits are the same.  Box
+// rows outside a plane's column belong to other columns (or are zero fill) and are never used:
+// the column table decides every neighbour.  Every wait is bounded; a block whose wait gives up
+// sets *err, drains its loads in flight (bounded) and stops.
+struct GmTile {
+    static constexpr int TR = 16, TN = 128, XR = TR + 2, XS = TN + 8, SLOTS = 5;
+    static constexpr int PLANE = XR * XS;                // floats of one box
+    static constexpr int SLOT = (PLANE + 31) / 32 * 32;  // 128-byte aligned slots
+    static constexpr uint32_t BOX_BYTES = 4u * PLANE;
+    static constexpr int OFF_BAR = 4 * SLOTS * SLOT;
+    static constexpr int SMEM_BYTES = OFF_BAR + SLOTS * 8 + 8 + 128;  // + abort flag, alignment slack
+};
+constexpr int kGmThreads = 256;
+
+__global__ void __launch_bounds__(kGmThreads, 4)
+    grad_magn_tiled_kernel(Geometry g, const int4 *__restrict__ cols, int col_begin, int col_end,
+                           const int4 *__restrict__ work, const __grid_constant__ CUtensorMap u_map,
+                           float *__restrict__ v, int *err)
 {
-    const int lane = threadIdx.x & 31;
-    constexpr int kWarps = kHistThreads / 32;
-    const int nq = g.ns / 4;
-    for (int64_t L = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5); L < g.n_lines; L += (int64_t)gridDim.x * kWarps) {
-        const LineInfo li = load_line(g, L);
-        const bool inner = (li.flags & kHasNextRow) && (li.flags & kHasPrevRow) && li.next_col >= 0 &&
-                           li.prev_col >= 0;
-        const float4 *c4 = reinterpret_cast<const float4 *>(u + L * g.nstride_w);
-        float4 *o4 = reinterpret_cast<float4 *>(v + L * g.nstride_w);
-        if (!inner) {
-            for (int q = lane; q < nq; q += 32) o4[q] = make_float4(-1.0f, -1.0f, -1.0f, -1.0f);
-            continue;
+    using T = GmTile;
+    static_assert(kGmThreads == 256 && T::TR == 16 && T::TN == 128, "thread assignments are for 16 x 128 tiles");
+    extern __shared__ __align__(128) uint8_t gm_raw[];
+    uint8_t *const base = gm_raw + ((128u - (smem_addr(gm_raw) & 127u)) & 127u);
+    float *const smf = reinterpret_cast<float *>(base);
+    uint64_t *const bar = reinterpret_cast<uint64_t *>(base + T::OFF_BAR);
+    volatile int *const abort = reinterpret_cast<volatile int *>(base + T::OFF_BAR + T::SLOTS * 8);
+    const int t = threadIdx.x;
+    const int4 wk = work[blockIdx.x];
+    const int r0 = wk.x, n0 = wk.y, ca = wk.z, cb = wk.w;
+    auto col_at = [&](int c) { return (c >= col_begin && c < col_end) ? __ldg(cols + c) : make_int4(0, 0, 0, 0); };
+    if (t == 0) {
+        for (int k = 0; k < T::SLOTS; ++k) mbar_init(bar + k, 1);
+        *abort = 0;
+        mbar_fence_init();
+        tma_prefetch_desc(&u_map);
+    }
+    __syncthreads();
+    // plane c (ca - 1 <= c <= cb) sits in slot (c - ca + 1) mod SLOTS
+    auto slot_of = [&](int c) { return (c - ca + 1) % T::SLOTS; };
+    uint32_t phase = 0, pending = 0;  // per slot: parity of the next wait, load in flight (thread 0's view)
+    auto issue = [&](int c) {         // thread 0 only
+        const int s = slot_of(c);
+        const int4 ci = col_at(c);
+        mbar_arrive_expect_tx(bar + s, T::BOX_BYTES);
+        tma_load_2d(smf + s * T::SLOT, &u_map, bar + s, n0 - 4, ci.x - ci.y + r0 - 1);
+        pending |= 1u << s;
+    };
+    auto wait_plane = [&](int c) {  // every thread
+        const int s = slot_of(c);
+        const bool ok = mbar_wait_warp(bar + s, (phase >> s) & 1u, abort);
+        if (ok) {
+            phase ^= 1u << s;
+            pending &= ~(1u << s);
         }
-        const float4 *rn = reinterpret_cast<const float4 *>(u + (L + 1) * g.nstride_w);
-        const float4 *rp = reinterpret_cast<const float4 *>(u + (L - 1) * g.nstride_w);
-        const float4 *cn = reinterpret_cast<const float4 *>(u + (int64_t)li.next_col * g.nstride_w);
-        const float4 *cp = reinterpret_cast<const float4 *>(u + (int64_t)li.prev_col * g.nstride_w);
-        const float *line = u + L * g.nstride_w;
-        for (int q0 = 0; q0 < nq; q0 += 32) {
-            const int q = q0 + lane;
-            const bool live = q < nq;
-            float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b = a, c = a, d = a, e = a;
-            if (live) {
-                a = __ldg(c4 + q);
-                b = __ldg(rn + q);
-                c = __ldg(rp + q);
-                d = __ldg(cn + q);
-                e = __ldg(cp + q);
-            }
-            // slice 4q-1 and 4q+4 of the line
-            float before = __shfl_up_sync(0xffffffffu, a.w, 1);
-            float after = __shfl_down_sync(0xffffffffu, a.x, 1);
-            if (live && lane == 0 && q > 0) before = __ldg(line + 4 * q - 1);
-            if (live && (lane == 31 || q + 1 >= nq) && 4 * q + 4 < g.ns) after = __ldg(line + 4 * q + 4);
-            if (!live) continue;
-            const float xs[6] = {before, a.x, a.y, a.z, a.w, after};
-            const float rnv[4] = {b.x, b.y, b.z, b.w}, rpv[4] = {c.x, c.y, c.z, c.w};
-            const float cnv[4] = {d.x, d.y, d.z, d.w}, cpv[4] = {e.x, e.y, e.z, e.w};
-            float r[4];
+        return ok;
+    };
+    if (t == 0)
+        for (int c = ca - 1; c <= cb && c < ca - 1 + (T::SLOTS - 1); ++c) issue(c);
+    wait_plane(ca - 1);
+    wait_plane(ca);
+    const int qd = t & 31, h = t >> 5;
+    const int nq = n0 + 4 * qd;  // first slice of the thread's quad
+    const bool qin = nq < g.ns;  // g.ns % 4 == 0: the whole quad is in the line
+#pragma unroll 1
+    for (int c = ca; c < cb; ++c) {
+        wait_plane(c + 1);
+        // past this barrier every thread is done with plane c-2: its slot takes plane c+SLOTS-2
+        __syncthreads();
+        if (*abort) break;
+        if (t == 0 && c + T::SLOTS - 2 <= cb) issue(c + T::SLOTS - 2);
+        const int4 ci = col_at(c), cp = col_at(c - 1), cn = col_at(c + 1);
+        const float *X = smf + slot_of(c) * T::SLOT;
+        const float *Xp = smf + slot_of(c - 1) * T::SLOT, *Xn = smf + slot_of(c + 1) * T::SLOT;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int n = 4 * q + j;
-                r[j] = -1.0f;
-                if (n > 0 && n + 1 < g.ns) {
-                    float q1 = 0.0f, q2 = 0.0f, q3 = 0.0f;
-                    q1 += xs[j + 2];
-                    q2 += rnv[j];
-                    q3 += cnv[j];
-                    q1 -= xs[j];
-                    q2 -= rpv[j];
-                    q3 -= cpv[j];
-                    float s = q1 * q1;
-                    s = fmaf(q2, q2, s);
-                    s = fmaf(q3, q3, s);
-                    r[j] = 0.5f * __fsqrt_rn(s);
+        for (int m = 0; m < 2; ++m) {
+            const int rr = h + 8 * m, row = r0 + rr;
+            const int b = (rr + 1) * T::XS + 4 * qd + 4;  // slice nq of this row in a box
+            const float4 a = *reinterpret_cast<const float4 *>(X + b);
+            // slices nq-1 and nq+4 (every lane takes part in the shuffles)
+            float before = __shfl_up_sync(0xffffffffu, a.w, 1), after = __shfl_down_sync(0xffffffffu, a.x, 1);
+            if (qd == 0) before = X[b - 1];
+            if (qd == 31) after = X[b + 4];
+            if (!(row >= ci.y && row < ci.z && qin)) continue;
+            float r[4] = {-1.0f, -1.0f, -1.0f, -1.0f};
+            if (row > ci.y && row + 1 < ci.z && row >= cp.y && row < cp.z && row >= cn.y && row < cn.z) {
+                const float4 rn = *reinterpret_cast<const float4 *>(X + b + T::XS);
+                const float4 rp = *reinterpret_cast<const float4 *>(X + b - T::XS);
+                const float4 cnv = *reinterpret_cast<const float4 *>(Xn + b);
+                const float4 cpv = *reinterpret_cast<const float4 *>(Xp + b);
+                const float xs[6] = {before, a.x, a.y, a.z, a.w, after};
+                const float rnv[4] = {rn.x, rn.y, rn.z, rn.w}, rpv[4] = {rp.x, rp.y, rp.z, rp.w};
+                const float cnl[4] = {cnv.x, cnv.y, cnv.z, cnv.w}, cpl[4] = {cpv.x, cpv.y, cpv.z, cpv.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int n = nq + j;
+                    if (n > 0 && n + 1 < g.ns) {
+                        float q1 = 0.0f, q2 = 0.0f, q3 = 0.0f;
+                        q1 += xs[j + 2];
+                        q2 += rnv[j];
+                        q3 += cnl[j];
+                        q1 -= xs[j];
+                        q2 -= rpv[j];
+                        q3 -= cpl[j];
+                        float s = q1 * q1;
+                        s = fmaf(q2, q2, s);
+                        s = fmaf(q3, q3, s);
+                        r[j] = 0.5f * __fsqrt_rn(s);
+                    }
                 }
             }
-            o4[q] = make_float4(r[0], r[1], r[2], r[3]);
+            const int64_t line = (int64_t)ci.x + (row - ci.y);
+            *reinterpret_cast<float4 *>(v + line * g.nstride_w + nq) = make_float4(r[0], r[1], r[2], r[3]);
         }
+    }
+    if (t == 0 && *abort) {
+        // loads still in flight must land before the block's shared memory goes away
+        for (int k = 0; k < T::SLOTS; ++k)
+            if ((pending >> k) & 1u) mbar_wait_bounded(bar + k, (phase >> k) & 1u, kDrainTries);
+        atomicExch(err, 1);
     }
 }
 

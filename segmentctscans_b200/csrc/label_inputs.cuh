@@ -89,17 +89,41 @@ int minmax_pair_run(potts_context *ctx, const float *d_u, const float *d_v, floa
     return POTTS_OK;
 }
 
-// grad_magn (grad-magn/grad_magn.cpp:60-79): v at every in-mask voxel.
+// The column march of grad_magn_tiled_kernel over the work items of GmTile tiles: one TMA box
+// of u per column plane; waits for the stream to report a device-side wait that gave up.
+int grad_magn_tiled(potts_context *ctx, const Geometry &g, const float *d_u, float *d_v)
+{
+    using T = potts::GmTile;
+    POTTS_TRY(plan_tiles(ctx, g.ns, TileChoice{T::TR, T::TN, 1, 64}));
+    if (ctx->n_work == 0) return POTTS_OK;
+    POTTS_TRY(ensure(ctx, ctx->err, sizeof(int)));
+    CUtensorMap map;
+    const uint64_t dims[2] = {(uint64_t)g.nstride_w, (uint64_t)g.n_lines};
+    const uint64_t strides[1] = {sizeof(float) * (uint64_t)g.nstride_w};
+    const uint32_t box[2] = {(uint32_t)T::XS, (uint32_t)T::XR};
+    POTTS_TRY(encode_map(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, d_u, 2, dims, strides, box));
+    POTTS_CUDA(cudaFuncSetAttribute(potts::grad_magn_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    T::SMEM_BYTES));
+    POTTS_CUDA(cudaMemsetAsync(ctx->err.p, 0, sizeof(int), ctx->stream));
+    const MappingCopy &mc = ctx->mapping;
+    potts::grad_magn_tiled_kernel<<<ctx->n_work, potts::kGmThreads, T::SMEM_BYTES, ctx->stream>>>(
+        g, static_cast<const int4 *>(ctx->cols.p), (int)mc.m.col_begin, (int)mc.m.col_end,
+        static_cast<const int4 *>(ctx->work.p), map, d_v, (int *)ctx->err.p);
+    ctx->total_launches += 1;
+    POTTS_CUDA(cudaGetLastError());
+    return check_device_error(ctx);
+}
+
+// grad_magn (grad-magn/grad_magn.cpp:60-79): v at every in-mask voxel.  Fields of 16-byte lines
+// and stride march along the columns (grad_magn_tiled: 0.76 ms at 768^2 x 1024 against 1.09 ms
+// for one warp per line with 16-byte loads of the line and its four neighbour lines, which
+// waited on those loads); others take one thread per voxel.
 int grad_magn_run(potts_context *ctx, const float *d_u, float *d_v)
 {
     const Geometry g = field_geometry(ctx);
     if (field_empty(g)) return POTTS_OK;
-    if (field_vec(g, d_u) && field_vec(g, d_v))  // one warp per line
-        potts::grad_magn_vec_kernel<<<field_blocks(ctx, (g.n_lines + 7) / 8, 8), potts::kHistThreads, 0,
-                                      ctx->stream>>>(g, d_u, d_v);
-    else
-        potts::grad_magn_kernel<<<field_blocks(ctx, g.n_lines, 8), potts::kHistThreads, 0, ctx->stream>>>(g, d_u,
-                                                                                                         d_v);
+    if (field_vec(g, d_u) && field_vec(g, d_v)) return grad_magn_tiled(ctx, g, d_u, d_v);
+    potts::grad_magn_kernel<<<field_blocks(ctx, g.n_lines, 8), potts::kHistThreads, 0, ctx->stream>>>(g, d_u, d_v);
     ctx->total_launches += 1;
     POTTS_CUDA(cudaGetLastError());
     return POTTS_OK;

@@ -40,6 +40,25 @@ def test_min_max_and_grad_magn_bitwise(cuda_device, oracle_mod, geom):
     assert np.array_equal(m.mask_values(v), m.mask_values(ref))
 
 
+@pytest.mark.parametrize("geom", [(260, 150, 150, 70.0, None), (132, 37, 70, 16.5, 136), (8, 90, 20, 9.5, None)],
+                         ids=["segments", "padded-stride", "short-lines"])
+def test_grad_magn_column_march(cuda_device, oracle_mod, geom):
+    """Fields of 16-byte lines march along the columns in 16 x 128 tiles: several row tiles, slice
+    tiles and 64-column segments, a line stride above the slice count, lines shorter than a tile."""
+    n, rows, cols, r, nstride = geom
+    m, u, _ = random_volume(n, rows, cols, r, 3, seed=n + cols, nstride=nstride)
+    with potts.make_context(0) as ctx:
+        du = _dev(ctx, m, u)
+        dv = _dev(ctx, m, np.zeros_like(u))
+        potts.grad_magn(ctx, m, du.data_ptr(), dv.data_ptr())
+        v = potts.download(ctx, dv)
+        for f in (du, dv):
+            f.free()
+    ref = oracle_mod.grad_magn(m, u)
+    assert np.array_equal(m.mask_values(v), m.mask_values(ref))
+    assert (m.mask_values(ref) >= 0).any() and (m.mask_values(ref) == -1).any()
+
+
 @pytest.mark.parametrize("nb,jitter", [(1024, 0.0), (1, 0.0), (37, 0.0), (500, 0.004), (60000, 0.0)],
                          ids=["1024", "1", "37", "500-jitter", "60000-global"])
 def test_calc_hist_bitwise(cuda_device, oracle_mod, nb, jitter):
