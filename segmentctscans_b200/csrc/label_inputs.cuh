@@ -94,7 +94,14 @@ int minmax_pair_run(potts_context *ctx, const float *d_u, const float *d_v, floa
 int grad_magn_tiled(potts_context *ctx, const Geometry &g, const float *d_u, float *d_v)
 {
     using T = potts::GmTile;
-    POTTS_TRY(plan_tiles(ctx, g.ns, TileChoice{T::TR, T::TN, 1, 64}));
+    // segments of 64 columns; of 16 when 64 leave fewer than four blocks per multiprocessor (decided
+    // once per mapping and slice count)
+    if (ctx->gm_segment == 0 || ctx->gm_ns != g.ns) {
+        const size_t items = work_items(ctx->mapping.m, g.ns, TileChoice{T::TR, T::TN, 1, 64}).size();
+        ctx->gm_segment = items < (size_t)4 * std::max(ctx->n_sm, 1) ? 16 : 64;
+        ctx->gm_ns = g.ns;
+    }
+    POTTS_TRY(plan_tiles(ctx, g.ns, TileChoice{T::TR, T::TN, 1, ctx->gm_segment}));
     if (ctx->n_work == 0) return POTTS_OK;
     POTTS_TRY(ensure(ctx, ctx->err, sizeof(int)));
     CUtensorMap map;

@@ -214,6 +214,7 @@ struct potts_context {
     int n_sm = 0;  // multiprocessors of the device
     bool cols_valid = false;
     int work_key[5] = {-1, -1, -1, -1, -1};
+    int gm_segment = 0, gm_ns = -1;  // grad_magn's column segment for this mapping and slice count
     int n_work = 0;
     // Event pairs around runs of consecutive iteration launches (energy
     // evaluations and slab set-up fall outside them), and launch counters.
@@ -307,6 +308,7 @@ int upload_lines(potts_context *ctx, const potts_mapping *map)
     ctx->mapping_valid = false;
     ctx->cols_valid = false;
     ctx->work_key[0] = -1;
+    ctx->gm_segment = 0;
     POTTS_TRY(copy_mapping(map, ctx->mapping));
     const size_t bytes = sizeof(int4) * (size_t)std::max<int64_t>(ctx->mapping.n_lines, 1);
     POTTS_TRY(ensure(ctx, ctx->lines, bytes));
