@@ -412,6 +412,12 @@ def run_ours(args, dist_: Dist) -> None:
                 "bytes_per_voxel_iter": bpv, "avg_launch_ms": round(launch_s * 1000, 4),
                 "avg_iter_ms": round(iter_s * 1000, 4), "iters_per_launch": round(loop_iters / max(loop_launches, 1), 2),
                 "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)"}
+    # the same time against the unfused per-voxel traffic (Xi, V and Vbar each read and written once,
+    # u read once: 2 * 5 (K - 1) stored values + 4 B), the figure the reference's two-kernel
+    # structure has to move; frac above stays on the fused form's own bytes
+    sb = 2 * 5 * (k - 1) * STORE_BYTES[args.storage] + 4
+    roofline["unfused_bytes_per_voxel_iter"] = sb
+    roofline["unfused_frac"] = round(sb * vox / iter_s / 1e9 / peaks["hbm_gbs"], 4)
 
     # quality figures of the last solve
     last = stats[-1]
