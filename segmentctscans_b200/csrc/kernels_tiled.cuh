@@ -137,6 +137,10 @@ __device__ __forceinline__ void ldv(float (&a)[VPT], const ST *p)
     if constexpr (VPT == 4 && sizeof(ST) == 4) {
         const float4 v = *reinterpret_cast<const float4 *>(p);
         a[0] = v.x, a[1] = v.y, a[2] = v.z, a[3] = v.w;
+    } else if constexpr (VPT == 4 && sizeof(ST) == 2) {  // one 8-byte access
+        const uint2 w = *reinterpret_cast<const uint2 *>(p);
+        const float2 lo = Store<ST>::cvt2(w.x), hi = Store<ST>::cvt2(w.y);
+        a[0] = lo.x, a[1] = lo.y, a[2] = hi.x, a[3] = hi.y;
     } else {
 #pragma unroll
         for (int j = 0; j < VPT; j += 2) {
@@ -150,6 +154,9 @@ __device__ __forceinline__ void stv(ST *p, const float (&a)[VPT])
 {
     if constexpr (VPT == 4 && sizeof(ST) == 4) {
         *reinterpret_cast<float4 *>(p) = make_float4(a[0], a[1], a[2], a[3]);
+    } else if constexpr (VPT == 4 && sizeof(ST) == 2) {
+        *reinterpret_cast<uint2 *>(p) =
+            make_uint2(Store<ST>::pack2(make_float2(a[0], a[1])), Store<ST>::pack2(make_float2(a[2], a[3])));
     } else {
 #pragma unroll
         for (int j = 0; j < VPT; j += 2) Store<ST>::st2(p + j, make_float2(a[j], a[j + 1]));

@@ -83,6 +83,16 @@ struct Store<__nv_bfloat16> {
     {
         *reinterpret_cast<__nv_bfloat162 *>(p) = __float22bfloat162_rn(v);
     }
+    // two stored values as one 32-bit word (the first in the low half), widened / rounded
+    __device__ __forceinline__ static float2 cvt2(uint32_t w)
+    {
+        return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+    }
+    __device__ __forceinline__ static uint32_t pack2(float2 v)
+    {
+        const __nv_bfloat162 b = __float22bfloat162_rn(v);
+        return (uint32_t)__bfloat16_as_ushort(b.x) | ((uint32_t)__bfloat16_as_ushort(b.y) << 16);
+    }
 };
 
 template <>
@@ -101,6 +111,16 @@ struct Store<__half> {
     __device__ __forceinline__ static void st2(__half *p, float2 v)
     {
         *reinterpret_cast<__half2 *>(p) = __float22half2_rn(v);
+    }
+    __device__ __forceinline__ static float2 cvt2(uint32_t w)
+    {
+        return __half22float2(__halves2half2(__ushort_as_half((unsigned short)(w & 0xffffu)),
+                                             __ushort_as_half((unsigned short)(w >> 16))));
+    }
+    __device__ __forceinline__ static uint32_t pack2(float2 v)
+    {
+        const __half2 h = __float22half2_rn(v);
+        return (uint32_t)__half_as_ushort(__low2half(h)) | ((uint32_t)__half_as_ushort(__high2half(h)) << 16);
     }
 };
 
