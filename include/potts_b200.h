@@ -394,8 +394,12 @@ int potts_min_max_positive(potts_context *ctx, const potts_mapping *map, const f
                            float *out_max);
 /* grad_magn() (include/grad_magn.h:5-6, grad-magn/grad_magn.cpp:17-79): d_v =
  * 0.5 |central-difference gradient of d_u| at every in-mask voxel, -1 where a
- * neighbour along n, row or column is outside the mask.  Enqueued on the
- * context's stream; d_u and d_v must differ. */
+ * neighbour along n, row or column is outside the mask.  Runs on the
+ * context's stream; d_u and d_v must differ.  Fields of 16-byte lines (slice
+ * count and stride multiples of 4, 16-byte aligned pointers) take the
+ * column-march kernel, and the call then waits for it: POTTS_ETIMEOUT if one
+ * of its bounded waits for a tile load gave up.  Other fields return with the
+ * kernel enqueued. */
 int potts_grad_magn(potts_context *ctx, const potts_mapping *map, const float *d_u, float *d_v);
 /* calc_hist(ctx, in, range_start, range_end, nbins, delta) (include/calc_hist.h:12-13,
  * calc_hist/calc_hist.cpp:23-80,93-138): counts of nbins (1..65535) bins over
