@@ -410,13 +410,12 @@ __device__ __forceinline__ float hist_jitter(uint64_t seed, uint64_t idx, float 
 }
 
 // Adds 1 to counter `id` for every lane whose id it is (kNoBin, and -1 converted: the lane adds
-// nothing).  The lanes that share lane 0's id add together with one atomic from lane 0 (a warp
-// inside one bin: a saturated or constant region, where 32 atomics on one counter would queue);
-// every other lane adds its own 1.  One shuffle and one ballot: grouping every distinct id
-// (match.any) or the first active lane's (a ballot, a find-first and a shuffle more) cost more
-// than they saved on spread intensities, where a warp's ids are mostly distinct and lanes that
-// share a counter only serialise in the atomic unit.  add(id, count) does the atomic; every
-// lane that adds reaches the same call, so the warp issues it once.
+// nothing).  The lanes that share lane 0's id add together with one atomic from lane 0; every
+// other lane adds its own 1 (one shuffle and one ballot).  Used where a warp's lanes often share a
+// counter or a shared counter is costly: the coarse cell count of the 2-D histogram (64 x 64
+// cells) and the 1-D histogram in global memory.  The shared-memory histogram kernels add one
+// atomic per lane instead (see hist1d_kernel).  add(id, count) does the atomic; every lane that
+// adds reaches the same call, so the warp issues it once.
 constexpr uint32_t kNoBin = 0xffffffffu;
 template <typename Add>
 __device__ __forceinline__ void warp_count(uint32_t id, Add add)
