@@ -107,9 +107,7 @@ __global__ void __launch_bounds__(kHistThreads) minmax_final_kernel(const float2
     }
 }
 
-// The ranges of the 2-D histogram in one pass over both fields (uv-hist-kernel.cpp:70-98): per
-// block (min u, max u, min v, max v) over every u and the strictly positive v; kVec: 16-byte
-// loads of both.  minmax_pair_final_kernel folds the blocks into out[0..3].
+// Block-wide fold of (min, max, min, max) into thread 0's a.
 __device__ __forceinline__ void fold_minmax4(float4 &a)
 {
 #pragma unroll
@@ -131,6 +129,9 @@ __device__ __forceinline__ void fold_minmax4(float4 &a)
         }
 }
 
+// The ranges of the 2-D histogram in one pass over both fields (uv-hist-kernel.cpp:70-98): per
+// block (min u, max u, min v, max v) over every u and the strictly positive v; kVec: 16-byte
+// loads of both.  minmax_pair_final_kernel folds the blocks into out[0..3].
 template <bool kVec>
 __global__ void __launch_bounds__(kHistThreads) minmax_pair_partial_kernel(Geometry g, const float *__restrict__ u,
                                                                            const float *__restrict__ v,
