@@ -859,7 +859,7 @@ def run_adjoint(args, dist_: Dist) -> None:
                              "rel": float(abs(gu_h[j] - g) / abs(g) if g != 0 else abs(gu_h[j]))})
         # scalars: rows whose differences cross a nearest-label tie on both sides measure a jump of
         # the loss (a voxel within FP32 spacing of a tie), not its derivative; they are reported,
-        # not judged.  u: relative L2 over the sampled coordinates, per step.
+        # not held to the tolerance.  u: relative L2 over the sampled coordinates, per step.
         smooth = [r for r in rows[: len(ci) + 1] if "jumps" not in r.get("difference", "")]
         u_l2 = {}
         for step in (1e-6, 1e-4):
