@@ -1194,7 +1194,9 @@ def run_labels(args, dist_: Dist) -> None:
     dist_.barrier()
     clocks = ClockSampler(dev.index)
     clocks.start()
+    launches0 = potts._native.host_lib().potts_context_launches(ctx.handle)
     times = [step() for _ in range(args.steps)]
+    launches = potts._native.host_lib().potts_context_launches(ctx.handle) - launches0
     torch.cuda.synchronize(dev)
     dist_.barrier()
     clk = clocks.stop()
@@ -1268,7 +1270,7 @@ def run_labels(args, dist_: Dist) -> None:
             "config": {"workload": f"labels_{m.rows}x{m.cols}x{m.n_images}", "in_mask_voxels": vox,
                        "parallelism": f"replica x{dist_.world}" if dist_.world > 1 else "single",
                        "l2": "inputs larger than L2"},
-            "roofline": roofline, "kernels": kernels, "e2e": e2e, "gpu_launches": 11 * args.steps, "clocks": clk,
+            "roofline": roofline, "kernels": kernels, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
             "cpu_baseline": cpu,
         }
         print(json.dumps(out), flush=True)

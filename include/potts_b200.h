@@ -151,6 +151,9 @@ int potts_context_create(int device, potts_context **out);
 int potts_context_create_on_stream(int device, void *stream, potts_context **out);
 void potts_context_destroy(potts_context *ctx);
 int potts_context_synchronize(potts_context *ctx);
+/* Kernel launches of the library on this context since the last solve began (a solve restarts the
+ * count; the other calls add theirs); 0 for NULL.  No counterpart in the reference. */
+long long potts_context_launches(const potts_context *ctx);
 /* device_memory() (cuda-context/cuda-context.cpp:22-42): free bytes + bytes cached by this context. */
 int potts_device_memory(potts_context *ctx, size_t *available, size_t *total);
 

@@ -99,6 +99,7 @@ SIGNATURES = {
     "potts_context_create_on_stream": (_I, [_I, _P, ctypes.POINTER(_P)]),
     "potts_context_destroy": (None, [_P]),
     "potts_context_synchronize": (_I, [_P]),
+    "potts_context_launches": (ctypes.c_longlong, [_P]),
     "potts_device_memory": (_I, [_P, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]),
     "potts_field_create": (_I, [_P, _MP, ctypes.POINTER(_P)]),
     "potts_field_upload": (_I, [_P, _MP, _FP, ctypes.POINTER(_P)]),

@@ -1231,6 +1231,8 @@ int potts_context_create_on_stream(int device, void *stream, potts_context **out
     return context_init(device, stream, true, out);
 }
 
+long long potts_context_launches(const potts_context *ctx) { return ctx ? (long long)ctx->total_launches : 0; }
+
 void potts_context_destroy(potts_context *ctx)
 {
     if (!ctx) return;
