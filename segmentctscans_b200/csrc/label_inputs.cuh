@@ -206,15 +206,17 @@ int uv_hist_hot(potts_context *ctx, const Geometry &g, const float *d_u, const f
     int16_t *d_table = reinterpret_cast<int16_t *>(d_coarse + cells);
     int16_t *d_cells = d_table + cells;
     POTTS_CUDA(cudaMemsetAsync(d_coarse, 0, sizeof(uint32_t) * cells, ctx->stream));
-    constexpr int kSampleStep = 8;
+    // every step-th line, at least 4096 lines where the field has them (the cell ranking needs no
+    // more; which cells get slots changes only the speed)
+    const int step = (int)std::min<int64_t>(32, std::max<int64_t>(1, g.n_lines / 4096));
     const bool vec = field_vec(g, d_u) && field_vec(g, d_v);
-    const unsigned cblocks = field_blocks(ctx, ((g.n_lines + kSampleStep - 1) / kSampleStep + 7) / 8, 8);
+    const unsigned cblocks = field_blocks(ctx, ((g.n_lines + step - 1) / step + 7) / 8, 8);
     if (vec)
         potts::uv_coarse_kernel<true><<<cblocks, potts::kHistThreads, 0, ctx->stream>>>(g, d_u, d_v, r, cs, cdim,
-                                                                                       kSampleStep, d_coarse);
+                                                                                       step, d_coarse);
     else
         potts::uv_coarse_kernel<false><<<cblocks, potts::kHistThreads, 0, ctx->stream>>>(g, d_u, d_v, r, cs, cdim,
-                                                                                        kSampleStep, d_coarse);
+                                                                                        step, d_coarse);
     ctx->total_launches += 1;
     POTTS_CUDA(cudaGetLastError());
     std::vector<uint32_t> counts((size_t)cells);
