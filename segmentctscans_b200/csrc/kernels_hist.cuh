@@ -500,7 +500,9 @@ __global__ void __launch_bounds__(kHistThreads) hist1d_kernel(Geometry g, const 
                     float xv = x[j];
                     if (kJitter)
                         xv = __fadd_rn(xv, hist_jitter(seed, (uint64_t)L * g.ns + slice8<kVec>(base, lane, j), delta));
-                    if (lo <= xv && __fadd_rn(xv, hd) <= re) id = (uint32_t)hist_bin_r(xv, rs, re, rinv, nb);
+                    // x + 0 compares as x: without jitter the upper test needs no addition
+                    if (lo <= xv && (kJitter ? __fadd_rn(xv, hd) : xv) <= re)
+                        id = (uint32_t)hist_bin_r(xv, rs, re, rinv, nb);
                 }
                 // each lane adds its own 1 to its warp's copy (or the block's): grouping the lanes
                 // of one bin measured slower even where half the field sits in one bin
