@@ -39,6 +39,7 @@ def test_status_strings(native_lib):
     assert native_lib.potts_status_string(0) == b"ok"
     assert b"memory" in native_lib.potts_status_string(2)
     assert native_lib.potts_get_stride(1) == 32 and native_lib.potts_get_stride(33) == 64
+    assert native_lib.potts_context_launches(None) == 0
 
 
 def test_default_options(native_lib):
