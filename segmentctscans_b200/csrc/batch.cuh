@@ -350,7 +350,7 @@ template <int K, typename ST>
 int batch_capture(potts_batch *b, const TileChoice &tile)
 {
     potts_context *ctx = b->ctx;
-    const int launches0 = ctx->total_launches;
+    const int64_t launches0 = ctx->total_launches;
     int cur = 0;
     for (int part = 0; part < 3; ++part) {
         POTTS_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
@@ -391,7 +391,7 @@ int batch_capture(potts_batch *b, const TileChoice &tile)
         b->graph[part] = graph;
         POTTS_CUDA(cudaGraphInstantiate(&b->exec[part], graph, 0));
     }
-    b->graph_launches = ctx->total_launches - launches0;
+    b->graph_launches = (int)(ctx->total_launches - launches0);
     return POTTS_OK;
 }
 

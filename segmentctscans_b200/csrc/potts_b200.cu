@@ -221,7 +221,8 @@ struct potts_context {
     std::vector<cudaEvent_t> seg_ev;
     int seg_used = 0;
     bool seg_open = false;
-    int loop_launches = 0, total_launches = 0;
+    int loop_launches = 0;
+    int64_t total_launches = 0;  // since the last solve began (solves report theirs as int)
     int loop_iters = 0;  // iterations inside the event pairs
     // control words of persistent fused launches (item counters per iteration, grid barrier)
     DevBuf pctl;
@@ -932,7 +933,7 @@ int solve_k(potts_context *ctx, const float *d_u, const float *ci, float lam, fl
         POTTS_TRY(seg_total_ms(ctx, &stats->loop_ms));
         stats->loop_launches = ctx->loop_launches;
         stats->loop_iters = ctx->loop_iters;
-        stats->total_launches = ctx->total_launches;
+        stats->total_launches = (int)ctx->total_launches;
         stats->state_bytes = state_bytes;
         stats->dq_last = 0.0f;
         if (o.track_dq && iters > 0) {
@@ -1163,7 +1164,7 @@ int tv_run(potts_context *ctx, float *d_g, float lam, float tau, int iters, int 
         POTTS_TRY(seg_total_ms(ctx, &stats->loop_ms));
         stats->loop_launches = ctx->loop_launches;
         stats->loop_iters = ctx->loop_iters;
-        stats->total_launches = ctx->total_launches;
+        stats->total_launches = (int)ctx->total_launches;
         stats->state_bytes = sizeof(float) * planes * (uint64_t)std::max<int64_t>(g.plane_w, 1);
         stats->dq_last = 0.0f;
         if (iters > 0) {

@@ -510,7 +510,7 @@ int shard_solve_k(potts_shard *const *sh, int n, int iters, float *const *d_res,
     POTTS_TRY(seg_total_ms(ctx, &stats->loop_ms));
     stats->loop_launches = ctx->loop_launches;
     stats->loop_iters = ctx->loop_iters;
-    stats->total_launches = ctx->total_launches;
+    stats->total_launches = (int)ctx->total_launches;
     stats->state_bytes = 0;
     for (int i = 0; i < n; ++i) stats->state_bytes += sh[i]->state_bytes;
     stats->dq_last = iters > 0 ? std::sqrt(dq[(size_t)iters - 1]) : 0.0f;
