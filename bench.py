@@ -1082,7 +1082,9 @@ def run_fieldio(args, dist_: Dist) -> None:
     dist_.barrier()
     clocks = ClockSampler(dev.index)
     clocks.start()
+    launches0 = potts._native.host_lib().potts_context_launches(ctx.handle)
     times = [step(False) for _ in range(args.steps)]
+    launches = potts._native.host_lib().potts_context_launches(ctx.handle) - launches0
     torch.cuda.synchronize(dev)
     dist_.barrier()
     clk = clocks.stop()
@@ -1140,7 +1142,7 @@ def run_fieldio(args, dist_: Dist) -> None:
                        "archive_bytes": n_arch, "box_bytes": box_bytes,
                        "parallelism": f"replica x{dist_.world}" if dist_.world > 1 else "single",
                        "l2": "inputs larger than L2"},
-            "roofline": roofline, "kernels": kernels, "e2e": e2e, "gpu_launches": 5 * args.steps, "clocks": clk,
+            "roofline": roofline, "kernels": kernels, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
             "cpu_baseline": cpu, "check": "archive round trip equal on every in-mask voxel",
         }
         print(json.dumps(out), flush=True)
