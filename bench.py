@@ -764,10 +764,12 @@ def run_adjoint(args, dist_: Dist) -> None:
     clocks = ClockSampler(dev.index)
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = potts._native.host_lib().potts_context_launches(ctx.handle)
     e0.record(stream)
     for _ in range(args.steps):
         loss, gc, gl = step()
     e1.record(stream)
+    launches = potts._native.host_lib().potts_context_launches(ctx.handle) - launches0
     torch.cuda.synchronize(dev)
     dist_.barrier()
     clk = clocks.stop()
@@ -881,7 +883,7 @@ def run_adjoint(args, dist_: Dist) -> None:
                        "lambda": lam, "tau": tau, "iters": iters, "checkpoint_every": every, "loss_eps": eps,
                        "step": "forward with checkpoints + loss + backward (gradients of u, c, lambda)",
                        "parallelism": f"replica x{dist_.world}" if dist_.world > 1 else "single"},
-            "roofline": None, "e2e": None, "gpu_launches": None, "clocks": clk, "cpu_baseline": None,
+            "roofline": None, "e2e": None, "gpu_launches": launches, "clocks": clk, "cpu_baseline": None,
             "gradient_check": check,
         }
         print(json.dumps(out), flush=True)

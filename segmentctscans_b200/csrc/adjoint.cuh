@@ -81,6 +81,7 @@ int tape_loss(potts_tape *t, const TapeState &final_state, double *loss)
     potts::adj_loss_kernel<K><<<nb, potts::kPlainThreads, 0, ctx->stream>>>(
         t->g, final_state.v, t->d_truth, t->eps, t->inv_count, static_cast<float *>(t->A.p),
         static_cast<double *>(t->loss.p));
+    ctx->total_launches += 1;
     POTTS_CUDA(cudaGetLastError());
     if (loss) {
         POTTS_CUDA(cudaMemcpyAsync(loss, t->loss.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
